@@ -1,0 +1,220 @@
+"""ctypes binding of the oracle (oracle/libcntr_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, never by the nessi_b200 package.  Functions take
+any object with the attributes of ``nessi_b200.herm_matrix.herm_matrix``
+(nt, ntau, size1, sig and contiguous complex128 arrays ret/les/tv/mat) and
+operate on those arrays in place, following libcntr's serial routines (see
+cntr_oracle.hpp for the reference lines).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "libcntr_oracle.so")
+_lib = None
+
+CNTR_MAT_FOURIER = 0
+CNTR_MAT_FIXPOINT = 2
+
+
+class _OrcHM(ctypes.Structure):
+    _fields_ = [("nt", ctypes.c_int), ("ntau", ctypes.c_int), ("size", ctypes.c_int), ("sig", ctypes.c_int),
+                ("ret", ctypes.c_void_p), ("les", ctypes.c_void_p), ("tv", ctypes.c_void_p),
+                ("mat", ctypes.c_void_p)]
+
+
+def build():
+    """Compile the oracle with its Makefile (system g++, OpenMP)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SO):
+            build()
+        L = ctypes.CDLL(_SO)
+        P = ctypes.POINTER(_OrcHM)
+        d, i, vp = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+        sig = {
+            "orc_gregory_weights": (d, [i, i, i]),
+            "orc_gregory_omega": (d, [i, i]),
+            "orc_poly_integration": (d, [i, i, i, i]),
+            "orc_poly_differentiation": (d, [i, i, i]),
+            "orc_poly_interpolation": (d, [i, i, i]),
+            "orc_bd_weights": (d, [i, i]),
+            "orc_rcorr": (d, [i, i, i, i]),
+            "orc_cplx_solve": (i, [i, i, vp, vp, vp]),
+            "orc_green_from_H_const": (None, [P, d, vp, d, d]),
+            "orc_convolution_timestep": (None, [i, P, P, P, P, P, i, d, d]),
+            "orc_convolution_matsubara": (None, [P, P, P, i, d]),
+            "orc_dyson_mat": (None, [P, P, d, vp, i, d, i, i]),
+            "orc_dyson_start": (None, [P, d, vp, P, i, d, d]),
+            "orc_dyson_timestep": (None, [i, P, d, vp, P, i, d, d]),
+            "orc_vie2_mat": (None, [P, P, P, P, d, i, i]),
+            "orc_vie2_start": (None, [P, P, P, P, i, d, d]),
+            "orc_vie2_timestep": (None, [i, P, P, P, P, i, d, d, i]),
+            "orc_extrapolate_timestep": (None, [i, P, i]),
+            "orc_distance_norm2": (d, [i, P, P]),
+            "orc_force_matsubara_hermitian": (None, [P]),
+            "orc_bubble1_scalar": (None, [i, P, P, P, P, P]),
+            "orc_bubble2_scalar": (None, [i, P, P, P, P, P]),
+            "orc_dyson_timestep_batch": (None, [i, i, i, P, d, vp, ctypes.c_long, P, i, d, d, i]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None or a.size == 0:
+        return None
+    assert a.dtype == np.complex128 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def hm(G):
+    """ctypes view of a herm_matrix-like object (keeps no copy)."""
+    return _OrcHM(G.nt, G.ntau, G.size1, G.sig, _ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat))
+
+
+def _H(H):
+    a = H.data if hasattr(H, "data") and not isinstance(H, np.ndarray) else H
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a, a.ctypes.data
+
+
+# --- tables -------------------------------------------------------------------------
+def gregory_weights(k, m, j):
+    return lib().orc_gregory_weights(k, m, j)
+
+
+def gregory_omega(k, j):
+    return lib().orc_gregory_omega(k, j)
+
+
+def poly_integration(k, i, j, l):
+    return lib().orc_poly_integration(k, i, j, l)
+
+
+def poly_differentiation(k, i, l):
+    return lib().orc_poly_differentiation(k, i, l)
+
+
+def poly_interpolation(k, a, l):
+    return lib().orc_poly_interpolation(k, a, l)
+
+
+def bd_weights(k, l):
+    return lib().orc_bd_weights(k, l)
+
+
+def rcorr(k, m, j, l):
+    return lib().orc_rcorr(k, m, j, l)
+
+
+def cplx_solve(M, Q):
+    M = np.ascontiguousarray(M, np.complex128)
+    Q = np.ascontiguousarray(Q, np.complex128)
+    n = M.shape[0]
+    Q2 = Q.reshape(n, -1)
+    X = np.zeros_like(Q2)
+    st = lib().orc_cplx_solve(n, Q2.shape[1], M.ctypes.data, Q2.ctypes.data, X.ctypes.data)
+    return st, X.reshape(Q.shape)
+
+
+# --- contour routines ------------------------------------------------------------------
+def green_from_H(G, mu, H0, beta, h):
+    H0 = np.ascontiguousarray(np.asarray(H0, np.complex128).reshape(G.size1, G.size1))
+    g = hm(G)
+    lib().orc_green_from_H_const(ctypes.byref(g), mu, H0.ctypes.data, beta, h)
+
+
+def convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, k=5):
+    c, a, acc, b, bcc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    lib().orc_convolution_timestep(n, ctypes.byref(c), ctypes.byref(a), ctypes.byref(acc), ctypes.byref(b),
+                                   ctypes.byref(bcc), k, beta, h)
+
+
+def convolution_matsubara(C, A, B, beta, k=5):
+    c, a, b = hm(C), hm(A), hm(B)
+    lib().orc_convolution_matsubara(ctypes.byref(c), ctypes.byref(a), ctypes.byref(b), k, beta)
+
+
+def dyson_mat(G, Sigma, mu, H, beta, k=5, method=CNTR_MAT_FIXPOINT, force_hermitian=True):
+    g, s = hm(G), hm(Sigma)
+    Ha, hp = _H(H)
+    lib().orc_dyson_mat(ctypes.byref(g), ctypes.byref(s), mu, hp, k, beta, method, int(force_hermitian))
+
+
+def dyson_start(G, mu, H, Sigma, beta, h, k=5):
+    g, s = hm(G), hm(Sigma)
+    Ha, hp = _H(H)
+    lib().orc_dyson_start(ctypes.byref(g), mu, hp, ctypes.byref(s), k, beta, h)
+
+
+def dyson_timestep(n, G, mu, H, Sigma, beta, h, k=5):
+    g, s = hm(G), hm(Sigma)
+    Ha, hp = _H(H)
+    lib().orc_dyson_timestep(n, ctypes.byref(g), mu, hp, ctypes.byref(s), k, beta, h)
+
+
+def vie2_mat(G, F, Fcc, Q, beta, k=5, method=CNTR_MAT_FIXPOINT):
+    g, f, fc, q = hm(G), hm(F), hm(Fcc), hm(Q)
+    lib().orc_vie2_mat(ctypes.byref(g), ctypes.byref(f), ctypes.byref(fc), ctypes.byref(q), beta, k, method)
+
+
+def vie2_start(G, F, Fcc, Q, beta, h, k=5):
+    g, f, fc, q = hm(G), hm(F), hm(Fcc), hm(Q)
+    lib().orc_vie2_start(ctypes.byref(g), ctypes.byref(f), ctypes.byref(fc), ctypes.byref(q), k, beta, h)
+
+
+def vie2_timestep(n, G, F, Fcc, Q, beta, h, k=5, method=CNTR_MAT_FIXPOINT):
+    g, f, fc, q = hm(G), hm(F), hm(Fcc), hm(Q)
+    lib().orc_vie2_timestep(n, ctypes.byref(g), ctypes.byref(f), ctypes.byref(fc), ctypes.byref(q), k, beta, h,
+                            method)
+
+
+def extrapolate_timestep(n, G, k=5):
+    g = hm(G)
+    lib().orc_extrapolate_timestep(n, ctypes.byref(g), k)
+
+
+def distance_norm2(tstp, g1, g2):
+    a, b = hm(g1), hm(g2)
+    return lib().orc_distance_norm2(tstp, ctypes.byref(a), ctypes.byref(b))
+
+
+def force_matsubara_hermitian(G):
+    g = hm(G)
+    lib().orc_force_matsubara_hermitian(ctypes.byref(g))
+
+
+def bubble1(tstp, C, A, Acc, B, Bcc):
+    c, a, acc, b, bcc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    lib().orc_bubble1_scalar(tstp, ctypes.byref(c), ctypes.byref(a), ctypes.byref(acc), ctypes.byref(b),
+                             ctypes.byref(bcc))
+
+
+def bubble2(tstp, C, A, Acc, B, Bcc):
+    c, a, acc, b, bcc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    lib().orc_bubble2_scalar(tstp, ctypes.byref(c), ctypes.byref(a), ctypes.byref(acc), ctypes.byref(b),
+                             ctypes.byref(bcc))
+
+
+def dyson_timestep_batch(n0, n1, Gs, mu, Hs, Sigma, beta, h, k=5, nthreads=0):
+    """Time steps n0..n1 for every problem in ``Gs`` (shared Sigma), OpenMP over problems.
+    ``Hs`` is an array (nprob, nt+2, s, s)."""
+    arr = (_OrcHM * len(Gs))(*[hm(G) for G in Gs])
+    Ha = np.ascontiguousarray(Hs, np.complex128)
+    stride = Ha[0].size
+    s = hm(Sigma)
+    lib().orc_dyson_timestep_batch(n0, n1, len(Gs), arr, mu, Ha.ctypes.data, stride, ctypes.byref(s), k, beta, h,
+                                   nthreads)

@@ -1,0 +1,96 @@
+"""The oracle against the known-answer tests of libcntr's own suite (libcntr/test/*.cpp):
+the embedding fixture of dyson.cpp:23-160 and the free-propagator convolution identity
+A*B = (A-B)/(wa-wb) of convolution.cpp:30-185.  Tolerances are the reference's."""
+import numpy as np
+import pytest
+
+from nessi_b200 import herm_matrix, function
+
+
+def _embedding(O, Nt=200, Ntau=400, dt=0.05, beta=10.0):
+    eps1, eps2, lam, mu, k = -1.0, 1.0, 0.2, -0.1, 5
+    h2 = np.array([[eps1, 1j * lam], [-1j * lam, eps2]])
+    hf = function(Nt, 1)
+    hf.set_constant(np.array([[eps1]]))
+    G2 = herm_matrix(Nt, Ntau, 2, -1)
+    O.green_from_H(G2, mu, h2, beta, dt)
+    Gx = herm_matrix(Nt, Ntau, 1, -1)
+    for t in range(-1, Nt + 1):
+        Gx.set_matrixelement(t, 0, 0, G2, 0, 0)
+    Sig = herm_matrix(Nt, Ntau, 1, -1)
+    O.green_from_H(Sig, mu, np.array([[eps2]]), beta, dt)
+    for t in range(-1, Nt + 1):
+        Sig.smul(t, lam * lam)
+    return dict(Nt=Nt, Ntau=Ntau, dt=dt, beta=beta, mu=mu, k=k, hf=hf, Gx=Gx, Sig=Sig, eps1=eps1)
+
+
+def test_dyson_embedding_integro_differential(oracle):
+    O = oracle
+    c = _embedding(O)
+    Ga = herm_matrix(c["Nt"], c["Ntau"], 1, -1)
+    O.dyson_mat(Ga, c["Sig"], c["mu"], c["hf"], c["beta"], c["k"])
+    O.dyson_start(Ga, c["mu"], c["hf"], c["Sig"], c["beta"], c["dt"], c["k"])
+    for n in range(c["k"] + 1, c["Nt"] + 1):
+        O.dyson_timestep(n, Ga, c["mu"], c["hf"], c["Sig"], c["beta"], c["dt"], c["k"])
+    err = sum(O.distance_norm2(t, c["Gx"], Ga) for t in range(c["Nt"] + 1))
+    assert err / c["Nt"] < 1.0e-3          # dyson.cpp:95 (tol_coarse)
+    assert err / c["Nt"] < 1.0e-5          # what the restatement actually reaches (2.1e-6)
+
+
+def test_dyson_embedding_integral_form(oracle):
+    O = oracle
+    c = _embedding(O)
+    Nt, Ntau, k, beta, dt = c["Nt"], c["Ntau"], c["k"], c["beta"], c["dt"]
+    Ga = herm_matrix(Nt, Ntau, 1, -1)
+    O.dyson_mat(Ga, c["Sig"], c["mu"], c["hf"], beta, k)
+    G0 = herm_matrix(Nt, Ntau, 1, -1)
+    O.green_from_H(G0, c["mu"], np.array([[c["eps1"]]]), beta, dt)
+    F, Fcc = herm_matrix(Nt, Ntau, 1, -1), herm_matrix(Nt, Ntau, 1, -1)
+    for t in range(0, Nt + 1):
+        O.convolution_timestep(t, F, G0, G0, c["Sig"], c["Sig"], beta, dt, k)
+        O.convolution_timestep(t, Fcc, c["Sig"], c["Sig"], G0, G0, beta, dt, k)
+        F.smul(t, -1)
+        Fcc.smul(t, -1)
+        if t == k:
+            O.vie2_start(Ga, F, Fcc, G0, beta, dt, k)
+        elif t > k:
+            O.vie2_timestep(t, Ga, F, Fcc, G0, beta, dt, k)
+    err = sum(O.distance_norm2(t, c["Gx"], Ga) for t in range(Nt + 1))
+    assert err / Nt < 1.0e-6               # dyson.cpp:133 (tol_tight)
+
+
+@pytest.mark.parametrize("sig", [-1, 1])
+def test_convolution_free_propagators(oracle, sig):
+    O = oracle
+    nt, ntau, beta, h, wa, wb, k = 7, 500, 5.0, 0.01, 1.123, 0.345, 5
+    A, B, C, AB = (herm_matrix(nt, ntau, 1, sig) for _ in range(4))
+    O.green_from_H(A, 0.0, np.array([[wa]]), beta, h)
+    O.green_from_H(B, 0.0, np.array([[wb]]), beta, h)
+    C = A.copy()
+    for t in range(-1, nt + 1):
+        C.incr_timestep(t, B, -1.0)
+        C.smul(t, 1.0 / (wa - wb))
+    for t in range(-1, nt + 1):
+        O.convolution_timestep(t, AB, A, A, B, B, beta, h, k)
+    err = sum(O.distance_norm2(t, C, AB) for t in range(-1, nt + 1))
+    assert err < 1e-6 * 4                  # convolution.cpp:28 (eps, four norms summed there)
+
+
+def test_extrapolation_is_exact_for_polynomials(oracle):
+    """extrapolate_timestep reproduces a degree-k polynomial in t exactly
+    (the property libcntr/test/utilities.cpp:213-300 checks)."""
+    O = oracle
+    nt, ntau, k = 12, 6, 5
+    G = herm_matrix(nt, ntau, 1, -1)
+    f = lambda t, tp: (0.3 + 0.1j) * t ** 3 - 0.2 * t * tp + 0.05j * tp ** 2 + 1.0
+    for t in range(nt + 1):
+        for tp in range(t + 1):
+            G.ret[G.ret_index(t, tp)] = f(t, tp)
+        for tp in range(t + 1):
+            G.les[G.les_index(tp, t)] = f(tp, t)
+        G.tv[t, :, 0, 0] = [f(t, m) for m in range(ntau + 1)]
+    n = 9
+    O.extrapolate_timestep(n, G, k)
+    assert np.allclose(G.tv[n + 1, :, 0, 0], [f(n + 1, m) for m in range(ntau + 1)], rtol=1e-10, atol=1e-9)
+    assert np.allclose(G.ret_row(n + 1)[k + 1:, 0, 0], [f(n + 1, tp) for tp in range(k + 1, n + 2)],
+                       rtol=1e-10, atol=1e-9)
