@@ -1,0 +1,94 @@
+/* nessi_gpu.h - C ABI of libnessi_gpu.so, the B200 implementation of libcntr's
+ * Kadanoff-Baym time-stepping hot path.
+ *
+ * The reference has no plugin system: its boundary is the C++ template API of namespace
+ * cntr (libcntr/cntr/cntr_dyson_decl.hpp, cntr_vie2_decl.hpp, cntr_convolution_decl.hpp),
+ * instantiated for double in libcntr.so.  Each entry point below names the reference
+ * interface it replaces.  All functions return 0 on success or one of NESSI_ERR_*;
+ * nessi_gpu_last_error() gives a one-line description of the last failure.
+ *
+ * Data are exchanged in libcntr's herm_matrix<double> layout
+ * (libcntr/cntr/cntr_herm_matrix_impl.hpp:457-477), so a caller passes
+ * G.retptr(0,0), G.lesptr(0,0), G.tvptr(0,0) and G.matptr(0) unchanged:
+ *   ret(t,t') [t'<=t] at (t(t+1)/2+t') s^2,  les(t,t') [t<=t'] at (t'(t'+1)/2+t) s^2,
+ *   tv(t,tau) at (t(ntau+1)+tau) s^2,        mat(tau) at tau s^2,
+ * every element a row-major s x s block of complex<double> (re, im interleaved).
+ * cntr::function<double> H is passed as H.ptr(-1): (nt+2) blocks, t = -1 first
+ * (libcntr/cntr/cntr_function_decl.hpp:45).
+ *
+ * A batch holds many problems ("k-points") that are advanced together on one GPU.
+ * Problems with the same sigma_group share one self-energy Sigma (a local or
+ * k-independent Sigma, as in the reference's lattice drivers, examples/programs/gw.cpp:386-420);
+ * all problems of a group have the same size1, ntau, sig, beta, h and solve order.
+ * Calls on one batch are stream-ordered on the batch's stream and must come from one host
+ * thread at a time.
+ */
+#ifndef NESSI_GPU_H
+#define NESSI_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NESSI_OK 0
+#define NESSI_ERR_ARG 1       /* bad argument or state */
+#define NESSI_ERR_OOM 2       /* device allocation failed */
+#define NESSI_ERR_CUDA 3      /* CUDA / cuBLAS runtime error */
+#define NESSI_ERR_SINGULAR 4  /* a step matrix had a zero pivot */
+#define NESSI_ERR_TIMEOUT 5   /* a bounded device wait gave up */
+
+#define NESSI_PREC_FP64 0     /* every sum and solve in complex<double> */
+#define NESSI_PREC_MIXED 1    /* history sums from an FP32 copy of G^tv, FP64 solves */
+
+typedef struct nessi_batch nessi_batch;
+
+/* One problem: the dimensions of its herm_matrix G and of the Dyson equation
+ * [i d/dt + mu - H(t)] G - Sigma * G = delta (cntr_dyson_decl.hpp:92). */
+typedef struct {
+    int nt, ntau, size1, sig; /* herm_matrix<double>(nt, ntau, size1, sig) */
+    int solve_order;          /* SolveOrder k, 1..5 (MAX_SOLVE_ORDER, cntr_global_settings.hpp:37) */
+    int sigma_group;          /* problems with equal group share one Sigma */
+    double beta, h, mu;
+} nessi_problem_desc;
+
+/* Select the CUDA device used by later batches; replaces nothing (libcntr is CPU-only). */
+int nessi_gpu_init(int device);
+const char *nessi_gpu_last_error(void);
+
+/* Allocate device storage for `count` problems.  precision is NESSI_PREC_*. */
+int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, int count, int precision);
+int nessi_gpu_batch_destroy(nessi_batch *b);
+/* Bytes of device memory held by the batch. */
+int nessi_gpu_batch_bytes(nessi_batch *b, long long *bytes);
+
+/* Copy a whole herm_matrix G of problem p (host, libcntr layout) to / from the device.
+ * Any pointer may be NULL to skip that component.  Replaces direct access to
+ * herm_matrix<T>::ret_/les_/tv_/mat_ (cntr_herm_matrix_decl.hpp:79-93). */
+int nessi_gpu_set_G(nessi_batch *b, int p, const void *ret, const void *les, const void *tv, const void *mat);
+int nessi_gpu_get_G(nessi_batch *b, int p, void *ret, void *les, void *tv, void *mat);
+/* One time step of G as a herm_matrix_timestep slice [ret(n,0..n) | tv(n,0..ntau) |
+ * les(0..n,n)] (cntr_herm_matrix_timestep_decl.hpp:67-75; herm_matrix::get_timestep,
+ * cntr_herm_matrix_impl.hpp:2156).  tstp = -1 gives mat. */
+int nessi_gpu_get_timestep(nessi_batch *b, int p, int tstp, void *slice);
+int nessi_gpu_set_timestep(nessi_batch *b, int p, int tstp, const void *slice);
+/* H(t) of problem p as cntr::function<double> data, (nt+2) s^2 complex. */
+int nessi_gpu_set_H(nessi_batch *b, int p, const void *H);
+
+/* The shared Sigma of a group: full herm_matrix, or one time step slice
+ * (herm_matrix::set_timestep, cntr_herm_matrix_impl.hpp:2098). */
+int nessi_gpu_set_sigma(nessi_batch *b, int group, const void *ret, const void *les, const void *tv,
+                        const void *mat);
+int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void *slice);
+
+/* cntr::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder) for every problem of the
+ * batch with nt >= n (cntr_dyson_decl.hpp:92, cntr_dyson_impl.hpp:1618-1648).  n > k.
+ * G must hold time steps 0..n-1 and mat; Sigma and H must hold 0..n. */
+int nessi_gpu_dyson_timestep(nessi_batch *b, int n);
+
+/* Wait for all work queued on the batch. */
+int nessi_gpu_synchronize(nessi_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NESSI_GPU_H */

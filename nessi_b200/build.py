@@ -1,0 +1,48 @@
+"""Build recipe for libnessi_gpu.so (in-tree, sm_100a).
+
+``python -m nessi_b200.build`` compiles nessi_b200/csrc/*.cu with nvcc for
+``-gencode arch=compute_100a,code=sm_100a`` into nessi_b200/libnessi_gpu.so.
+No GPU is needed to build.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libnessi_gpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+         "-Xcompiler", "-fPIC", "-shared", "-ccbin", "/usr/bin/g++"]
+SOURCES = ["nessi_gpu.cu"]
+
+
+def _inputs():
+    out = []
+    for f in os.listdir(CSRC):
+        if f.endswith((".cu", ".cuh", ".inc", ".h")):
+            out.append(os.path.join(CSRC, f))
+    out.append(os.path.join(os.path.dirname(HERE), "include", "nessi_gpu.h"))
+    return out
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(f) <= t for f in _inputs())
+
+
+def build(force=False, verbose=False):
+    if not force and up_to_date():
+        return LIB
+    cmd = [NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcublas"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd, cwd=CSRC)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print("built", LIB)

@@ -1,0 +1,494 @@
+// libnessi_gpu.so: batches of Kadanoff-Baym problems advanced on one B200.
+// Host side of the C ABI declared in include/nessi_gpu.h.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/nessi_gpu.h"
+#include "kernels_dyson.cuh"
+
+
+
+namespace {
+
+thread_local std::string g_err;
+int g_device = 0;
+std::vector<int> g_tables_ready;  // devices whose c_tab was filled
+
+void set_err(const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess) {                                                                \
+            set_err("CUDA error %s (%s) at %s:%d", cudaGetErrorName(e_), cudaGetErrorString(e_), \
+                    __FILE__, __LINE__);                                                        \
+            return e_ == cudaErrorMemoryAllocation ? NESSI_ERR_OOM : NESSI_ERR_CUDA;            \
+        }                                                                                       \
+    } while (0)
+
+#define CKB(x)                                                                      \
+    do {                                                                            \
+        cublasStatus_t s_ = (x);                                                    \
+        if (s_ != CUBLAS_STATUS_SUCCESS) {                                          \
+            set_err("cuBLAS error %d at %s:%d", (int)s_, __FILE__, __LINE__);       \
+            return NESSI_ERR_CUDA;                                                  \
+        }                                                                           \
+    } while (0)
+
+#define CKR(x)                      \
+    do {                            \
+        int r_ = (x);               \
+        if (r_ != NESSI_OK) return r_; \
+    } while (0)
+
+inline long tri_h(long t) { return t * (t + 1) / 2; }
+
+int ensure_tables(int dev) {
+    if (std::find(g_tables_ready.begin(), g_tables_ready.end(), dev) != g_tables_ready.end()) return NESSI_OK;
+    IntegTables t;
+    std::memcpy(t.greg, cntr_tab_gregory, sizeof t.greg);
+    std::memcpy(t.omega, cntr_tab_omega, sizeof t.omega);
+    std::memcpy(t.poly_int, cntr_tab_poly_int, sizeof t.poly_int);
+    std::memcpy(t.poly_diff, cntr_tab_poly_diff, sizeof t.poly_diff);
+    std::memcpy(t.poly_interp, cntr_tab_poly_interp, sizeof t.poly_interp);
+    std::memcpy(t.bd, cntr_tab_bd, sizeof t.bd);
+    std::memcpy(t.rcorr, cntr_tab_rcorr, sizeof t.rcorr);
+    CK(cudaMemcpyToSymbol(c_tab, &t, sizeof t));
+    g_tables_ready.push_back(dev);
+    return NESSI_OK;
+}
+
+struct Prob {
+    nessi_problem_desc d;
+    int group = -1;
+    double2 *gret = nullptr, *gles = nullptr, *gtv = nullptr, *gmat = nullptr;
+    double2 *H = nullptr, *minv_ret = nullptr, *minv_les = nullptr;
+};
+
+struct Group {
+    int user_id = 0;
+    int s = 1, ntau = 0, sig = -1, k = 5, ntmax = 0;
+    double h = 0, beta = 0;
+    double2 *sret = nullptr, *sles = nullptr, *stv = nullptr, *smat = nullptr;
+    double2 *Ldense = nullptr, *Tdense = nullptr, *tvcoef = nullptr;
+    double2 *badv = nullptr, *btv = nullptr, *gles = nullptr;
+    int ldc = 0;
+    int dense_valid = -1, ret_valid = -1, les_valid = -1;
+    std::vector<int> members;        // problem indices, nt descending
+    std::vector<ProbDev> h_probs;    // same order; col = position
+    ProbDev *d_probs = nullptr;
+};
+
+}  // namespace
+
+struct nessi_batch {
+    int device = 0;
+    int precision = NESSI_PREC_FP64;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t cublas = nullptr;
+    std::vector<Prob> probs;
+    std::vector<Group> groups;
+    std::vector<void *> allocs;
+    long long bytes = 0;
+
+    int alloc(double2 **p, long long n_cplx) {
+        if (n_cplx <= 0) { *p = nullptr; return NESSI_OK; }
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, (size_t)n_cplx * sizeof(double2));
+        if (e != cudaSuccess) {
+            set_err("cudaMalloc of %lld bytes failed: %s", n_cplx * 16LL, cudaGetErrorString(e));
+            return NESSI_ERR_OOM;
+        }
+        e = cudaMemsetAsync(q, 0, (size_t)n_cplx * sizeof(double2), stream);
+        if (e != cudaSuccess) { set_err("cudaMemset failed"); return NESSI_ERR_CUDA; }
+        allocs.push_back(q);
+        bytes += n_cplx * 16LL;
+        *p = (double2 *)q;
+        return NESSI_OK;
+    }
+};
+
+namespace {
+
+GroupDev group_dev(const Group &g) {
+    GroupDev d;
+    d.sret = g.sret; d.sles = g.sles; d.stv = g.stv; d.smat = g.smat;
+    d.Ldense = g.Ldense; d.Tdense = g.Tdense; d.tvcoef = g.tvcoef;
+    d.badv = g.badv; d.btv = g.btv; d.gles = g.gles;
+    d.ntmax = g.ntmax; d.ntau = g.ntau; d.s = g.s; d.sig = g.sig; d.k = g.k;
+    d.ldc = g.ldc; d.h = g.h; d.beta = g.beta;
+    return d;
+}
+
+int check_batch(nessi_batch *b) {
+    if (!b) { set_err("null batch"); return NESSI_ERR_ARG; }
+    CK(cudaSetDevice(b->device));
+    return NESSI_OK;
+}
+
+int check_prob(nessi_batch *b, int p) {
+    CKR(check_batch(b));
+    if (p < 0 || p >= (int)b->probs.size()) { set_err("problem index %d out of range", p); return NESSI_ERR_ARG; }
+    return NESSI_OK;
+}
+
+int find_group(nessi_batch *b, int user_id) {
+    for (size_t i = 0; i < b->groups.size(); i++)
+        if (b->groups[i].user_id == user_id) return (int)i;
+    return -1;
+}
+
+// ---- per-size kernel launch table ----------------------------------------------------
+template <int S> size_t ret_smem(int k) {
+    size_t start = (size_t)(k * k * S * S + k * S * S + (k * S) * (k * S) + k * S * S) * 16 + 16;
+    size_t phase = (size_t)(RetCfg<S>::GM * RetCfg<S>::E + RetCfg<S>::E + S * S) * 16;
+    return std::max(start, phase);
+}
+template <int S> size_t les_smem(int k) {
+    size_t start = (size_t)((k * S) * (k * S) + k * S * S) * 16 + 16;
+    size_t phase = (size_t)(RetCfg<S>::JB * S * S + S * S + 8 * 32 * S) * 16;
+    return std::max(start, phase);
+}
+
+template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
+    const GroupDev gd = group_dev(g);
+    cudaStream_t st = b->stream;
+    const int k = g.k;
+    // step-matrix inverses
+    int les_lo = std::min(n, std::max(k + 1, g.les_valid + 1));
+    int r0 = g.ret_valid + 1, r1 = n - k - 1;
+    k_prep_problem<S><<<nact, 64, 0, st>>>(gd, g.d_probs, n, les_lo, r0, r1);
+    CK(cudaGetLastError());
+    g.les_valid = n - 1;
+    if (r1 >= r0) g.ret_valid = r1;
+    int d_lo = std::min(n, g.dense_valid + 1);
+    {
+        long work = (long)(n + 1) * S * S * (n - d_lo + 1) + (long)n * S * S;
+        int blocks = (int)std::min<long>(std::max<long>(1, (work + 255) / 256), 1184);
+        k_prep_group<S><<<blocks, 256, 0, st>>>(gd, n, d_lo);
+        CK(cudaGetLastError());
+        g.dense_valid = n - 1;
+    }
+    // retarded row
+    {
+        size_t sm = ret_smem<S>(k);
+        CK(cudaFuncSetAttribute(k_ret<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_ret<S><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+        CK(cudaGetLastError());
+    }
+    // tv row
+    {
+        constexpr int TT = 128 / S;
+        dim3 grid((g.ntau + 1 + TT - 1) / TT, nact);
+        k_tv<S, TT><<<grid, TT * S, 0, st>>>(gd, g.d_probs, n);
+        CK(cudaGetLastError());
+    }
+    // Sigma-shared convolutions tv*vt + les*adv for all active problems
+    {
+        long rows = (long)(n + 1 + g.ntau + 1) * S * S;
+        dim3 grid((unsigned)std::min<long>((rows + 255) / 256, 64), nact);
+        k_les_operands<S><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+        CK(cudaGetLastError());
+        const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+        const int m = nact * S, nn = (n + 1) * S;
+        const long ldL = (long)(g.ntmax + 1) * S, ldT = (long)(g.ntau + 1) * S;
+        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (n + 1) * S, &one,
+                        (const cuDoubleComplex *)g.badv, g.ldc, (const cuDoubleComplex *)g.Ldense, (int)ldL, &zero,
+                        (cuDoubleComplex *)g.gles, g.ldc));
+        const double2 *T = S == 1 ? g.stv : g.Tdense;
+        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (g.ntau + 1) * S, &one,
+                        (const cuDoubleComplex *)g.btv, g.ldc, (const cuDoubleComplex *)T, (int)ldT, &one,
+                        (cuDoubleComplex *)g.gles, g.ldc));
+    }
+    // lesser column
+    {
+        size_t sm = les_smem<S>(k);
+        CK(cudaFuncSetAttribute(k_les<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_les<S><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+        CK(cudaGetLastError());
+    }
+    return NESSI_OK;
+}
+
+int step_dispatch(nessi_batch *b, Group &g, int n, int nact) {
+    switch (g.s) {
+        case 1: return step_group<1>(b, g, n, nact);
+        case 2: return step_group<2>(b, g, n, nact);
+        case 3: return step_group<3>(b, g, n, nact);
+        case 4: return step_group<4>(b, g, n, nact);
+        case 5: return step_group<5>(b, g, n, nact);
+        case 6: return step_group<6>(b, g, n, nact);
+        case 7: return step_group<7>(b, g, n, nact);
+        case 8: return step_group<8>(b, g, n, nact);
+    }
+    set_err("size1 = %d not supported (1..8)", g.s);
+    return NESSI_ERR_ARG;
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+const char *nessi_gpu_last_error(void) { return g_err.c_str(); }
+
+int nessi_gpu_init(int device) {
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) { set_err("device %d not present (%d devices)", device, n); return NESSI_ERR_ARG; }
+    g_device = device;
+    CK(cudaSetDevice(device));
+    return ensure_tables(device);
+}
+
+int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, int count, int precision) {
+    if (!out || !desc || count <= 0) { set_err("batch_create: bad arguments"); return NESSI_ERR_ARG; }
+    if (precision != NESSI_PREC_FP64 && precision != NESSI_PREC_MIXED) { set_err("bad precision %d", precision); return NESSI_ERR_ARG; }
+    *out = nullptr;
+    for (int i = 0; i < count; i++) {
+        const nessi_problem_desc &d = desc[i];
+        if (d.nt < 0 || d.ntau < d.solve_order || d.size1 < 1 || d.size1 > NESSI_MAXS || (d.sig != 1 && d.sig != -1) ||
+            d.solve_order < 1 || d.solve_order > CNTR_KMAX || !(d.h > 0) || !(d.beta > 0)) {
+            set_err("problem %d: bad descriptor (nt=%d ntau=%d size1=%d sig=%d k=%d)", i, d.nt, d.ntau, d.size1,
+                    d.sig, d.solve_order);
+            return NESSI_ERR_ARG;
+        }
+    }
+    CK(cudaSetDevice(g_device));
+    CKR(ensure_tables(g_device));
+    nessi_batch *b = new nessi_batch();
+    b->device = g_device;
+    b->precision = precision;
+    auto fail = [&](int r) { nessi_gpu_batch_destroy(b); return r; };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_err("stream creation failed");
+        return fail(NESSI_ERR_CUDA);
+    }
+    if (cublasCreate(&b->cublas) != CUBLAS_STATUS_SUCCESS) { set_err("cublasCreate failed"); return fail(NESSI_ERR_CUDA); }
+    cublasSetStream(b->cublas, b->stream);
+    cublasSetMathMode(b->cublas, CUBLAS_DEFAULT_MATH);
+    b->probs.resize(count);
+    // groups
+    for (int i = 0; i < count; i++) {
+        const nessi_problem_desc &d = desc[i];
+        b->probs[i].d = d;
+        int gi = find_group(b, d.sigma_group);
+        if (gi < 0) {
+            Group g;
+            g.user_id = d.sigma_group; g.s = d.size1; g.ntau = d.ntau; g.sig = d.sig; g.k = d.solve_order;
+            g.h = d.h; g.beta = d.beta; g.ntmax = d.nt;
+            b->groups.push_back(g);
+            gi = (int)b->groups.size() - 1;
+        }
+        Group &g = b->groups[gi];
+        if (g.s != d.size1 || g.ntau != d.ntau || g.sig != d.sig || g.k != d.solve_order || g.h != d.h || g.beta != d.beta) {
+            set_err("problem %d does not match the other problems of sigma_group %d", i, d.sigma_group);
+            return fail(NESSI_ERR_ARG);
+        }
+        g.ntmax = std::max(g.ntmax, d.nt);
+        g.members.push_back(i);
+        b->probs[i].group = gi;
+    }
+    // device storage
+    for (int i = 0; i < count; i++) {
+        Prob &p = b->probs[i];
+        const long s2 = (long)p.d.size1 * p.d.size1, nt = p.d.nt, M = p.d.ntau + 1;
+        int r;
+        if ((r = b->alloc(&p.gret, tri_h(nt + 1) * s2)) || (r = b->alloc(&p.gles, tri_h(nt + 1) * s2)) ||
+            (r = b->alloc(&p.gtv, (nt + 1) * M * s2)) || (r = b->alloc(&p.gmat, M * s2)) ||
+            (r = b->alloc(&p.H, (nt + 2) * s2)) || (r = b->alloc(&p.minv_ret, (nt + 1) * s2)) ||
+            (r = b->alloc(&p.minv_les, (nt + 1) * s2)))
+            return fail(r);
+    }
+    for (Group &g : b->groups) {
+        std::stable_sort(g.members.begin(), g.members.end(),
+                         [&](int x, int y) { return b->probs[x].d.nt > b->probs[y].d.nt; });
+        const long S = g.s, s2 = S * S, N = g.ntmax + 1, M = g.ntau + 1;
+        g.ldc = (int)(g.members.size() * S);
+        int r;
+        if ((r = b->alloc(&g.sret, tri_h(N) * s2)) || (r = b->alloc(&g.sles, tri_h(N) * s2)) ||
+            (r = b->alloc(&g.stv, N * M * s2)) || (r = b->alloc(&g.smat, M * s2)) ||
+            (r = b->alloc(&g.Ldense, N * S * N * S)) || (S > 1 && (r = b->alloc(&g.Tdense, N * S * M * S))) ||
+            (r = b->alloc(&g.tvcoef, N * s2)) || (r = b->alloc(&g.badv, N * S * g.ldc)) ||
+            (r = b->alloc(&g.btv, M * S * g.ldc)) || (r = b->alloc(&g.gles, N * S * g.ldc)))
+            return fail(r);
+        for (size_t c = 0; c < g.members.size(); c++) {
+            const Prob &p = b->probs[g.members[c]];
+            ProbDev pd;
+            pd.gret = p.gret; pd.gles = p.gles; pd.gtv = p.gtv; pd.gmat = p.gmat;
+            pd.H = p.H; pd.minv_ret = p.minv_ret; pd.minv_les = p.minv_les;
+            pd.mu = p.d.mu; pd.nt = p.d.nt; pd.col = (int)c; pd.pad = 0;
+            g.h_probs.push_back(pd);
+        }
+        void *q = nullptr;
+        if (cudaMalloc(&q, g.h_probs.size() * sizeof(ProbDev)) != cudaSuccess) { set_err("cudaMalloc failed"); return fail(NESSI_ERR_OOM); }
+        b->allocs.push_back(q);
+        g.d_probs = (ProbDev *)q;
+        if (cudaMemcpyAsync(g.d_probs, g.h_probs.data(), g.h_probs.size() * sizeof(ProbDev), cudaMemcpyHostToDevice,
+                            b->stream) != cudaSuccess) {
+            set_err("descriptor upload failed");
+            return fail(NESSI_ERR_CUDA);
+        }
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) { set_err("stream sync failed"); return fail(NESSI_ERR_CUDA); }
+    *out = b;
+    return NESSI_OK;
+}
+
+int nessi_gpu_batch_destroy(nessi_batch *b) {
+    if (!b) return NESSI_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (void *q : b->allocs) cudaFree(q);
+    if (b->cublas) cublasDestroy(b->cublas);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return NESSI_OK;
+}
+
+int nessi_gpu_batch_bytes(nessi_batch *b, long long *bytes) {
+    CKR(check_batch(b));
+    *bytes = b->bytes;
+    return NESSI_OK;
+}
+
+static int copy_cplx(nessi_batch *b, void *dst, const void *src, long n_cplx, cudaMemcpyKind kind) {
+    if (!dst || !src || n_cplx <= 0) return NESSI_OK;
+    CK(cudaMemcpyAsync(dst, src, (size_t)n_cplx * 16, kind, b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_G(nessi_batch *b, int p, const void *ret, const void *les, const void *tv, const void *mat) {
+    CKR(check_prob(b, p));
+    Prob &q = b->probs[p];
+    const long s2 = (long)q.d.size1 * q.d.size1, nt = q.d.nt, M = q.d.ntau + 1;
+    CKR(copy_cplx(b, q.gret, ret, tri_h(nt + 1) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, q.gles, les, tri_h(nt + 1) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, q.gtv, tv, (nt + 1) * M * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, q.gmat, mat, M * s2, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_get_G(nessi_batch *b, int p, void *ret, void *les, void *tv, void *mat) {
+    CKR(check_prob(b, p));
+    Prob &q = b->probs[p];
+    const long s2 = (long)q.d.size1 * q.d.size1, nt = q.d.nt, M = q.d.ntau + 1;
+    CKR(copy_cplx(b, ret, q.gret, tri_h(nt + 1) * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, les, q.gles, tri_h(nt + 1) * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, tv, q.gtv, (nt + 1) * M * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, mat, q.gmat, M * s2, cudaMemcpyDeviceToHost));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+static int slice_copy(nessi_batch *b, double2 *ret, double2 *tv, double2 *les, double2 *mat, int nt, int ntau, int s,
+                      int tstp, void *slice, bool to_device) {
+    const long s2 = (long)s * s, M = ntau + 1;
+    if (tstp < -1 || tstp > nt) { set_err("time step %d out of range [-1, %d]", tstp, nt); return NESSI_ERR_ARG; }
+    if (!slice) { set_err("null slice"); return NESSI_ERR_ARG; }
+    double2 *h = (double2 *)slice;
+    cudaMemcpyKind kd = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    auto cp = [&](double2 *dev, double2 *host, long n) {
+        return to_device ? copy_cplx(b, dev, host, n, kd) : copy_cplx(b, host, dev, n, kd);
+    };
+    if (tstp == -1) {
+        CKR(cp(mat, h, M * s2));
+    } else {
+        const long n1 = tstp + 1;
+        CKR(cp(ret + tri_h(tstp) * s2, h, n1 * s2));
+        CKR(cp(tv + tstp * M * s2, h + n1 * s2, M * s2));
+        CKR(cp(les + tri_h(tstp) * s2, h + (n1 + M) * s2, n1 * s2));
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_get_timestep(nessi_batch *b, int p, int tstp, void *slice) {
+    CKR(check_prob(b, p));
+    Prob &q = b->probs[p];
+    return slice_copy(b, q.gret, q.gtv, q.gles, q.gmat, q.d.nt, q.d.ntau, q.d.size1, tstp, slice, false);
+}
+
+int nessi_gpu_set_timestep(nessi_batch *b, int p, int tstp, const void *slice) {
+    CKR(check_prob(b, p));
+    Prob &q = b->probs[p];
+    return slice_copy(b, q.gret, q.gtv, q.gles, q.gmat, q.d.nt, q.d.ntau, q.d.size1, tstp, (void *)slice, true);
+}
+
+int nessi_gpu_set_H(nessi_batch *b, int p, const void *H) {
+    CKR(check_prob(b, p));
+    Prob &q = b->probs[p];
+    if (!H) { set_err("null H"); return NESSI_ERR_ARG; }
+    CKR(copy_cplx(b, q.H, H, (long)(q.d.nt + 2) * q.d.size1 * q.d.size1, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
+    Group &g = b->groups[q.group];
+    g.ret_valid = -1;
+    g.les_valid = -1;
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_sigma(nessi_batch *b, int group, const void *ret, const void *les, const void *tv, const void *mat) {
+    CKR(check_batch(b));
+    int gi = find_group(b, group);
+    if (gi < 0) { set_err("unknown sigma_group %d", group); return NESSI_ERR_ARG; }
+    Group &g = b->groups[gi];
+    const long s2 = (long)g.s * g.s, N = g.ntmax + 1, M = g.ntau + 1;
+    CKR(copy_cplx(b, g.sret, ret, tri_h(N) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g.sles, les, tri_h(N) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g.stv, tv, N * M * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g.smat, mat, M * s2, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
+    g.ret_valid = g.les_valid = g.dense_valid = -1;
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void *slice) {
+    CKR(check_batch(b));
+    int gi = find_group(b, group);
+    if (gi < 0) { set_err("unknown sigma_group %d", group); return NESSI_ERR_ARG; }
+    Group &g = b->groups[gi];
+    CKR(slice_copy(b, g.sret, g.stv, g.sles, g.smat, g.ntmax, g.ntau, g.s, tstp, (void *)slice, true));
+    if (tstp >= 0) {
+        g.ret_valid = std::min(g.ret_valid, tstp - 1);
+        g.les_valid = std::min(g.les_valid, tstp - 1);
+        g.dense_valid = std::min(g.dense_valid, tstp - 1);
+    }
+    return NESSI_OK;
+}
+
+int nessi_gpu_dyson_timestep(nessi_batch *b, int n) {
+    CKR(check_batch(b));
+    for (Group &g : b->groups) {
+        if (n <= g.k) { set_err("dyson_timestep: n = %d must exceed the solve order %d", n, g.k); return NESSI_ERR_ARG; }
+        int nact = 0;
+        for (int i : g.members) nact += b->probs[i].d.nt >= n ? 1 : 0;
+        if (nact == 0) continue;
+        CKR(step_dispatch(b, g, n, nact));
+    }
+    return NESSI_OK;
+}
+
+int nessi_gpu_synchronize(nessi_batch *b) {
+    CKR(check_batch(b));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+}  // extern "C"

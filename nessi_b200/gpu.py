@@ -1,0 +1,171 @@
+"""Python host API over libnessi_gpu.so (C ABI in include/nessi_gpu.h).
+
+``Batch`` advances many problems ("k-points") sharing a self-energy on one GPU.  The
+cntr-style functions at the bottom (``dyson_timestep`` ...) mirror libcntr's signatures
+(libcntr/cntr/cntr_dyson_decl.hpp:92) for single problems.
+
+There is no CPU fallback: if the CUDA library is missing or no device is present every
+call raises ``NessiGpuError``.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .herm_matrix import herm_matrix, function
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libnessi_gpu.so")
+_lib = None
+_inited = False
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_ERRNAMES = {1: "NESSI_ERR_ARG", 2: "NESSI_ERR_OOM", 3: "NESSI_ERR_CUDA", 4: "NESSI_ERR_SINGULAR",
+             5: "NESSI_ERR_TIMEOUT"}
+
+
+class NessiGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (_ERRNAMES.get(code, str(code)), msg))
+        self.code = code
+
+
+class ProblemDesc(ctypes.Structure):
+    _fields_ = [("nt", ctypes.c_int), ("ntau", ctypes.c_int), ("size1", ctypes.c_int), ("sig", ctypes.c_int),
+                ("solve_order", ctypes.c_int), ("sigma_group", ctypes.c_int),
+                ("beta", ctypes.c_double), ("h", ctypes.c_double), ("mu", ctypes.c_double)]
+
+
+EXPORTS = {
+    "nessi_gpu_init": (ctypes.c_int, [ctypes.c_int]),
+    "nessi_gpu_last_error": (ctypes.c_char_p, []),
+    "nessi_gpu_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ProblemDesc),
+                                              ctypes.c_int, ctypes.c_int]),
+    "nessi_gpu_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_batch_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "nessi_gpu_set_G": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_get_G": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_get_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "nessi_gpu_set_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "nessi_gpu_set_H": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "nessi_gpu_set_sigma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_set_sigma_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "nessi_gpu_dyson_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "nessi_gpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+}
+
+
+def load_library(path=None):
+    """Load libnessi_gpu.so and declare its exports (no device needed)."""
+    global _lib
+    if _lib is None:
+        p = path or _LIB_PATH
+        if not os.path.exists(p):
+            raise NessiGpuError(3, "%s is missing: run `python -m nessi_b200.build`" % p)
+        L = ctypes.CDLL(p)
+        for name, (res, args) in EXPORTS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise NessiGpuError(rc, load_library().nessi_gpu_last_error().decode())
+
+
+def init(device=0):
+    global _inited
+    L = load_library()
+    _check(L.nessi_gpu_init(device))
+    _inited = True
+
+
+def _ptr(a):
+    if a is None or a.size == 0:
+        return None
+    if a.dtype != np.complex128 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("arrays must be C-contiguous complex128")
+    return a.ctypes.data
+
+
+class Batch:
+    """Problems advanced together on one GPU; problems with equal ``sigma_group`` share Sigma."""
+
+    def __init__(self, descs, precision=PREC_FP64):
+        if not _inited:
+            init(0)
+        arr = (ProblemDesc * len(descs))()
+        for i, d in enumerate(descs):
+            arr[i] = ProblemDesc(d["nt"], d["ntau"], d.get("size1", 1), d.get("sig", -1), d.get("solve_order", 5),
+                                 d.get("sigma_group", 0), d["beta"], d["h"], d.get("mu", 0.0))
+        self.descs = [dict(d) for d in descs]
+        h = ctypes.c_void_p()
+        _check(load_library().nessi_gpu_batch_create(ctypes.byref(h), arr, len(descs), precision))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().nessi_gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nbytes(self):
+        v = ctypes.c_longlong()
+        _check(load_library().nessi_gpu_batch_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    def set_G(self, p, G):
+        _check(load_library().nessi_gpu_set_G(self._h, p, _ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
+
+    def get_G(self, p, G):
+        _check(load_library().nessi_gpu_get_G(self._h, p, _ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
+
+    def get_timestep(self, p, tstp, out):
+        _check(load_library().nessi_gpu_get_timestep(self._h, p, tstp, _ptr(out)))
+
+    def set_timestep(self, p, tstp, data):
+        _check(load_library().nessi_gpu_set_timestep(self._h, p, tstp, _ptr(np.ascontiguousarray(data))))
+
+    def set_H(self, p, H):
+        a = H.data if isinstance(H, function) else H
+        _check(load_library().nessi_gpu_set_H(self._h, p, _ptr(np.ascontiguousarray(a, np.complex128))))
+
+    def set_sigma(self, group, S):
+        _check(load_library().nessi_gpu_set_sigma(self._h, group, _ptr(S.ret), _ptr(S.les), _ptr(S.tv), _ptr(S.mat)))
+
+    def set_sigma_timestep(self, group, tstp, data):
+        _check(load_library().nessi_gpu_set_sigma_timestep(self._h, group, tstp,
+                                                           _ptr(np.ascontiguousarray(data, np.complex128))))
+
+    def dyson_timestep(self, n):
+        _check(load_library().nessi_gpu_dyson_timestep(self._h, n))
+
+    def synchronize(self):
+        _check(load_library().nessi_gpu_synchronize(self._h))
+
+
+# ---- cntr-style single-problem entry points ---------------------------------------------
+def dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder=5):
+    """cntr::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder) on the GPU
+    (cntr_dyson_decl.hpp:92): writes G's time step n in place."""
+    b = Batch([dict(nt=G.nt, ntau=G.ntau, size1=G.size1, sig=G.sig, solve_order=SolveOrder, beta=beta, h=h,
+                    mu=mu)])
+    b.set_G(0, G)
+    b.set_H(0, H)
+    b.set_sigma(0, Sigma)
+    b.dyson_timestep(n)
+    slc = np.zeros((2 * (n + 1) + G.ntau + 1, G.size1, G.size1), np.complex128)
+    b.get_timestep(0, n, slc)
+    G.set_timestep_data(n, slc)
+    b.close()

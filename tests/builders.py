@@ -1,0 +1,65 @@
+"""Seeded synthetic problems for the parity tests, built with the oracle (CPU).
+
+A problem is a Dyson equation [i d/dt + mu - H(t)] G - Sigma*G = 1 with
+  Sigma = lam^2 * G_bath, G_bath = green_from_H of a random Hermitian s x s bath matrix,
+  H(t)  = h0 + f(t) h1 for t >= 0 and H(-1) = h0 (h0, h1 random Hermitian),
+solved by the oracle with dyson_mat (fixpoint) -> dyson_start -> dyson_timestep.
+"""
+import numpy as np
+
+from nessi_b200 import herm_matrix, function
+
+
+def rand_herm(rng, s, scale):
+    x = rng.normal(0, scale, (s, s)) + 1j * rng.normal(0, scale, (s, s))
+    return (x + x.conj().T) / 2
+
+
+def make_sigma(O, rng, nt, ntau, s, sig, beta, h, lam=0.5):
+    hb = rand_herm(rng, s, 0.7) + np.diag(rng.uniform(-1, 1, s))
+    S = herm_matrix(nt, ntau, s, sig)
+    O.green_from_H(S, 0.0, hb, beta, h)
+    for t in range(-1, nt + 1):
+        S.smul(t, lam * lam)
+    return S
+
+
+def make_H(rng, nt, s, h):
+    h0 = rand_herm(rng, s, 0.8)
+    h1 = rand_herm(rng, s, 0.4)
+    H = function(nt, s)
+    H.set_value(-1, h0)
+    for t in range(nt + 1):
+        H.set_value(t, h0 + np.sin(1.3 * t * h) * h1)
+    return H
+
+
+def solve_oracle(O, G, H, Sigma, mu, beta, h, k, nt_stop=None):
+    """Full oracle solution; returns G (all steps) and a copy after the bootstrap."""
+    O.dyson_mat(G, Sigma, mu, H, beta, k)
+    O.dyson_start(G, mu, H, Sigma, beta, h, k)
+    G0 = G.copy()
+    nt = G.nt if nt_stop is None else nt_stop
+    for n in range(k + 1, nt + 1):
+        O.dyson_timestep(n, G, mu, H, Sigma, beta, h, k)
+    return G, G0
+
+
+def rel_err(a, b):
+    """max|a - b| / max|b| (0 when both vanish)."""
+    den = np.max(np.abs(b)) if b.size else 0.0
+    num = np.max(np.abs(a - b)) if a.size else 0.0
+    return 0.0 if den == 0 else num / den
+
+
+def component_errors(Gg, Go, n0, n1):
+    """Relative errors of ret/les/tv over time steps n0..n1."""
+    out = {}
+    rr = [Gg.ret_row(n) for n in range(n0, n1 + 1)]
+    ro = [Go.ret_row(n) for n in range(n0, n1 + 1)]
+    out["ret"] = rel_err(np.concatenate(rr), np.concatenate(ro))
+    lr = [Gg.les_col(n) for n in range(n0, n1 + 1)]
+    lo = [Go.les_col(n) for n in range(n0, n1 + 1)]
+    out["les"] = rel_err(np.concatenate(lr), np.concatenate(lo))
+    out["tv"] = rel_err(Gg.tv[n0:n1 + 1], Go.tv[n0:n1 + 1])
+    return out
