@@ -1,0 +1,348 @@
+"""Benchmark of the batched Dyson time stepping (libcntr dyson_timestep hot path) on B200.
+
+One bench step = the whole time-stepping phase n = k+1..nt of every k-point of the workload
+(the metric counts k-point time steps; Matsubara and bootstrap are set-up, outside the timed
+region).  Inputs are resident in HBM for `value`; `e2e` repeats the step through the public
+API with host buffers (Sigma, H and bootstrap uploaded, the full G downloaded every step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload config1] [--precision fp64|mixed]
+
+Under torchrun each rank advances its own k-grid (shifted by rank/N of a grid spacing): the
+k-points are independent, so ranks share no data ("scaling": "weak").  `--impl reference`
+times the CPU restatement of libcntr's serial path (oracle/, OpenMP over k-points) on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "k-point timesteps/s (batched Dyson), mixed vs FP64 on B200 at <=1e-8 rel err"
+UNIT = "k-point time steps/s"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", "nessi_clocks_%d_%d.csv" % (os.getpid(), device_index))
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        load = [x for x in sm if smax and x > 0.3 * smax] or sm
+        med = float(np.median(load)) if load else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (CPU restatement of libcntr's serial dyson_timestep), OpenMP over k
+# ------------------------------------------------------------------------------------------
+def cpu_sample(W, target_s=15.0, max_threads=None):
+    """Time windows of consecutive time steps at several n for P problems in parallel, fit
+    t(n) = a + b N + c N^2 (N = n+1) per step and integrate over n = k+1..nt.
+    Returns (kpt_steps_per_s, threads, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import psutil
+    from nessi_b200 import herm_matrix
+    d0 = W.descs[0]
+    nt, ntau, s, k = d0["nt"], d0["ntau"], d0["size1"], W.k
+    threads = max_threads or os.cpu_count() or 1
+    gbytes = 16.0 * s * s * ((nt + 1) * (nt + 2) + (nt + 1) * (ntau + 1)) / 1e9
+    avail = psutil.virtual_memory().available / 1e9
+    P = int(max(1, min(threads, W.nprob, (0.25 * avail) // max(gbytes, 1e-9))))
+    Gs = []
+    for p in range(P):
+        G = herm_matrix(nt, ntau, s, d0["sig"])
+        B = W.boot[p]
+        G.mat[...] = B.mat
+        for t in range(k + 1):
+            G.set_timestep_data(t, B.get_timestep(t))
+        Gs.append(G)
+    Hs = np.ascontiguousarray(W.H[:P])
+    beta, h, mu = d0["beta"], d0["h"], d0["mu"]
+    # probe one step at the largest n to size the windows
+    t0 = time.perf_counter()
+    O.dyson_timestep_batch(nt, nt, Gs, mu, Hs, W.sigma, beta, h, k, threads)
+    t1 = time.perf_counter() - t0
+    pts = sorted(set([max(k + 1, int(nt * f)) for f in (0.1, 0.3, 0.6, 1.0)]))
+    win = int(max(1, min(40, target_s / (len(pts) * max(t1, 1e-6)))))
+    ns, ts = [], []
+    for n in pts:
+        a = max(k + 1, n - win + 1)
+        t0 = time.perf_counter()
+        O.dyson_timestep_batch(a, n, Gs, mu, Hs, W.sigma, beta, h, k, threads)
+        dt = (time.perf_counter() - t0) / (n - a + 1)
+        ns.append(0.5 * (a + n) + 1)
+        ts.append(dt)
+    N = np.array(ns)
+    A = np.stack([np.ones_like(N), N, N * N], 1)
+    coef, *_ = np.linalg.lstsq(A, np.array(ts), rcond=None)
+    allN = np.arange(k + 2, nt + 2, dtype=float)
+    total = float(np.sum(coef[0] + coef[1] * allN + coef[2] * allN * allN))
+    value = P * (nt - k) / total
+    resid = float(np.max(np.abs(A @ coef - np.array(ts)) / np.array(ts)))
+    desc = ("%d problems in parallel on %d threads, windows of %d steps at n=%s, fit t(n)=a+bN+cN^2 "
+            "integrated over n=%d..%d (max fit residual %.1f%%)" % (P, threads, win, pts, k + 1, nt, 100 * resid))
+    return value, threads, desc
+
+
+# ------------------------------------------------------------------------------------------
+def build_workload(name, rank, world):
+    from nessi_b200 import workloads
+    shift = 0.0 if world == 1 else (2 * math.pi / 256) * rank / world
+    if name == "config1":
+        return workloads.config1(kshift=shift)
+    if name == "config1-small":
+        return workloads.config1(nk=64, nt=200, ntau=100, kshift=shift)
+    if name == "config1-ncu":  # config-1 chain at nt=ntau=300: 1.5 GB of G^tv history, > L2
+        return workloads.config1(nk=256, nt=300, ntau=300, kshift=shift)
+    raise SystemExit("unknown workload %s" % name)
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    W = build_workload(args.workload, 0, 1)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, thr, desc = cpu_sample(W, target_s=args.cpu_seconds)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * W.kpt_steps() / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+            "impl": "reference",
+            "config": dict(workload=args.workload, **W.info),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "libcntr needs Eigen3, absent here: the timed CPU path is the oracle's C++ restatement "
+                    "of libcntr's serial dyson_timestep with OpenMP over k-points"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config1")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    from nessi_b200 import gpu, workloads
+    torch.cuda.set_device(local)
+    gpu.init(local)
+    W = build_workload(args.workload, rank, world)
+    prec = gpu.PREC_MIXED if args.precision == "mixed" else gpu.PREC_FP64
+    b = gpu.Batch(W.descs, precision=prec)
+    workloads.upload(b, W)
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    k = W.k
+    nt = max(d["nt"] for d in W.descs)
+
+    def propagate():
+        for n in range(k + 1, nt + 1):
+            b.dyson_timestep(n)
+
+    for _ in range(args.warmup):
+        propagate()
+    b.synchronize()
+    b.set_profiling(True)
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        propagate()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = allmax(e0.elapsed_time(e1), world)
+    prof = b.read_profile()
+    b.set_profiling(False)
+    units = world * W.kpt_steps() * args.steps
+    value = units / (ms / 1000.0)
+    kernels_per_step = 7  # prep_problem, prep_group, ret, mat_operator, tv, les_operands, les
+    gpu_launches = kernels_per_step * (nt - k) * args.steps
+
+    # roofline of the dominant kernel of ours (GEMM is cuBLAS)
+    peak, peak_kind = load_peaks()
+    own = {kname: v for kname, v in prof.items() if kname != "gemm"}
+    dom = max(own, key=lambda x: own[x][0])
+    dms, dl, dbytes = own[dom]
+    achieved = (dbytes / dl) / ((dms / dl) / 1000.0) / 1e9 if dl else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (dom, args.workload))
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+    roofline = {"kernel": "k_" + dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": dbytes / dl if dl else None,
+                "avg_launch_ms": dms / dl if dl else None}
+    breakdown = {kname: {"ms": v[0] / args.steps, "launches": v[1] // args.steps,
+                         "share": v[0] / max(1e-9, sum(x[0] for x in prof.values()))}
+                 for kname, v in prof.items()}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        from nessi_b200 import herm_matrix
+        host = []
+        for d in W.descs:
+            host.append(herm_matrix(d["nt"], d["ntau"], d["size1"], d["sig"]))
+        try:
+            import torch as _t
+            pinned = True
+            for G in host:
+                for nm in ("ret", "les", "tv", "mat"):
+                    a = getattr(G, nm)
+                    t = _t.empty(a.size * 2, dtype=_t.float64, pin_memory=True)
+                    setattr(G, nm, t.numpy().view(np.complex128).reshape(a.shape))
+        except Exception:
+            pinned = False
+        sig_bytes = sum(getattr(W.sigma, x).nbytes for x in ("ret", "les", "tv", "mat"))
+        h2d = sig_bytes + W.H.nbytes + sum(B.mat.nbytes + sum(B.get_timestep(t).nbytes for t in range(k + 1))
+                                           for B in W.boot)
+        d2h = sum(G.ret.nbytes + G.les.nbytes + G.tv.nbytes + G.mat.nbytes for G in host)
+        barrier(world)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            workloads.upload(b, W)
+            propagate()
+            for p, G in enumerate(host):
+                b.get_G(p, G)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ems = allmax(f0.elapsed_time(f1), world)
+        e2e = {"value": units / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "pinned_host": pinned, "ms_per_step": ems / args.steps}
+        # sanity: the downloaded result is finite
+        if not all(np.isfinite(G.tv[nt]).all() for G in host[:4]):
+            e2e["warning"] = "non-finite values in the result"
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, thr, desc = cpu_sample(W, target_s=args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "complex128" if args.precision == "fp64" else "complex64 history / complex128 solves",
+                "data": "synthetic",
+                "config": dict(workload=args.workload, precision=args.precision,
+                               l2="inputs larger than L2 (G^tv history %.1f GB per GPU)" % (
+                                   16.0 * W.nprob * (nt + 1) * (W.descs[0]["ntau"] + 1) * W.descs[0]["size1"] ** 2 / 1e9),
+                               bootstrap="free propagator of H_k(-1) for mat and steps 0..k (set-up, untimed)",
+                               **W.info),
+                "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": gpu_launches, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

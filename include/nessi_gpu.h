@@ -85,6 +85,25 @@ int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void
  * G must hold time steps 0..n-1 and mat; Sigma and H must hold 0..n. */
 int nessi_gpu_dyson_timestep(nessi_batch *b, int n);
 
+/* Run the batch's work on the caller's cudaStream_t (NULL: a private stream again).
+ * libcntr has no streams; this lets a caller order the batch with its own work. */
+int nessi_gpu_set_stream(nessi_batch *b, void *stream);
+
+/* Kernel timing with CUDA events on the batch stream.  Kernel ids: */
+#define NESSI_KERNEL_PREP 0          /* step-matrix inverses, tv coefficients, dense Sigma copies */
+#define NESSI_KERNEL_RET 1           /* G^R(n, .) Volterra recursion */
+#define NESSI_KERNEL_TV 2            /* G^tv(n, .) history stream + solve */
+#define NESSI_KERNEL_LES_OPERANDS 3  /* operands of the Sigma-shared products */
+#define NESSI_KERNEL_GEMM 4          /* K_n G^mat, tv*vt and les*adv products (cuBLAS ZGEMM) */
+#define NESSI_KERNEL_LES 5           /* G^<(., n) Volterra recursion */
+#define NESSI_KERNEL_MATOP 6         /* Matsubara operator K_n of the tv row */
+#define NESSI_KERNEL_COUNT 7
+/* Turn timing on/off (resets counters).  No reference counterpart. */
+int nessi_gpu_set_profiling(nessi_batch *b, int on);
+/* Total device time (ms), launches and algorithmic bytes (flops for GEMM) recorded for one
+ * kernel id since the last read; resets that counter.  No reference counterpart. */
+int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *launches, double *bytes);
+
 /* Wait for all work queued on the batch. */
 int nessi_gpu_synchronize(nessi_batch *b);
 

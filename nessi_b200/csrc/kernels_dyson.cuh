@@ -17,6 +17,7 @@ struct ProbDev {
     double2 *gret, *gles, *gtv, *gmat;  // this problem's G (libcntr layout)
     const double2 *H;                   // (nt+2) s^2 blocks, H(-1) first
     double2 *minv_ret, *minv_les;       // (nt+1) s^2: inverses of the ret / les+tv step matrices
+    float2 *gtv32;                      // mixed precision: FP32 copy of G^tv (plane layout) or null
     double mu;
     int nt;
     int col;                            // column of this problem in the group's GEMM operands
@@ -29,6 +30,9 @@ struct GroupDev {
     double2 *Tdense;   // ((ntmax+1)s) x ((ntau+1)s) row-major: Sigma^tv(j,m) reordered (s>1)
     double2 *tvcoef;   // (ntmax+1) s^2: coefficients of the tv history sum at the current step
     double2 *badv, *btv, *gles;  // GEMM operands / result, leading dimension ldc
+    double2 *Kmat;     // ((ntau+1)s) x ((ntau+1)s) row-major: Matsubara operator of the step
+    double2 *Gmat_all; // ((ntau+1)s) x ldc: every problem's G^mat as columns
+    double2 *Cmat;     // ((ntau+1)s) x ldc: Matsubara part of the tv right-hand side
     int ntmax, ntau, s, sig, k;
     int ldc;           // >= nprob * s
     double h, beta;
@@ -247,194 +251,190 @@ __device__ void les_start_block(const GroupDev &g, const ProbDev &p, int n, cons
 }
 
 // ---------------------------------------------------------------------------------------
-// k_ret: G^R(n, j), j = n-k-1 .. 0 (dyson_impl :158-213), blocked left-looking:
-//   qq(j) = h sum_{m=j+1}^{n} w(n-j, n-m) G(n,m) Sigma(m,j) - sum_{p=1}^{k+1} (i/h) bd(p) G(n, j+p)
-//   G(n,j) = qq(j) Minv_ret[j]
-// Blocks of JB consecutive j: phase A sums all m above the block (CTA-parallel), phase B
-// finishes the block sequentially on warp 0.
-// ---------------------------------------------------------------------------------------
-template <int S> struct RetCfg {
-    static constexpr int JB = (S == 1) ? 32 : (S == 2 ? 32 : (256 / (S * S) > 1 ? 256 / (S * S) : 1));
-    static constexpr int E = JB * S * S;               // entries of one block
-    static constexpr int GM = (256 / E) > 0 ? 256 / E : 1;  // m-groups in phase A
-};
-
-template <int S>
-__global__ void __launch_bounds__(256) k_ret(GroupDev g, const ProbDev *__restrict__ probs, int n) {
-    extern __shared__ double2 smem[];
-    const ProbDev p = probs[blockIdx.x];
-    const int k = g.k, s2 = S * S;
-    const double h = g.h;
-    constexpr int JB = RetCfg<S>::JB, E = RetCfg<S>::E, GM = RetCfg<S>::GM;
-    double2 *grow = p.gret + tri(n) * s2;  // G(n, 0..n)
-    // zero the row, G(n,n) = -i
-    for (long e = threadIdx.x; e < (long)(n + 1) * s2; e += blockDim.x) {
-        int ab = (int)(e % s2);
-        grow[e] = (e / s2 == n && (ab / S == ab % S)) ? cmk(0.0, -1.0) : cmk(0, 0);
-    }
-    __syncthreads();
-    ret_start_block<S>(g, p, n, smem);
-    double2 *part = smem;            // GM * E partial sums
-    double2 *acc = part + GM * E;    // E block sums
-    double2 *qv = acc + E;           // s2 scratch for phase B
-    const int tid = threadIdx.x;
-    for (int jhi = n - k - 1; jhi >= 0; jhi -= JB) {
-        const int jlo = jhi - JB + 1 < 0 ? 0 : jhi - JB + 1;
-        const int nb = jhi - jlo + 1;
-        // ---- phase A: acc(j) = sum_{m=jhi+1}^{n} w(n-j,n-m) G(n,m) Sigma(m,j)
-        if (tid < GM * E) {
-            const int gi = tid / E, e = tid % E;
-            const int jj = e / s2, ad = e % s2, a = ad / S, d = ad % S;
-            double2 sum = cmk(0, 0);
-            if (jj < nb) {
-                const int j = jhi - jj;
-                for (int m = jhi + 1 + gi; m <= n; m += GM) {
-                    const double2 *gm = grow + (long)m * s2 + a * S;
-                    const double2 *sm = g.sret + (tri(m) + j) * s2 + d;
-                    double2 t = cmk(0, 0);
-#pragma unroll
-                    for (int b = 0; b < S; b++) t = cfma(gm[b], sm[b * S], t);
-                    sum = cfma(cmk(greg_w(k, n - j, n - m), 0.0), t, sum);
-                }
-            }
-            part[gi * E + e] = sum;
-        }
-        __syncthreads();
-        for (int e = tid; e < E; e += blockDim.x) {
-            double2 s = part[e];
-            for (int gi = 1; gi < GM; gi++) s = cadd(s, part[gi * E + e]);
-            acc[e] = s;
-        }
-        __syncthreads();
-        // ---- phase B: sequential within the block (warp 0)
-        if (tid < 32) {
-            const int lane = tid;
-            for (int jj = 0; jj < nb; jj++) {
-                const int j = jhi - jj;
-                for (int ad = lane; ad < s2; ad += 32) {
-                    const int a = ad / S, d = ad % S;
-                    double2 sum = acc[jj * s2 + ad];
-                    for (int m = j + 1; m <= jhi; m++) {
-                        const double2 *gm = grow + (long)m * s2 + a * S;
-                        const double2 *sm = g.sret + (tri(m) + j) * s2 + d;
-                        double2 t = cmk(0, 0);
-                        for (int b = 0; b < S; b++) t = cfma(gm[b], sm[b * S], t);
-                        sum = cfma(cmk(greg_w(k, n - j, n - m), 0.0), t, sum);
-                    }
-                    double2 q = cscale(sum, h);
-                    for (int pp = 1; pp <= k + 1; pp++)
-                        q = csub(q, cmul(cmk(0.0, bd_w(k, pp) / h), grow[(long)(j + pp) * s2 + ad]));
-                    qv[ad] = q;
-                }
-                __syncwarp();
-                for (int ad = lane; ad < s2; ad += 32) {
-                    const int a = ad / S, d = ad % S;
-                    const double2 *mi = p.minv_ret + (long)j * s2;
-                    double2 x = cmk(0, 0);
-                    for (int b = 0; b < S; b++) x = cfma(qv[a * S + b], mi[b * S + d], x);
-                    grow[(long)j * s2 + ad] = x;
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------------------
 // k_tv: G^tv(n, tau) for one problem and a tile of tau (dyson_impl :651-741):
 //   Q(tau) = sum_{j<n} a_j G^tv(j,tau) + dtau * matsubara_integral_2(Sigma^tv(n,.), G^mat)(tau)
 //   G^tv(n,tau) = Minv_les[n] Q(tau)
+// The Matsubara integral is linear in G^mat with an operator K_n built from Sigma^tv(n,.)
+// alone (k_mat_operator), so for a group sharing Sigma it is one GEMM over all problems
+// (Cmat = K_n Gmat_all); this kernel streams the history and adds Cmat.
 // Thread per (tau, column d); the history G^tv(0..n-1, tile) is streamed once.
 // ---------------------------------------------------------------------------------------
-template <int S>
-__device__ __forceinline__ void acc_col(double2 *acc, const double2 *A, const double2 *B, int d, double w) {
-    // acc[a] += w * sum_b A[a][b] B[b][d]
+// k_tv works on the device layout of G^tv: element planes, (t*s^2 + e)*(ntau+1) + tau, so a
+// warp reading 32 consecutive tau of one plane issues one contiguous 512-byte access.
+template <int S> struct TvCfg {
+    static constexpr int DCH = S <= 2 ? S : (S <= 4 ? 2 : 1);  // block columns per pass
+    static constexpr int NW = 8;                // warps per CTA, splitting the history sum over j
+};
+
+// MIXED: history rows j < n-k-1 are read from the FP32 copy (half the bytes); the k+1 rows
+// that carry the backward-difference terms, and all sums, stay in FP64.
+template <int S, bool MIXED>
+__global__ void __launch_bounds__(256) k_tv(GroupDev g, const ProbDev *__restrict__ probs, int n) {
+    constexpr int s2 = S * S, DCH = TvCfg<S>::DCH, NW = TvCfg<S>::NW;
+    __shared__ double2 red[NW * 32 * S * DCH];
+    const ProbDev p = probs[blockIdx.y];
+    const int ntau = g.ntau, M = ntau + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tau = blockIdx.x * 32 + lane;
+    const bool live = tau <= ntau;
+    const long rowstride = (long)s2 * M;
+    for (int c0 = 0; c0 < S; c0 += DCH) {
+        double2 acc[S][DCH];
 #pragma unroll
-    for (int a = 0; a < S; a++) {
-        double2 t = cmk(0, 0);
+        for (int a = 0; a < S; a++)
 #pragma unroll
-        for (int b = 0; b < S; b++) t = cfma(A[a * S + b], B[b * S + d], t);
-        acc[a] = cfma(cmk(w, 0.0), t, acc[a]);
+            for (int c = 0; c < DCH; c++) acc[a][c] = cmk(0, 0);
+        if (live) {
+            const double2 *gb = p.gtv + tau;
+            const double2 *cf = g.tvcoef;
+            const int j64 = MIXED ? (n - g.k - 1 > 0 ? n - g.k - 1 : 0) : 0;  // first FP64 row
+            if (MIXED) {
+                const float2 *gb32 = p.gtv32 + tau;
+#pragma unroll 4
+                for (int j = warp; j < j64; j += NW) {
+                    const float2 *gj = gb32 + (long)j * rowstride;
+                    double2 bv[S][DCH];
+#pragma unroll
+                    for (int b = 0; b < S; b++)
+#pragma unroll
+                        for (int c = 0; c < DCH; c++) {
+                            float2 f = (c0 + c < S) ? __ldg(gj + (long)(b * S + c0 + c) * M) : make_float2(0.f, 0.f);
+                            bv[b][c] = cmk((double)f.x, (double)f.y);
+                        }
+                    const double2 *cj = cf + (long)j * s2;
+#pragma unroll
+                    for (int a = 0; a < S; a++)
+#pragma unroll
+                        for (int b = 0; b < S; b++) {
+                            const double2 cab = __ldg(cj + a * S + b);
+#pragma unroll
+                            for (int c = 0; c < DCH; c++) acc[a][c] = cfma(cab, bv[b][c], acc[a][c]);
+                        }
+                }
+            }
+            const int jfirst = j64 + ((warp - j64 % NW) + NW) % NW;  // keep j = warp (mod NW)
+#pragma unroll 4
+            for (int j = jfirst; j < n; j += NW) {
+                const double2 *gj = gb + (long)j * rowstride;
+                double2 bv[S][DCH];
+#pragma unroll
+                for (int b = 0; b < S; b++)
+#pragma unroll
+                    for (int c = 0; c < DCH; c++)
+                        bv[b][c] = (c0 + c < S) ? __ldg(gj + (long)(b * S + c0 + c) * M) : cmk(0, 0);
+                const double2 *cj = cf + (long)j * s2;
+#pragma unroll
+                for (int a = 0; a < S; a++)
+#pragma unroll
+                    for (int b = 0; b < S; b++) {
+                        const double2 cab = __ldg(cj + a * S + b);
+#pragma unroll
+                        for (int c = 0; c < DCH; c++) acc[a][c] = cfma(cab, bv[b][c], acc[a][c]);
+                    }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < S; a++)
+#pragma unroll
+            for (int c = 0; c < DCH; c++) red[((warp * 32 + lane) * S + a) * DCH + c] = acc[a][c];
+        __syncthreads();
+        if (warp == 0 && live) {
+#pragma unroll
+            for (int a = 0; a < S; a++)
+#pragma unroll
+                for (int c = 0; c < DCH; c++) {
+                    double2 v = red[(lane * S + a) * DCH + c];
+                    for (int w = 1; w < NW; w++) v = cadd(v, red[((w * 32 + lane) * S + a) * DCH + c]);
+                    acc[a][c] = v;
+                }
+            // Matsubara part dtau*[c2 + sig c1] from the group GEMM (k_mat_operator)
+            const double2 *cm = g.Cmat + (long)tau * S * g.ldc + (long)p.col * S + c0;
+#pragma unroll
+            for (int a = 0; a < S; a++)
+#pragma unroll
+                for (int c = 0; c < DCH; c++)
+                    if (c0 + c < S) acc[a][c] = cadd(acc[a][c], cm[(long)a * g.ldc + c]);
+            // solve: G^tv(n,tau)[a][d] = sum_b Minv[a][b] Q[b][d]
+            const double2 *mi = p.minv_les + (long)n * s2;
+            double2 *out = p.gtv + (long)n * rowstride + tau;
+#pragma unroll
+            for (int a = 0; a < S; a++)
+#pragma unroll
+                for (int c = 0; c < DCH; c++) {
+                    if (c0 + c >= S) continue;
+                    double2 x = cmk(0, 0);
+#pragma unroll
+                    for (int b = 0; b < S; b++) x = cfma(mi[a * S + b], acc[b][c], x);
+                    out[(long)(a * S + c0 + c) * M] = x;
+                    if (MIXED) p.gtv32[(long)n * rowstride + tau + (long)(a * S + c0 + c) * M] =
+                        make_float2((float)x.x, (float)x.y);
+                }
+        }
+        __syncthreads();
     }
 }
 
-template <int S, int TT>
-__global__ void __launch_bounds__(TT * S) k_tv(GroupDev g, const ProbDev *__restrict__ probs, int n) {
-    constexpr int s2 = S * S, CH = (s2 <= 32) ? 64 : 2048 / s2;  // coefficient chunk (j) staged in shared memory
-    __shared__ double2 coef[CH * s2];
-    const ProbDev p = probs[blockIdx.y];
-    const int k = g.k, ntau = g.ntau, M = ntau + 1;
-    const int tl = threadIdx.x / S, d = threadIdx.x % S;
-    const int tau = blockIdx.x * TT + tl;
-    const bool live = tau <= ntau;
-    double2 acc[S];
-#pragma unroll
-    for (int a = 0; a < S; a++) acc[a] = cmk(0, 0);
-    // history: j = 0..n-1 (G^tv(n,.) itself is zero at this point in the reference)
-    for (int j0 = 0; j0 < n; j0 += CH) {
-        const int nj = n - j0 < CH ? n - j0 : CH;
-        __syncthreads();
-        for (int e = threadIdx.x; e < nj * s2; e += blockDim.x) coef[e] = g.tvcoef[(long)j0 * s2 + e];
-        __syncthreads();
-        if (live) {
-            const double2 *gcol = p.gtv + ((long)j0 * M + tau) * s2 + d;
-#pragma unroll 4
-            for (int jj = 0; jj < nj; jj++) {
-                const double2 *gj = gcol + (long)jj * M * s2;
-                double2 bv[S];
-#pragma unroll
-                for (int b = 0; b < S; b++) bv[b] = __ldg(gj + b * S);
-#pragma unroll
-                for (int a = 0; a < S; a++) {
-                    double2 t = acc[a];
-#pragma unroll
-                    for (int b = 0; b < S; b++) t = cfma(coef[jj * s2 + a * S + b], bv[b], t);
-                    acc[a] = t;
-                }
-            }
-        }
+// k_tv_to32: FP32 copy of G^tv rows [t0, t0+rows) (plane layout, same indexing)
+__global__ void k_tv_to32(float2 *__restrict__ dst, const double2 *__restrict__ src, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        dst[i] = make_float2((float)src[i].x, (float)src[i].y);
+}
+
+// k_tv_relayout: G^tv between libcntr's layout ((t*M + tau)*s^2 + e) and the element-plane
+// layout ((t*s^2 + e)*M + tau) used on the device; rows t = 0..rows-1.
+__global__ void k_tv_relayout(double2 *__restrict__ dst, const double2 *__restrict__ src, long rows, int M, int s2,
+                              int to_planes) {
+    const long total = rows * M * s2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        // i indexes the plane layout: t, e, tau
+        const long t = i / ((long)s2 * M);
+        const int rem = (int)(i % ((long)s2 * M)), e = rem / M, tau = rem % M;
+        const long j = (t * M + tau) * s2 + e;  // libcntr index
+        if (to_planes) dst[i] = src[j]; else dst[j] = src[i];
     }
-    if (!live) return;
-    // Matsubara part: dtau * [c2 + sig c1] (conv_impl :410-540), A = Sigma^tv(n,.), B = G^mat
+}
+
+// ---------------------------------------------------------------------------------------
+// k_mat_operator: K_n[(m,a),(x,c)] such that dtau * matsubara_integral_2(Sigma^tv(n,.), B)(m)
+// = sum_x K_n[m,x] B(x) for every B (conv_impl :410-540 read as a linear map of B):
+//   c2 = sum_{l=0}^{r} w(r,l) A(m+l) B(l)           (r = ntau-m >= k; rcorr for 0<r<k)
+//   c1 = sum_{l=0}^{m} w(m,l) A(m-l) B(ntau-l)      (m >= k; rcorr for 0<m<k),  C = c2 + sig c1
+// ---------------------------------------------------------------------------------------
+template <int S>
+__global__ void k_mat_operator(GroupDev g, int n) {
+    const int k = g.k, s2 = S * S, ntau = g.ntau, M = ntau + 1;
+    const long KS = (long)M * S;
     const double2 *A = g.stv + (long)n * M * s2;
-    const double2 *B = p.gmat;
-    const int m = tau;
-    double2 c1[S], c2[S];
-#pragma unroll
-    for (int a = 0; a < S; a++) { c1[a] = cmk(0, 0); c2[a] = cmk(0, 0); }
-    if (m == 0) {
-    } else if (m < k) {
-        for (int j = 0; j <= k; j++)
-            for (int l = 0; l <= k; l++)
-                acc_col<S>(c1, A + (long)j * s2, B + (long)(ntau - l) * s2, d, rcorr_w(k, m, l, j));
-    } else {
-        for (int l = 0; l <= m; l++)
-            acc_col<S>(c1, A + (long)(m - l) * s2, B + (long)(ntau - l) * s2, d, greg_w(k, m, l));
-    }
-    const int r = ntau - m;
-    if (r == 0) {
-    } else if (r < k) {
-        for (int l = 0; l <= k; l++)
-            for (int j = 0; j <= k; j++)
-                acc_col<S>(c2, A + (long)(ntau - l) * s2, B + (long)j * s2, d, rcorr_w(k, r, l, j));
-    } else {
-        for (int l = 0; l <= r; l++)
-            acc_col<S>(c2, A + (long)(m + l) * s2, B + (long)l * s2, d, greg_w(k, r, l));
-    }
     const double dtau = g.beta / ntau, sg = (double)g.sig;
-    double2 q[S];
-#pragma unroll
-    for (int a = 0; a < S; a++) q[a] = cadd(acc[a], cscale(cadd(c2[a], cscale(c1[a], sg)), dtau));
-    // solve: G^tv(n,tau)[a][d] = sum_b Minv[a][b] Q[b][d]
-    const double2 *mi = p.minv_les + (long)n * s2;
-    double2 *out = p.gtv + ((long)n * M + tau) * s2;
-#pragma unroll
-    for (int a = 0; a < S; a++) {
-        double2 x = cmk(0, 0);
-#pragma unroll
-        for (int b = 0; b < S; b++) x = cfma(mi[a * S + b], q[b], x);
-        out[a * S + d] = x;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < (long)M * M * s2; e += (long)gridDim.x * blockDim.x) {
+        const int m = (int)(e / ((long)M * s2));
+        const int rem = (int)(e % ((long)M * s2));
+        const int x = rem / s2, ac = rem % s2, a = ac / S, c = ac % S;
+        const int r = ntau - m;
+        double2 v = cmk(0, 0);
+        if (r >= k) {
+            if (x <= r) v = cfma(cmk(greg_w(k, r, x), 0), A[(long)(m + x) * s2 + ac], v);
+        } else if (r > 0 && x <= k) {
+            for (int l = 0; l <= k; l++) v = cfma(cmk(rcorr_w(k, r, l, x), 0), A[(long)(ntau - l) * s2 + ac], v);
+        }
+        const int l = ntau - x;
+        if (m >= k) {
+            if (l >= 0 && l <= m) v = cfma(cmk(sg * greg_w(k, m, l), 0), A[(long)(m - l) * s2 + ac], v);
+        } else if (m > 0 && l >= 0 && l <= k) {
+            for (int jj = 0; jj <= k; jj++) v = cfma(cmk(sg * rcorr_w(k, m, l, jj), 0), A[(long)jj * s2 + ac], v);
+        }
+        g.Kmat[((long)m * S + a) * KS + (long)x * S + c] = cscale(v, dtau);
+    }
+}
+
+// k_gmat_stack: Gmat_all[(x,c)][(col,d)] = G^mat_col(x)[c][d]
+template <int S>
+__global__ void k_gmat_stack(GroupDev g, const ProbDev *__restrict__ probs) {
+    const ProbDev p = probs[blockIdx.y];
+    const int s2 = S * S, M = g.ntau + 1;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < M * s2; e += gridDim.x * blockDim.x) {
+        const int x = e / s2, cd = e % s2, c = cd / S, d = cd % S;
+        g.Gmat_all[((long)x * S + c) * g.ldc + (long)p.col * S + d] = p.gmat[e];
     }
 }
 
@@ -444,21 +444,22 @@ __global__ void __launch_bounds__(TT * S) k_tv(GroupDev g, const ProbDev *__rest
 //   btv [(m,c)][(col,d)] = w(ntau,m) (-i dtau)(-sig) G^tv(n,ntau-m)^dagger[c][d]
 // ---------------------------------------------------------------------------------------
 template <int S>
-__global__ void k_les_operands(GroupDev g, const ProbDev *__restrict__ probs, int n) {
+__global__ void k_les_operands(GroupDev g, const ProbDev *__restrict__ probs, int n, int which) {
     const ProbDev p = probs[blockIdx.y];
     const int k = g.k, s2 = S * S, ntau = g.ntau;
     const double h = g.h, dtau = g.beta / ntau;
     const long ldc = g.ldc;
-    const int rows = (n + 1) + (ntau + 1);
-    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < (long)rows * s2; e += (long)gridDim.x * blockDim.x) {
-        int r = (int)(e / s2), cd = (int)(e % s2), c = cd / S, d = cd % S;
+    // which: 1 = badv rows only, 2 = btv rows only, 3 = both
+    const int r0 = (which & 1) ? 0 : n + 1, r1 = (which & 2) ? (n + 1) + (ntau + 1) : n + 1;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < (long)(r1 - r0) * s2; e += (long)gridDim.x * blockDim.x) {
+        int r = r0 + (int)(e / s2), cd = (int)(e % s2), c = cd / S, d = cd % S;
         if (r <= n) {
             const int m = r;
             double2 v = cconj(p.gret[(tri(n) + m) * s2 + d * S + c]);
             g.badv[((long)m * S + c) * ldc + (long)p.col * S + d] = cscale(v, h * greg_w(k, n, m));
         } else {
             const int m = r - (n + 1);
-            double2 v = cconj(p.gtv[((long)n * (ntau + 1) + (ntau - m)) * s2 + d * S + c]);
+            double2 v = cconj(p.gtv[((long)n * s2 + d * S + c) * (ntau + 1) + (ntau - m)]);
             // (-i dtau)(-sig) v * w
             double2 f = cmk(0.0, dtau * (double)g.sig * greg_w(k, ntau, m));
             g.btv[((long)m * S + c) * ldc + (long)p.col * S + d] = cmul(f, v);
@@ -466,119 +467,4 @@ __global__ void k_les_operands(GroupDev g, const ProbDev *__restrict__ probs, in
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// k_les: G^<(j, n), j = 0..n (dyson_impl :893-1056):
-//   x_0 = -G^tv(n,0)^dagger; x_1..x_k from the k-block start system;
-//   qq(j) = gles(j) - sum_{p=1}^{k+1} (i/h) bd(p) x_{j-p} + h sum_{m<j} w(j,m) Sigma^R(j,m) x_m
-//   x_j = Minv_les[j] qq(j)
-// Blocked left-looking as k_ret; phase A rows are Sigma^R(j, 0..jlo-1) (contiguous).
-// ---------------------------------------------------------------------------------------
-template <int S>
-__global__ void __launch_bounds__(256) k_les(GroupDev g, const ProbDev *__restrict__ probs, int n) {
-    extern __shared__ double2 smem[];
-    const ProbDev p = probs[blockIdx.x];
-    const int k = g.k, s2 = S * S, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const double h = g.h;
-    const long ldc = g.ldc;
-    constexpr int JB = RetCfg<S>::JB;
-    const double2 *gl = g.gles + (long)p.col * S;   // gles(j)[a][d] at gl[(j*S+a)*ldc + d]
-    double2 *xcol = p.gles + tri(n) * s2;           // G^<(0..n, n)
-    // x_0
-    for (int ad = tid; ad < s2; ad += blockDim.x) {
-        int a = ad / S, d = ad % S;
-        xcol[ad] = cneg(cconj(p.gtv[((long)n * (g.ntau + 1) + 0) * s2 + d * S + a]));
-    }
-    __syncthreads();
-    les_start_block<S>(g, p, n, gl, ldc, xcol, smem);
-    double2 *acc = smem;            // JB * s2
-    double2 *qv = acc + JB * s2;    // s2
-    const int nwarps = blockDim.x >> 5;
-    for (int jlo = k + 1; jlo <= n; jlo += JB) {
-        const int jhi = jlo + JB - 1 > n ? n : jlo + JB - 1;
-        const int nb = jhi - jlo + 1;
-        // ---- phase A: acc(j)[a][d] = sum_{m<jlo} w(j,m) Sigma^R(j,m)[a][b] x_m[b][d]
-        // warp per row j; lane = (m-group, d)
-        constexpr int LPG = S;                        // lanes per m-group
-        constexpr int NG = 32 / LPG;                  // m-groups per warp
-        for (int jj = warp; jj < nb; jj += nwarps) {
-            const int j = jlo + jj;
-            const int mg = lane / LPG, dd = lane % LPG;
-            double2 a_[S];
-#pragma unroll
-            for (int a = 0; a < S; a++) a_[a] = cmk(0, 0);
-            if (mg < NG) {
-                const double2 *srow = g.sret + tri(j) * s2;
-                for (int m = mg; m < jlo; m += NG) {
-                    const double w = greg_w(k, j, m);
-                    const double2 *sm = srow + (long)m * s2;
-                    const double2 *xm = xcol + (long)m * s2;
-#pragma unroll
-                    for (int a = 0; a < S; a++) {
-                        double2 t = cmk(0, 0);
-#pragma unroll
-                        for (int b = 0; b < S; b++) t = cfma(sm[a * S + b], xm[b * S + dd], t);
-                        a_[a] = cfma(cmk(w, 0.0), t, a_[a]);
-                    }
-                }
-            }
-            // reduce over m-groups (lanes with equal dd)
-            if constexpr ((S & (S - 1)) == 0) {
-#pragma unroll
-                for (int a = 0; a < S; a++) {
-                    double2 v = a_[a];
-                    for (int off = LPG; off < 32; off <<= 1) {
-                        v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
-                        v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
-                    }
-                    a_[a] = v;
-                }
-                if (mg == 0)
-                    for (int a = 0; a < S; a++) acc[jj * s2 + a * S + dd] = a_[a];
-            } else {
-                double2 *red = qv + s2 + warp * 32 * S;
-                for (int a = 0; a < S; a++) red[lane * S + a] = (mg < NG) ? a_[a] : cmk(0, 0);
-                __syncwarp();
-                if (lane < S) {
-                    for (int a = 0; a < S; a++) {
-                        double2 v = cmk(0, 0);
-                        for (int g2 = 0; g2 < NG; g2++) v = cadd(v, red[(g2 * S + lane) * S + a]);
-                        acc[jj * s2 + a * S + lane] = v;
-                    }
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        // ---- phase B on warp 0
-        if (tid < 32) {
-            for (int jj = 0; jj < nb; jj++) {
-                const int j = jlo + jj;
-                for (int ad = lane; ad < s2; ad += 32) {
-                    const int a = ad / S, d = ad % S;
-                    double2 sum = acc[jj * s2 + ad];
-                    const double2 *srow = g.sret + tri(j) * s2;
-                    for (int m = jlo; m < j; m++) {
-                        double2 t = cmk(0, 0);
-                        for (int b = 0; b < S; b++) t = cfma(srow[(long)m * s2 + a * S + b], xcol[(long)m * s2 + b * S + d], t);
-                        sum = cfma(cmk(greg_w(k, j, m), 0.0), t, sum);
-                    }
-                    double2 q = gl[((long)j * S + a) * ldc + d];
-                    for (int pp = 1; pp <= k + 1; pp++)
-                        q = csub(q, cmul(cmk(0.0, bd_w(k, pp) / h), xcol[(long)(j - pp) * s2 + ad]));
-                    q = cfma(cmk(h, 0.0), sum, q);
-                    qv[ad] = q;
-                }
-                __syncwarp();
-                for (int ad = lane; ad < s2; ad += 32) {
-                    const int a = ad / S, d = ad % S;
-                    const double2 *mi = p.minv_les + (long)j * s2;
-                    double2 x = cmk(0, 0);
-                    for (int b = 0; b < S; b++) x = cfma(mi[a * S + b], qv[b * S + d], x);
-                    xcol[(long)j * s2 + ad] = x;
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-    }
-}
+#include "kernels_volterra.cuh"

@@ -77,6 +77,7 @@ struct Prob {
     int group = -1;
     double2 *gret = nullptr, *gles = nullptr, *gtv = nullptr, *gmat = nullptr;
     double2 *H = nullptr, *minv_ret = nullptr, *minv_les = nullptr;
+    float2 *gtv32 = nullptr;
 };
 
 struct Group {
@@ -86,8 +87,10 @@ struct Group {
     double2 *sret = nullptr, *sles = nullptr, *stv = nullptr, *smat = nullptr;
     double2 *Ldense = nullptr, *Tdense = nullptr, *tvcoef = nullptr;
     double2 *badv = nullptr, *btv = nullptr, *gles = nullptr;
+    double2 *Kmat = nullptr, *Gmat_all = nullptr, *Cmat = nullptr;
     int ldc = 0;
     int dense_valid = -1, ret_valid = -1, les_valid = -1;
+    bool gmat_valid = false;
     std::vector<int> members;        // problem indices, nt descending
     std::vector<ProbDev> h_probs;    // same order; col = position
     ProbDev *d_probs = nullptr;
@@ -95,15 +98,47 @@ struct Group {
 
 }  // namespace
 
+// Per-kernel timing with CUDA events on the batch stream (enabled by nessi_gpu_set_profiling).
+struct KProf {
+    std::vector<cudaEvent_t> ev;
+    int used = 0;
+    long launches = 0;
+    double bytes = 0;  // algorithmic bytes of the recorded launches
+};
+
 struct nessi_batch {
     int device = 0;
+    bool prof = false;
+    KProf kp[NESSI_KERNEL_COUNT];
     int precision = NESSI_PREC_FP64;
     cudaStream_t stream = nullptr;
-    cublasHandle_t cublas = nullptr;
+    cudaStream_t side = nullptr;       // runs the retarded component concurrently with tv
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool own_stream = true;
+    cublasHandle_t cublas = nullptr, cublas_side = nullptr;
     std::vector<Prob> probs;
     std::vector<Group> groups;
     std::vector<void *> allocs;
     long long bytes = 0;
+    double2 *scratch = nullptr;  // G^tv in libcntr layout during layout conversion (size1 > 1)
+    long scratch_n = 0;
+
+    void prof_mark(int id, cudaStream_t st = nullptr) {
+        if (!prof) return;
+        KProf &k = kp[id];
+        if (k.used == (int)k.ev.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            k.ev.push_back(e);
+        }
+        cudaEventRecord(k.ev[k.used++], st ? st : stream);
+    }
+    void prof_end(int id, double bytes, cudaStream_t st = nullptr) {
+        if (!prof) return;
+        prof_mark(id, st);
+        kp[id].launches++;
+        kp[id].bytes += bytes;
+    }
 
     int alloc(double2 **p, long long n_cplx) {
         if (n_cplx <= 0) { *p = nullptr; return NESSI_OK; }
@@ -129,6 +164,7 @@ GroupDev group_dev(const Group &g) {
     d.sret = g.sret; d.sles = g.sles; d.stv = g.stv; d.smat = g.smat;
     d.Ldense = g.Ldense; d.Tdense = g.Tdense; d.tvcoef = g.tvcoef;
     d.badv = g.badv; d.btv = g.btv; d.gles = g.gles;
+    d.Kmat = g.Kmat; d.Gmat_all = g.Gmat_all; d.Cmat = g.Cmat;
     d.ntmax = g.ntmax; d.ntau = g.ntau; d.s = g.s; d.sig = g.sig; d.k = g.k;
     d.ldc = g.ldc; d.h = g.h; d.beta = g.beta;
     return d;
@@ -155,12 +191,12 @@ int find_group(nessi_batch *b, int user_id) {
 // ---- per-size kernel launch table ----------------------------------------------------
 template <int S> size_t ret_smem(int k) {
     size_t start = (size_t)(k * k * S * S + k * S * S + (k * S) * (k * S) + k * S * S) * 16 + 16;
-    size_t phase = (size_t)(RetCfg<S>::GM * RetCfg<S>::E + RetCfg<S>::E + S * S) * 16;
+    size_t phase = (size_t)VolLayout<S>::total * 16;
     return std::max(start, phase);
 }
 template <int S> size_t les_smem(int k) {
     size_t start = (size_t)((k * S) * (k * S) + k * S * S) * 16 + 16;
-    size_t phase = (size_t)(RetCfg<S>::JB * S * S + S * S + 8 * 32 * S) * 16;
+    size_t phase = (size_t)VolLayout<S>::total * 16;
     return std::max(start, phase);
 }
 
@@ -171,6 +207,7 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     // step-matrix inverses
     int les_lo = std::min(n, std::max(k + 1, g.les_valid + 1));
     int r0 = g.ret_valid + 1, r1 = n - k - 1;
+    b->prof_mark(NESSI_KERNEL_PREP);
     k_prep_problem<S><<<nact, 64, 0, st>>>(gd, g.d_probs, n, les_lo, r0, r1);
     CK(cudaGetLastError());
     g.les_valid = n - 1;
@@ -181,45 +218,95 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
         int blocks = (int)std::min<long>(std::max<long>(1, (work + 255) / 256), 1184);
         k_prep_group<S><<<blocks, 256, 0, st>>>(gd, n, d_lo);
         CK(cudaGetLastError());
+        b->prof_end(NESSI_KERNEL_PREP, 0.0);
         g.dense_valid = n - 1;
     }
-    // retarded row
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    // Matsubara part of the tv row: Cmat = K_n Gmat_all (one GEMM for the group)
+    {
+        const long M = g.ntau + 1;
+        if (!g.gmat_valid) {
+            dim3 grid((unsigned)((M * S * S + 255) / 256), (unsigned)g.members.size());
+            k_gmat_stack<S><<<grid, 256, 0, st>>>(gd, g.d_probs);
+            CK(cudaGetLastError());
+            g.gmat_valid = true;
+        }
+        b->prof_mark(NESSI_KERNEL_MATOP);
+        long work = M * M * S * S;
+        k_mat_operator<S><<<(unsigned)std::min<long>((work + 255) / 256, 4736), 256, 0, st>>>(gd, n);
+        CK(cudaGetLastError());
+        b->prof_end(NESSI_KERNEL_MATOP, 16.0 * (double)work + 16.0 * M * S * S);
+        b->prof_mark(NESSI_KERNEL_GEMM);
+        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, nact * S, (int)(M * S), (int)(M * S), &one,
+                        (const cuDoubleComplex *)g.Gmat_all, g.ldc, (const cuDoubleComplex *)g.Kmat, (int)(M * S),
+                        &zero, (cuDoubleComplex *)g.Cmat, g.ldc));
+        b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)nact * S * (M * S) * (M * S));
+    }
+    const int m = nact * S, nn = (n + 1) * S;
+    const long ldL = (long)(g.ntmax + 1) * S, ldT = (long)(g.ntau + 1) * S;
+    // side stream: retarded row, then les*adv = Ldense * badv (needs only G^R(n, .))
+    CK(cudaEventRecord(b->ev_fork, st));
+    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     {
         size_t sm = ret_smem<S>(k);
         CK(cudaFuncSetAttribute(k_ret<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_ret<S><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+        b->prof_mark(NESSI_KERNEL_RET, b->side);
+        k_ret<S><<<nact, 256, sm, b->side>>>(gd, g.d_probs, n);
         CK(cudaGetLastError());
-    }
-    // tv row
-    {
-        constexpr int TT = 128 / S;
-        dim3 grid((g.ntau + 1 + TT - 1) / TT, nact);
-        k_tv<S, TT><<<grid, TT * S, 0, st>>>(gd, g.d_probs, n);
-        CK(cudaGetLastError());
-    }
-    // Sigma-shared convolutions tv*vt + les*adv for all active problems
-    {
-        long rows = (long)(n + 1 + g.ntau + 1) * S * S;
+        // G^R row n written; Sigma^R triangle rows <= n read (shared by the group)
+        b->prof_end(NESSI_KERNEL_RET, 16.0 * S * S * ((double)nact * (n + 1) + tri_h(n + 1)), b->side);
+        long rows = (long)(n + 1) * S * S;
         dim3 grid((unsigned)std::min<long>((rows + 255) / 256, 64), nact);
-        k_les_operands<S><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+        b->prof_mark(NESSI_KERNEL_LES_OPERANDS, b->side);
+        k_les_operands<S><<<grid, 256, 0, b->side>>>(gd, g.d_probs, n, 1);
         CK(cudaGetLastError());
-        const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-        const int m = nact * S, nn = (n + 1) * S;
-        const long ldL = (long)(g.ntmax + 1) * S, ldT = (long)(g.ntau + 1) * S;
-        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (n + 1) * S, &one,
+        b->prof_end(NESSI_KERNEL_LES_OPERANDS, 32.0 * S * S * (double)nact * (n + 1), b->side);
+        b->prof_mark(NESSI_KERNEL_GEMM, b->side);
+        CKB(cublasZgemm(b->cublas_side, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (n + 1) * S, &one,
                         (const cuDoubleComplex *)g.badv, g.ldc, (const cuDoubleComplex *)g.Ldense, (int)ldL, &zero,
                         (cuDoubleComplex *)g.gles, g.ldc));
+        b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)m * nn * ((n + 1) * S), b->side);
+    }
+    CK(cudaEventRecord(b->ev_join, b->side));
+    // main stream: tv row, then the tv*vt operand
+    {
+        dim3 grid((g.ntau + 1 + 31) / 32, nact);
+        b->prof_mark(NESSI_KERNEL_TV);
+        const bool mixed = b->precision == NESSI_PREC_MIXED;
+        if (mixed) k_tv<S, true><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+        else k_tv<S, false><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+        CK(cudaGetLastError());
+        // per problem: G^tv history rows 0..n-1 read (FP32 below the k+1 BDF rows when mixed),
+        // row n written, Cmat column read; shared: the n coefficient blocks
+        const double M = g.ntau + 1;
+        const double n32 = mixed ? std::max(0, n - k - 1) : 0, n64 = n - n32;
+        b->prof_end(NESSI_KERNEL_TV, S * S * ((double)nact * (8.0 * n32 * M + 16.0 * n64 * M + 32.0 * M +
+                                                                 (mixed ? 8.0 * M : 0.0)) + 16.0 * n));
+        long rows = (long)(g.ntau + 1) * S * S;
+        dim3 grid2((unsigned)std::min<long>((rows + 255) / 256, 64), nact);
+        b->prof_mark(NESSI_KERNEL_LES_OPERANDS);
+        k_les_operands<S><<<grid2, 256, 0, st>>>(gd, g.d_probs, n, 2);
+        CK(cudaGetLastError());
+        b->prof_end(NESSI_KERNEL_LES_OPERANDS, 32.0 * S * S * (double)nact * (g.ntau + 1));
+    }
+    CK(cudaStreamWaitEvent(st, b->ev_join, 0));
+    // tv*vt: gles += Sigma^tv * btv
+    {
+        b->prof_mark(NESSI_KERNEL_GEMM);
         const double2 *T = S == 1 ? g.stv : g.Tdense;
         CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (g.ntau + 1) * S, &one,
                         (const cuDoubleComplex *)g.btv, g.ldc, (const cuDoubleComplex *)T, (int)ldT, &one,
                         (cuDoubleComplex *)g.gles, g.ldc));
+        b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)m * nn * ((g.ntau + 1) * S));
     }
     // lesser column
     {
         size_t sm = les_smem<S>(k);
         CK(cudaFuncSetAttribute(k_les<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        b->prof_mark(NESSI_KERNEL_LES);
         k_les<S><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
         CK(cudaGetLastError());
+        b->prof_end(NESSI_KERNEL_LES, 16.0 * S * S * ((double)nact * 2.0 * (n + 1) + tri_h(n + 1)));
     }
     return NESSI_OK;
 }
@@ -280,9 +367,18 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
         set_err("stream creation failed");
         return fail(NESSI_ERR_CUDA);
     }
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        set_err("stream/event creation failed");
+        return fail(NESSI_ERR_CUDA);
+    }
     if (cublasCreate(&b->cublas) != CUBLAS_STATUS_SUCCESS) { set_err("cublasCreate failed"); return fail(NESSI_ERR_CUDA); }
     cublasSetStream(b->cublas, b->stream);
     cublasSetMathMode(b->cublas, CUBLAS_DEFAULT_MATH);
+    if (cublasCreate(&b->cublas_side) != CUBLAS_STATUS_SUCCESS) { set_err("cublasCreate failed"); return fail(NESSI_ERR_CUDA); }
+    cublasSetStream(b->cublas_side, b->side);
+    cublasSetMathMode(b->cublas_side, CUBLAS_DEFAULT_MATH);
     b->probs.resize(count);
     // groups
     for (int i = 0; i < count; i++) {
@@ -315,6 +411,22 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
             (r = b->alloc(&p.H, (nt + 2) * s2)) || (r = b->alloc(&p.minv_ret, (nt + 1) * s2)) ||
             (r = b->alloc(&p.minv_les, (nt + 1) * s2)))
             return fail(r);
+        if (precision == NESSI_PREC_MIXED) {
+            void *q = nullptr;
+            size_t nb_ = (size_t)(nt + 1) * M * s2 * sizeof(float2);
+            if (cudaMalloc(&q, nb_) != cudaSuccess) { set_err("cudaMalloc of %zu bytes failed", nb_); return fail(NESSI_ERR_OOM); }
+            b->allocs.push_back(q);
+            b->bytes += nb_;
+            p.gtv32 = (float2 *)q;
+        }
+    }
+    {
+        long need = 0;
+        for (const Prob &p : b->probs)
+            if (p.d.size1 > 1) need = std::max(need, (long)(p.d.nt + 1) * (p.d.ntau + 1) * p.d.size1 * p.d.size1);
+        int r;
+        if (need > 0 && (r = b->alloc(&b->scratch, need))) return fail(r);
+        b->scratch_n = need;
     }
     for (Group &g : b->groups) {
         std::stable_sort(g.members.begin(), g.members.end(),
@@ -326,13 +438,15 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
             (r = b->alloc(&g.stv, N * M * s2)) || (r = b->alloc(&g.smat, M * s2)) ||
             (r = b->alloc(&g.Ldense, N * S * N * S)) || (S > 1 && (r = b->alloc(&g.Tdense, N * S * M * S))) ||
             (r = b->alloc(&g.tvcoef, N * s2)) || (r = b->alloc(&g.badv, N * S * g.ldc)) ||
-            (r = b->alloc(&g.btv, M * S * g.ldc)) || (r = b->alloc(&g.gles, N * S * g.ldc)))
+            (r = b->alloc(&g.btv, M * S * g.ldc)) || (r = b->alloc(&g.gles, N * S * g.ldc)) ||
+            (r = b->alloc(&g.Kmat, M * S * M * S)) || (r = b->alloc(&g.Gmat_all, M * S * g.ldc)) ||
+            (r = b->alloc(&g.Cmat, M * S * g.ldc)))
             return fail(r);
         for (size_t c = 0; c < g.members.size(); c++) {
             const Prob &p = b->probs[g.members[c]];
             ProbDev pd;
             pd.gret = p.gret; pd.gles = p.gles; pd.gtv = p.gtv; pd.gmat = p.gmat;
-            pd.H = p.H; pd.minv_ret = p.minv_ret; pd.minv_les = p.minv_les;
+            pd.H = p.H; pd.minv_ret = p.minv_ret; pd.minv_les = p.minv_les; pd.gtv32 = p.gtv32;
             pd.mu = p.d.mu; pd.nt = p.d.nt; pd.col = (int)c; pd.pad = 0;
             g.h_probs.push_back(pd);
         }
@@ -356,8 +470,14 @@ int nessi_gpu_batch_destroy(nessi_batch *b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (void *q : b->allocs) cudaFree(q);
+    for (auto &k : b->kp)
+        for (cudaEvent_t e : k.ev) cudaEventDestroy(e);
     if (b->cublas) cublasDestroy(b->cublas);
-    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->cublas_side) cublasDestroy(b->cublas_side);
+    if (b->side) { cudaStreamSynchronize(b->side); cudaStreamDestroy(b->side); }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return NESSI_OK;
 }
@@ -374,15 +494,48 @@ static int copy_cplx(nessi_batch *b, void *dst, const void *src, long n_cplx, cu
     return NESSI_OK;
 }
 
+static int refresh32(nessi_batch *b, float2 *dst, const double2 *src, long n) {
+    if (!dst || n <= 0) return NESSI_OK;
+    k_tv_to32<<<(int)std::min<long>((n + 255) / 256, 4096), 256, 0, b->stream>>>(dst, src, n);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+// G^tv rows [t0, t0+rows) between a host buffer in libcntr layout and the device planes
+static int tv_transfer(nessi_batch *b, double2 *dev_planes, void *host, long t0, long rows, int M, int s,
+                       bool to_device) {
+    if (!host || rows <= 0) return NESSI_OK;
+    const long s2 = (long)s * s, n = rows * M * s2;
+    double2 *dev = dev_planes + t0 * M * s2;
+    if (s == 1) {
+        return to_device ? copy_cplx(b, dev, host, n, cudaMemcpyHostToDevice)
+                         : copy_cplx(b, host, dev, n, cudaMemcpyDeviceToHost);
+    }
+    if (n > b->scratch_n) { set_err("internal: scratch too small"); return NESSI_ERR_ARG; }
+    const int blocks = (int)std::min<long>((n + 255) / 256, 4096);
+    if (to_device) {
+        CKR(copy_cplx(b, b->scratch, host, n, cudaMemcpyHostToDevice));
+        k_tv_relayout<<<blocks, 256, 0, b->stream>>>(dev, b->scratch, rows, M, (int)s2, 1);
+        CK(cudaGetLastError());
+    } else {
+        k_tv_relayout<<<blocks, 256, 0, b->stream>>>(b->scratch, dev, rows, M, (int)s2, 0);
+        CK(cudaGetLastError());
+        CKR(copy_cplx(b, host, b->scratch, n, cudaMemcpyDeviceToHost));
+    }
+    return NESSI_OK;
+}
+
 int nessi_gpu_set_G(nessi_batch *b, int p, const void *ret, const void *les, const void *tv, const void *mat) {
     CKR(check_prob(b, p));
     Prob &q = b->probs[p];
     const long s2 = (long)q.d.size1 * q.d.size1, nt = q.d.nt, M = q.d.ntau + 1;
     CKR(copy_cplx(b, q.gret, ret, tri_h(nt + 1) * s2, cudaMemcpyHostToDevice));
     CKR(copy_cplx(b, q.gles, les, tri_h(nt + 1) * s2, cudaMemcpyHostToDevice));
-    CKR(copy_cplx(b, q.gtv, tv, (nt + 1) * M * s2, cudaMemcpyHostToDevice));
+    CKR(tv_transfer(b, q.gtv, (void *)tv, 0, nt + 1, (int)M, q.d.size1, true));
+    if (tv) CKR(refresh32(b, q.gtv32, q.gtv, (nt + 1) * M * s2));
     CKR(copy_cplx(b, q.gmat, mat, M * s2, cudaMemcpyHostToDevice));
     CK(cudaStreamSynchronize(b->stream));
+    if (mat) b->groups[q.group].gmat_valid = false;
     return NESSI_OK;
 }
 
@@ -392,14 +545,14 @@ int nessi_gpu_get_G(nessi_batch *b, int p, void *ret, void *les, void *tv, void 
     const long s2 = (long)q.d.size1 * q.d.size1, nt = q.d.nt, M = q.d.ntau + 1;
     CKR(copy_cplx(b, ret, q.gret, tri_h(nt + 1) * s2, cudaMemcpyDeviceToHost));
     CKR(copy_cplx(b, les, q.gles, tri_h(nt + 1) * s2, cudaMemcpyDeviceToHost));
-    CKR(copy_cplx(b, tv, q.gtv, (nt + 1) * M * s2, cudaMemcpyDeviceToHost));
+    CKR(tv_transfer(b, q.gtv, tv, 0, nt + 1, (int)M, q.d.size1, false));
     CKR(copy_cplx(b, mat, q.gmat, M * s2, cudaMemcpyDeviceToHost));
     CK(cudaStreamSynchronize(b->stream));
     return NESSI_OK;
 }
 
 static int slice_copy(nessi_batch *b, double2 *ret, double2 *tv, double2 *les, double2 *mat, int nt, int ntau, int s,
-                      int tstp, void *slice, bool to_device) {
+                      int tstp, void *slice, bool to_device, bool tv_planes) {
     const long s2 = (long)s * s, M = ntau + 1;
     if (tstp < -1 || tstp > nt) { set_err("time step %d out of range [-1, %d]", tstp, nt); return NESSI_ERR_ARG; }
     if (!slice) { set_err("null slice"); return NESSI_ERR_ARG; }
@@ -413,7 +566,8 @@ static int slice_copy(nessi_batch *b, double2 *ret, double2 *tv, double2 *les, d
     } else {
         const long n1 = tstp + 1;
         CKR(cp(ret + tri_h(tstp) * s2, h, n1 * s2));
-        CKR(cp(tv + tstp * M * s2, h + n1 * s2, M * s2));
+        if (tv_planes) CKR(tv_transfer(b, tv, h + n1 * s2, tstp, 1, (int)M, s, to_device));
+        else CKR(cp(tv + tstp * M * s2, h + n1 * s2, M * s2));
         CKR(cp(les + tri_h(tstp) * s2, h + (n1 + M) * s2, n1 * s2));
     }
     CK(cudaStreamSynchronize(b->stream));
@@ -423,13 +577,20 @@ static int slice_copy(nessi_batch *b, double2 *ret, double2 *tv, double2 *les, d
 int nessi_gpu_get_timestep(nessi_batch *b, int p, int tstp, void *slice) {
     CKR(check_prob(b, p));
     Prob &q = b->probs[p];
-    return slice_copy(b, q.gret, q.gtv, q.gles, q.gmat, q.d.nt, q.d.ntau, q.d.size1, tstp, slice, false);
+    return slice_copy(b, q.gret, q.gtv, q.gles, q.gmat, q.d.nt, q.d.ntau, q.d.size1, tstp, slice, false, true);
 }
 
 int nessi_gpu_set_timestep(nessi_batch *b, int p, int tstp, const void *slice) {
     CKR(check_prob(b, p));
     Prob &q = b->probs[p];
-    return slice_copy(b, q.gret, q.gtv, q.gles, q.gmat, q.d.nt, q.d.ntau, q.d.size1, tstp, (void *)slice, true);
+    if (tstp == -1) b->groups[q.group].gmat_valid = false;
+    CKR(slice_copy(b, q.gret, q.gtv, q.gles, q.gmat, q.d.nt, q.d.ntau, q.d.size1, tstp, (void *)slice, true, true));
+    if (tstp >= 0) {
+        const long row = (long)(q.d.ntau + 1) * q.d.size1 * q.d.size1;
+        CKR(refresh32(b, q.gtv32 ? q.gtv32 + tstp * row : nullptr, q.gtv + tstp * row, row));
+        CK(cudaStreamSynchronize(b->stream));
+    }
+    return NESSI_OK;
 }
 
 int nessi_gpu_set_H(nessi_batch *b, int p, const void *H) {
@@ -464,7 +625,7 @@ int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void
     int gi = find_group(b, group);
     if (gi < 0) { set_err("unknown sigma_group %d", group); return NESSI_ERR_ARG; }
     Group &g = b->groups[gi];
-    CKR(slice_copy(b, g.sret, g.stv, g.sles, g.smat, g.ntmax, g.ntau, g.s, tstp, (void *)slice, true));
+    CKR(slice_copy(b, g.sret, g.stv, g.sles, g.smat, g.ntmax, g.ntau, g.s, tstp, (void *)slice, true, false));
     if (tstp >= 0) {
         g.ret_valid = std::min(g.ret_valid, tstp - 1);
         g.les_valid = std::min(g.les_valid, tstp - 1);
@@ -482,6 +643,46 @@ int nessi_gpu_dyson_timestep(nessi_batch *b, int n) {
         if (nact == 0) continue;
         CKR(step_dispatch(b, g, n, nact));
     }
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_stream(nessi_batch *b, void *stream) {
+    CKR(check_batch(b));
+    CK(cudaStreamSynchronize(b->stream));
+    if (b->own_stream) { cudaStreamDestroy(b->stream); b->own_stream = false; }
+    if (stream) {
+        b->stream = (cudaStream_t)stream;
+    } else {
+        CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        b->own_stream = true;
+    }
+    CKB(cublasSetStream(b->cublas, b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_profiling(nessi_batch *b, int on) {
+    CKR(check_batch(b));
+    CK(cudaStreamSynchronize(b->stream));
+    b->prof = on != 0;
+    for (auto &k : b->kp) { k.used = 0; k.launches = 0; k.bytes = 0; }
+    return NESSI_OK;
+}
+
+int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *launches, double *bytes) {
+    CKR(check_batch(b));
+    if (kernel < 0 || kernel >= NESSI_KERNEL_COUNT) { set_err("bad kernel id %d", kernel); return NESSI_ERR_ARG; }
+    CK(cudaStreamSynchronize(b->stream));
+    KProf &k = b->kp[kernel];
+    double t = 0;
+    for (int i = 0; i + 1 < k.used; i += 2) {
+        float x = 0;
+        CK(cudaEventElapsedTime(&x, k.ev[i], k.ev[i + 1]));
+        t += x;
+    }
+    if (ms) *ms = t;
+    if (launches) *launches = k.launches;
+    if (bytes) *bytes = k.bytes;
+    k.used = 0; k.launches = 0; k.bytes = 0;
     return NESSI_OK;
 }
 

@@ -54,7 +54,13 @@ EXPORTS = {
     "nessi_gpu_set_sigma_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "nessi_gpu_dyson_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "nessi_gpu_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
 }
+
+KERNELS = ["prep", "ret", "tv", "les_operands", "gemm", "les", "matop"]
 
 
 def load_library(path=None):
@@ -153,6 +159,23 @@ class Batch:
 
     def synchronize(self):
         _check(load_library().nessi_gpu_synchronize(self._h))
+
+    def set_stream(self, stream_handle):
+        """Use a caller-owned cudaStream_t (an int handle, e.g. torch.cuda.Stream().cuda_stream)."""
+        _check(load_library().nessi_gpu_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
+
+    def set_profiling(self, on=True):
+        _check(load_library().nessi_gpu_set_profiling(self._h, int(on)))
+
+    def read_profile(self):
+        """{kernel: (device ms, launches, algorithmic bytes or flops)} since the last read."""
+        out = {}
+        for i, name in enumerate(KERNELS):
+            ms, nl, by = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+            _check(load_library().nessi_gpu_read_profile(self._h, i, ctypes.byref(ms), ctypes.byref(nl),
+                                                         ctypes.byref(by)))
+            out[name] = (ms.value, nl.value, by.value)
+        return out
 
 
 # ---- cntr-style single-problem entry points ---------------------------------------------

@@ -1,0 +1,113 @@
+"""Synthetic inputs with the shapes of the benchmark configurations.
+
+Each builder returns a ``Workload``: one shared self-energy Sigma, per-problem Hamiltonians
+H_k(t) (cntr::function layout, t = -1 first), the bootstrap time steps (mat and 0..k) of every
+G_k, and the batch descriptors.  All values are generated from formulas and seeds; no dataset
+is involved.
+
+chain2 (2-band chain, size1 = 2, Nk k-points in [-pi, pi)):
+    h_k(t) = [[-2cos(k - A(t)), 0.5], [0.5, 1 - 2cos(k - A(t))]],
+    A(t) = exp(-(t-5)^2/2) sin(3t),  H(-1) at A = 0,
+    Sigma = V^2 G_bath (x) 1_2 with V = 0.5, G_bath a semicircular bath (half-bandwidth 2,
+    201 levels), shared by all k.
+chain4 (4-band chain, size1 = 4): diagonal -2cos(k - A) + eps_a, eps = (-1.5, -0.5, 0.5, 1.5),
+    nearest-band hoppings 0.3, same Sigma (x) 1_4.
+"""
+import numpy as np
+
+from . import equilibrium as eq
+from .herm_matrix import herm_matrix
+
+
+class Workload:
+    def __init__(self, name, descs, sigma, H, boot, k, info):
+        self.name = name
+        self.descs = descs          # list of batch descriptors
+        self.sigma = sigma          # herm_matrix shared by all problems (sigma_group 0)
+        self.H = H                  # (nprob, nt+2, s, s)
+        self.boot = boot            # list of herm_matrix(nt=k) with mat and steps 0..k per problem
+        self.k = k
+        self.info = info
+
+    @property
+    def nprob(self):
+        return len(self.descs)
+
+    def kpt_steps(self):
+        return sum(d["nt"] - self.k for d in self.descs)
+
+
+def peierls(t):
+    return np.exp(-(t - 5.0) ** 2 / 2.0) * np.sin(3.0 * t)
+
+
+def chain_H(kvals, nt, h, eps_band, hop):
+    """H_k(t) for a chain with band offsets eps_band and inter-band hopping matrix hop."""
+    s = len(eps_band)
+    nk = len(kvals)
+    H = np.zeros((nk, nt + 2, s, s), np.complex128)
+    times = np.concatenate([[None], np.arange(nt + 1) * h])
+    for it, t in enumerate(times):
+        A = 0.0 if t is None else peierls(t)
+        for a in range(s):
+            H[:, it, a, a] = -2.0 * np.cos(kvals - A) + eps_band[a]
+        H[:, it] += hop
+    return H
+
+
+def bootstrap_free(H0, mu, beta, h, k, ntau, sig=-1):
+    """Time steps -1..k of the free propagator of H0 (the interim bootstrap of the benchmark)."""
+    s = H0.shape[0]
+    G = herm_matrix(k, ntau, s, sig)
+    eq.green_from_H(G, mu, H0, beta, h)
+    return G
+
+
+def chain(nk, nt, ntau, beta, h, size1, k=5, V=0.5, mu=0.0, kshift=0.0):
+    if size1 == 2:
+        eps_band = np.array([0.0, 1.0])
+        hop = np.array([[0, 0.5], [0.5, 0]], np.complex128)
+    elif size1 == 4:
+        eps_band = np.array([-1.5, -0.5, 0.5, 1.5])
+        hop = np.zeros((4, 4), np.complex128)
+        for a in range(3):
+            hop[a, a + 1] = hop[a + 1, a] = 0.3
+    else:
+        raise ValueError("chain workloads have size1 2 or 4")
+    kvals = -np.pi + 2 * np.pi * np.arange(nk) / nk + kshift
+    H = chain_H(kvals, nt, h, eps_band, hop)
+    Gb = eq.semicircle_bath(nt, ntau, beta, h)
+    sigma = eq.kron_identity(Gb, size1, V * V)
+    boot = []
+    cache = {}
+    for i in range(nk):
+        key = H[i, 0].tobytes()
+        if key not in cache:
+            cache[key] = bootstrap_free(H[i, 0], mu, beta, h, k, ntau)
+        boot.append(cache[key])
+    descs = [dict(nt=nt, ntau=ntau, size1=size1, sig=-1, solve_order=k, sigma_group=0, beta=beta, h=h, mu=mu)
+             for _ in range(nk)]
+    info = dict(model="%d-band chain" % size1, size1=size1, nk=nk, nt=nt, ntau=ntau, beta=beta, h=h,
+                solve_order=k, sigma="V^2 G_bath (x) 1, V=%g, shared" % V)
+    return Workload("chain%d" % size1, descs, sigma, H, boot, k, info)
+
+
+def config1(nk=256, nt=1000, ntau=600, kshift=0.0):
+    """Plain method batched over k, FP64: 2-band chain, Nk=256, nt=1000, ntau=600, beta=20, h=0.01."""
+    return chain(nk, nt, ntau, 20.0, 0.01, 2, kshift=kshift)
+
+
+def config2(nk=512, nt=4000, ntau=800, kshift=0.0):
+    """4-band chain, Nk=512, nt=4000, ntau=800, beta=20, h=0.01 (k-chunked when it does not fit)."""
+    return chain(nk, nt, ntau, 20.0, 0.01, 4, kshift=kshift)
+
+
+def upload(batch, W):
+    """Copy Sigma, H and the bootstrap steps of a workload into a gpu.Batch."""
+    batch.set_sigma(0, W.sigma)
+    for p in range(W.nprob):
+        batch.set_H(p, W.H[p])
+        B = W.boot[p]
+        batch.set_timestep(p, -1, B.mat)
+        for t in range(W.k + 1):
+            batch.set_timestep(p, t, B.get_timestep(t))
