@@ -80,6 +80,14 @@ int nessi_gpu_set_sigma(nessi_batch *b, int group, const void *ret, const void *
                         const void *mat);
 int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void *slice);
 
+/* cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder) with the default CNTR_MAT_FIXPOINT
+ * method and force_hermitian (cntr_dyson_decl.hpp:78, cntr_dyson_impl.hpp:1393-1450): G^mat of
+ * every problem from H(-1) and the group's Sigma^mat.  ntau must be even. */
+int nessi_gpu_dyson_mat(nessi_batch *b);
+/* cntr::dyson_start(G, mu, H, Sigma, beta, h, SolveOrder) (cntr_dyson_decl.hpp:88,
+ * cntr_dyson_impl.hpp:1502-1535): time steps 0..k of every problem from G^mat. */
+int nessi_gpu_dyson_start(nessi_batch *b);
+
 /* cntr::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder) for every problem of the
  * batch with nt >= n (cntr_dyson_decl.hpp:92, cntr_dyson_impl.hpp:1618-1648).  n > k.
  * G must hold time steps 0..n-1 and mat; Sigma and H must hold 0..n. */

@@ -259,81 +259,80 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
 // =======================================================================================
 // lesser component
 // =======================================================================================
-// acc[r] = sum_{m<mhi} w(j,m) Sigma^R(j,m) x_m, j = jlo + r; warp per row (warps w0..w0+nw-1)
+// acc[r] = sum_{m<mhi} w(j,m) Sigma^R(j,m) x_m, j = jlo + r.  Warp wi (of nw) takes rows
+// r = wi, wi+nw, ... all at once (RM rows), so every loaded x_m column serves RM rows and each
+// lane keeps RM independent row streams in flight; lane = (m-group, column d).
+template <int S> struct LesACfg {
+    static constexpr int RM = (RetCfg<S>::JB + 6) / 7;  // rows per warp when 7 warps share a block
+};
+
 template <int S>
 __device__ void les_phaseA(const GroupDev &g, const double2 *xcol, int jlo, int nb, int mhi, double2 *acc,
                            double2 *redbase, int wi, int nw, int lane, int warp) {
-    constexpr int s2 = S * S, LPG = S, NG = 32 / S;
+    constexpr int s2 = S * S, LPG = S, NG = 32 / S, RM = LesACfg<S>::RM;
     const int k = g.k;
-    for (int r = wi; r < nb; r += nw) {
-        const int j = jlo + r;
-        const int mg = lane / LPG, dd = lane % LPG;
-        double2 a_[S];
+    const int mg = lane / LPG, dd = lane % LPG;
+    for (int r0 = wi; r0 < nb; r0 += RM * nw) {
+        double2 a_[RM][S];
+        const double2 *srow[RM];
+        int jr[RM];
+        bool ok[RM];
 #pragma unroll
-        for (int a = 0; a < S; a++) a_[a] = cmk(0, 0);
+        for (int q = 0; q < RM; q++) {
+            const int r = r0 + q * nw;
+            ok[q] = r < nb;
+            jr[q] = jlo + (ok[q] ? r : 0);
+            srow[q] = g.sret + tri(jr[q]) * s2;
+#pragma unroll
+            for (int a = 0; a < S; a++) a_[q][a] = cmk(0, 0);
+        }
         if (mg < NG) {
-            const double2 *srow = g.sret + tri(j) * s2;
-            constexpr int U = S == 1 ? 4 : (S == 2 ? 2 : 1);
-            int m = mg;
-            for (; m + (U - 1) * NG < mhi; m += U * NG) {
-                double2 sv[U][s2], xv[U][S];
+            for (int m = mg; m < mhi; m += NG) {
+                double2 xv[S];
 #pragma unroll
-                for (int u = 0; u < U; u++) {
-                    const long mu = m + u * NG;
+                for (int b = 0; b < S; b++) xv[b] = xcol[(long)m * s2 + b * S + dd];
 #pragma unroll
-                    for (int i = 0; i < s2; i++) sv[u][i] = srow[mu * s2 + i];
-#pragma unroll
-                    for (int b = 0; b < S; b++) xv[u][b] = xcol[mu * s2 + b * S + dd];
-                }
-#pragma unroll
-                for (int u = 0; u < U; u++) {
-                    const double w = greg_w(k, j, m + u * NG);
+                for (int q = 0; q < RM; q++) {
+                    if (!ok[q]) continue;
+                    const double w = greg_w(k, jr[q], m);
+                    const double2 *sm = srow[q] + (long)m * s2;
 #pragma unroll
                     for (int a = 0; a < S; a++) {
                         double2 tt = cmk(0, 0);
 #pragma unroll
-                        for (int b = 0; b < S; b++) tt = cfma(sv[u][a * S + b], xv[u][b], tt);
-                        a_[a] = cfma(cmk(w, 0.0), tt, a_[a]);
+                        for (int b = 0; b < S; b++) tt = cfma(sm[a * S + b], xv[b], tt);
+                        a_[q][a] = cfma(cmk(w, 0.0), tt, a_[q][a]);
                     }
                 }
             }
-            for (; m < mhi; m += NG) {
-                const double w = greg_w(k, j, m);
-                const double2 *sm = srow + (long)m * s2;
-                const double2 *xm = xcol + (long)m * s2;
-#pragma unroll
-                for (int a = 0; a < S; a++) {
-                    double2 tt = cmk(0, 0);
-#pragma unroll
-                    for (int b = 0; b < S; b++) tt = cfma(sm[a * S + b], xm[b * S + dd], tt);
-                    a_[a] = cfma(cmk(w, 0.0), tt, a_[a]);
-                }
-            }
         }
-        if constexpr ((S & (S - 1)) == 0) {
 #pragma unroll
-            for (int a = 0; a < S; a++) {
-                double2 v = a_[a];
-                for (int off = LPG; off < 32; off <<= 1) {
-                    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
-                    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
-                }
-                a_[a] = v;
-            }
-            if (mg == 0)
-                for (int a = 0; a < S; a++) acc[r * s2 + a * S + dd] = a_[a];
-        } else {
-            double2 *red = redbase + warp * 32 * S;
-            for (int a = 0; a < S; a++) red[lane * S + a] = (mg < NG) ? a_[a] : cmk(0, 0);
-            __syncwarp();
-            if (lane < S) {
+        for (int q = 0; q < RM; q++) {
+            const int r = r0 + q * nw;
+            if (r >= nb) continue;
+            if constexpr ((S & (S - 1)) == 0) {
+#pragma unroll
                 for (int a = 0; a < S; a++) {
-                    double2 v = cmk(0, 0);
-                    for (int g2 = 0; g2 < NG; g2++) v = cadd(v, red[(g2 * S + lane) * S + a]);
-                    acc[r * s2 + a * S + lane] = v;
+                    double2 v = a_[q][a];
+                    for (int off = LPG; off < 32; off <<= 1) {
+                        v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+                        v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+                    }
+                    if (mg == 0) acc[r * s2 + a * S + dd] = v;
                 }
+            } else {
+                double2 *red = redbase + warp * 32 * S;
+                for (int a = 0; a < S; a++) red[lane * S + a] = (mg < NG) ? a_[q][a] : cmk(0, 0);
+                __syncwarp();
+                if (lane < S) {
+                    for (int a = 0; a < S; a++) {
+                        double2 v = cmk(0, 0);
+                        for (int g2 = 0; g2 < NG; g2++) v = cadd(v, red[(g2 * S + lane) * S + a]);
+                        acc[r * s2 + a * S + lane] = v;
+                    }
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
 }

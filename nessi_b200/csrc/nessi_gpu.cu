@@ -12,6 +12,8 @@
 
 #include "../../include/nessi_gpu.h"
 #include "kernels_dyson.cuh"
+#include "kernels_start.cuh"
+#include "kernels_mat.cuh"
 
 
 
@@ -91,6 +93,7 @@ struct Group {
     int ldc = 0;
     int dense_valid = -1, ret_valid = -1, les_valid = -1;
     bool gmat_valid = false;
+    MatScratch *d_mat = nullptr;  // per-member scratch of dyson_mat (allocated on first use)
     std::vector<int> members;        // problem indices, nt descending
     std::vector<ProbDev> h_probs;    // same order; col = position
     ProbDev *d_probs = nullptr;
@@ -310,6 +313,58 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     }
     return NESSI_OK;
 }
+
+template <int S> int start_group(nessi_batch *b, Group &g) {
+    const GroupDev gd = group_dev(g);
+    const size_t sm = NESSI_START_SMEM * sizeof(double2);
+    CK(cudaFuncSetAttribute(k_dyson_start<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_dyson_start<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+template <int S> int mat_group(nessi_batch *b, Group &g) {
+    const GroupDev gd = group_dev(g);
+    const long M = g.ntau + 1, s2 = (long)S * S;
+    if (!g.d_mat) {
+        std::vector<MatScratch> h(g.members.size());
+        for (auto &w : h) {
+            int r;
+            if ((r = b->alloc(&w.G0, M * s2)) || (r = b->alloc(&w.F, M * s2)) || (r = b->alloc(&w.Q, M * s2)) ||
+                (r = b->alloc(&w.dG, M * s2)) || (r = b->alloc(&w.fdft, M * s2)) || (r = b->alloc(&w.qdft, M * s2)) ||
+                (r = b->alloc(&w.Z, 2 * g.ntau * s2)))
+                return r;
+        }
+        void *q = nullptr;
+        CK(cudaMalloc(&q, h.size() * sizeof(MatScratch)));
+        b->allocs.push_back(q);
+        g.d_mat = (MatScratch *)q;
+        CK(cudaMemcpyAsync(g.d_mat, h.data(), h.size() * sizeof(MatScratch), cudaMemcpyHostToDevice, b->stream));
+    }
+    const size_t sm = 2 * (size_t)g.ntau * sizeof(double2);
+    CK(cudaFuncSetAttribute(k_dyson_mat<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_dyson_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat);
+    CK(cudaGetLastError());
+    g.gmat_valid = false;
+    return NESSI_OK;
+}
+
+#define NESSI_SIZE_SWITCH(fn, ...)                 \
+    switch (g.s) {                                 \
+        case 1: return fn<1>(__VA_ARGS__);         \
+        case 2: return fn<2>(__VA_ARGS__);         \
+        case 3: return fn<3>(__VA_ARGS__);         \
+        case 4: return fn<4>(__VA_ARGS__);         \
+        case 5: return fn<5>(__VA_ARGS__);         \
+        case 6: return fn<6>(__VA_ARGS__);         \
+        case 7: return fn<7>(__VA_ARGS__);         \
+        case 8: return fn<8>(__VA_ARGS__);         \
+    }                                              \
+    set_err("size1 = %d not supported (1..8)", g.s); \
+    return NESSI_ERR_ARG;
+
+int start_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(start_group, b, g) }
+int mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(mat_group, b, g) }
 
 int step_dispatch(nessi_batch *b, Group &g, int n, int nact) {
     switch (g.s) {
@@ -683,6 +738,31 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
     if (launches) *launches = k.launches;
     if (bytes) *bytes = k.bytes;
     k.used = 0; k.launches = 0; k.bytes = 0;
+    return NESSI_OK;
+}
+
+int nessi_gpu_dyson_mat(nessi_batch *b) {
+    CKR(check_batch(b));
+    for (Group &g : b->groups) {
+        if (g.ntau % 2) { set_err("dyson_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
+        CKR(mat_dispatch(b, g));
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_dyson_start(nessi_batch *b) {
+    CKR(check_batch(b));
+    for (Group &g : b->groups) {
+        for (int i : g.members)
+            if (b->probs[i].d.nt < g.k) { set_err("dyson_start: nt must be >= SolveOrder"); return NESSI_ERR_ARG; }
+        CKR(start_dispatch(b, g));
+    }
+    for (Prob &q : b->probs) {
+        const long row = (long)(q.d.ntau + 1) * q.d.size1 * q.d.size1;
+        CKR(refresh32(b, q.gtv32, q.gtv, (b->groups[q.group].k + 1) * row));
+    }
+    CK(cudaStreamSynchronize(b->stream));
     return NESSI_OK;
 }
 

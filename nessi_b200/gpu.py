@@ -53,6 +53,8 @@ EXPORTS = {
     "nessi_gpu_set_sigma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
     "nessi_gpu_set_sigma_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "nessi_gpu_dyson_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "nessi_gpu_dyson_mat": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_dyson_start": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -156,6 +158,14 @@ class Batch:
 
     def dyson_timestep(self, n):
         _check(load_library().nessi_gpu_dyson_timestep(self._h, n))
+
+    def dyson_mat(self):
+        """G^mat of every problem (cntr::dyson_mat, fixpoint method)."""
+        _check(load_library().nessi_gpu_dyson_mat(self._h))
+
+    def dyson_start(self):
+        """Time steps 0..k of every problem (cntr::dyson_start)."""
+        _check(load_library().nessi_gpu_dyson_start(self._h))
 
     def synchronize(self):
         _check(load_library().nessi_gpu_synchronize(self._h))
