@@ -144,6 +144,143 @@ __device__ void ret_stage(const GroupDev &g, const ProbDev &p, int n, int jlo, i
     for (int e = t; e < nb * s2; e += nthr) minv[e] = p.minv_ret[(long)jlo * s2 + e];
 }
 
+// Register-resident solve of one block for S <= 2 (warp 0): lane r owns block row r and keeps
+// its sum (acc), its backward-difference partial sum and its step inverse in registers.  After
+// row rr is solved its value is broadcast with warp shuffles and every lane folds it into its
+// own sums, so the sequential path per row is a handful of dependent FP64 operations and one
+// shuffle.  ibd[p] = (i/h) bd(p) in shared memory.
+template <int S>
+__device__ __forceinline__ void shfl_blk(double2 *x, int src) {
+#pragma unroll
+    for (int e = 0; e < S * S; e++) {
+        x[e].x = __shfl_sync(0xffffffffu, x[e].x, src);
+        x[e].y = __shfl_sync(0xffffffffu, x[e].y, src);
+    }
+}
+
+// ret: rows solved from r = nb-1 down to 0; x_r = (h acc_r - bdf_r) Minv_r (left solve)
+template <int S>
+__device__ void ret_chain(const double2 *acc, const double2 *sig, const double *wb, const double2 *minv, double2 *xs,
+                          double2 *gout, int nb, int K1, const double2 *ibd, double h, int lane) {
+    constexpr int s2 = S * S;
+    const int r = lane;
+    const bool own = r < nb;
+    double2 a_[s2], bd[s2], mi[s2];
+#pragma unroll
+    for (int e = 0; e < s2; e++) {
+        a_[e] = own ? acc[r * s2 + e] : cmk(0, 0);
+        mi[e] = own ? minv[r * s2 + e] : cmk(0, 0);
+        bd[e] = cmk(0, 0);
+    }
+    if (own)
+        for (int pp = 1; pp <= K1; pp++)
+            if (r + pp >= nb)
+#pragma unroll
+                for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[pp], xs[(r + pp) * s2 + e], bd[e]);
+    for (int rr = nb - 1; rr >= 0; rr--) {
+        double2 x[s2];
+        if (r == rr) {
+            double2 q[s2];
+#pragma unroll
+            for (int e = 0; e < s2; e++) q[e] = csub(cscale(a_[e], h), bd[e]);
+#pragma unroll
+            for (int aa = 0; aa < S; aa++)
+#pragma unroll
+                for (int d = 0; d < S; d++) {
+                    double2 t = cmk(0, 0);
+#pragma unroll
+                    for (int bb = 0; bb < S; bb++) t = cfma(q[aa * S + bb], mi[bb * S + d], t);
+                    x[aa * S + d] = t;
+                }
+        }
+        shfl_blk<S>(x, rr);
+        if (r == rr) {
+#pragma unroll
+            for (int e = 0; e < s2; e++) { xs[rr * s2 + e] = x[e]; gout[(long)rr * s2 + e] = x[e]; }
+        }
+        if (r < rr) {
+            const int q = pk(rr, r);
+            const double w = wb[q];
+            const double2 *sg = sig + q * s2;
+#pragma unroll
+            for (int aa = 0; aa < S; aa++)
+#pragma unroll
+                for (int d = 0; d < S; d++) {
+                    double2 t = cmk(0, 0);
+#pragma unroll
+                    for (int bb = 0; bb < S; bb++) t = cfma(x[aa * S + bb], sg[bb * S + d], t);
+                    a_[aa * S + d] = cfma(cmk(w, 0.0), t, a_[aa * S + d]);
+                }
+            if (rr - r <= K1)
+#pragma unroll
+                for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[rr - r], x[e], bd[e]);
+        }
+    }
+}
+
+// les: rows solved from r = 0 up; x_r = Minv_r (gl_r + h acc_r - bdf_r) (right solve);
+// xs holds x(jlo - K1 + i) at index i
+template <int S>
+__device__ void les_chain(const double2 *acc, const double2 *sig, const double *wb, const double2 *minv,
+                          const double2 *glb, double2 *xs, double2 *gout, int nb, int K1, const double2 *ibd, double h,
+                          int lane) {
+    constexpr int s2 = S * S;
+    const int r = lane;
+    const bool own = r < nb;
+    double2 a_[s2], bd[s2], mi[s2], gv[s2];
+#pragma unroll
+    for (int e = 0; e < s2; e++) {
+        a_[e] = own ? acc[r * s2 + e] : cmk(0, 0);
+        mi[e] = own ? minv[r * s2 + e] : cmk(0, 0);
+        gv[e] = own ? glb[r * s2 + e] : cmk(0, 0);
+        bd[e] = cmk(0, 0);
+    }
+    if (own)
+        for (int pp = 1; pp <= K1; pp++)
+            if (r - pp < 0)
+#pragma unroll
+                for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[pp], xs[(r - pp + K1) * s2 + e], bd[e]);
+    for (int rr = 0; rr < nb; rr++) {
+        double2 x[s2];
+        if (r == rr) {
+            double2 q[s2];
+#pragma unroll
+            for (int e = 0; e < s2; e++) q[e] = csub(cfma(cmk(h, 0.0), a_[e], gv[e]), bd[e]);
+#pragma unroll
+            for (int aa = 0; aa < S; aa++)
+#pragma unroll
+                for (int d = 0; d < S; d++) {
+                    double2 t = cmk(0, 0);
+#pragma unroll
+                    for (int bb = 0; bb < S; bb++) t = cfma(mi[aa * S + bb], q[bb * S + d], t);
+                    x[aa * S + d] = t;
+                }
+        }
+        shfl_blk<S>(x, rr);
+        if (r == rr) {
+#pragma unroll
+            for (int e = 0; e < s2; e++) { xs[(rr + K1) * s2 + e] = x[e]; gout[(long)rr * s2 + e] = x[e]; }
+        }
+        if (r > rr && own) {
+            const int q = pk(r, rr);
+            const double w = wb[q];
+            const double2 *sg = sig + q * s2;
+#pragma unroll
+            for (int aa = 0; aa < S; aa++)
+#pragma unroll
+                for (int d = 0; d < S; d++) {
+                    double2 t = cmk(0, 0);
+#pragma unroll
+                    for (int bb = 0; bb < S; bb++) t = cfma(sg[aa * S + bb], x[bb * S + d], t);
+                    a_[aa * S + d] = cfma(cmk(w, 0.0), t, a_[aa * S + d]);
+                }
+            if (r - rr <= K1)
+#pragma unroll
+                for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[r - rr], x[e], bd[e]);
+        }
+    }
+}
+
 template <int S>
 __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__restrict__ probs, int n) {
     extern __shared__ double2 smem[];
@@ -163,6 +300,8 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
     double2 ibd[NESSI_K1MAX + 1];
 #pragma unroll
     for (int pp = 0; pp <= NESSI_K1MAX; pp++) ibd[pp] = cmk(0.0, pp <= K1 ? bd_w(k, pp) / h : 0.0);
+    __shared__ double2 ibds[NESSI_K1MAX + 1];
+    if (tid <= NESSI_K1MAX) ibds[tid] = cmk(0.0, tid <= K1 ? bd_w(k, tid) / h : 0.0);
     const int jtop = n - k - 1;
     auto ACC = [&](int bf) { return smem + L::acc + bf * JB * s2; };
     auto SIG = [&](int bf) { return smem + L::sig + bf * L::TRI * s2; };
@@ -182,7 +321,9 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
         const int jhi = jtop - b * JB, jlo = jhi - JB + 1 < 0 ? 0 : jhi - JB + 1, nb = jhi - jlo + 1;
         const bool has_next = jlo > 0;
         const int jhi2 = jlo - 1, jlo2 = jhi2 - JB + 1 < 0 ? 0 : jhi2 - JB + 1, nb2 = jhi2 - jlo2 + 1;
-        if (warp == 0) {
+        if (warp == 0 && S <= 2) {
+            ret_chain<S>(ACC(cur), SIG(cur), WBF(cur), MNV(cur), XS(cur), grow + (long)jlo * s2, nb, K1, ibds, h, lane);
+        } else if (warp == 0) {
             // ---- phase B: solve j = jhi .. jlo
             double2 *acc = ACC(cur), *sig = SIG(cur), *minv = MNV(cur), *xs = XS(cur);
             const double *wb = WBF(cur);
@@ -259,80 +400,81 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
 // =======================================================================================
 // lesser component
 // =======================================================================================
-// acc[r] = sum_{m<mhi} w(j,m) Sigma^R(j,m) x_m, j = jlo + r.  Warp wi (of nw) takes rows
-// r = wi, wi+nw, ... all at once (RM rows), so every loaded x_m column serves RM rows and each
-// lane keeps RM independent row streams in flight; lane = (m-group, column d).
-template <int S> struct LesACfg {
-    static constexpr int RM = (RetCfg<S>::JB + 6) / 7;  // rows per warp when 7 warps share a block
-};
-
+// acc[r] = sum_{m<mhi} w(j,m) Sigma^R(j,m) x_m, j = jlo + r; warp per row (warps w0..w0+nw-1)
 template <int S>
 __device__ void les_phaseA(const GroupDev &g, const double2 *xcol, int jlo, int nb, int mhi, double2 *acc,
                            double2 *redbase, int wi, int nw, int lane, int warp) {
-    constexpr int s2 = S * S, LPG = S, NG = 32 / S, RM = LesACfg<S>::RM;
+    constexpr int s2 = S * S, LPG = S, NG = 32 / S;
     const int k = g.k;
-    const int mg = lane / LPG, dd = lane % LPG;
-    for (int r0 = wi; r0 < nb; r0 += RM * nw) {
-        double2 a_[RM][S];
-        const double2 *srow[RM];
-        int jr[RM];
-        bool ok[RM];
+    for (int r = wi; r < nb; r += nw) {
+        const int j = jlo + r;
+        const int mg = lane / LPG, dd = lane % LPG;
+        double2 a_[S];
 #pragma unroll
-        for (int q = 0; q < RM; q++) {
-            const int r = r0 + q * nw;
-            ok[q] = r < nb;
-            jr[q] = jlo + (ok[q] ? r : 0);
-            srow[q] = g.sret + tri(jr[q]) * s2;
-#pragma unroll
-            for (int a = 0; a < S; a++) a_[q][a] = cmk(0, 0);
-        }
+        for (int a = 0; a < S; a++) a_[a] = cmk(0, 0);
         if (mg < NG) {
-            for (int m = mg; m < mhi; m += NG) {
-                double2 xv[S];
+            const double2 *srow = g.sret + tri(j) * s2;
+            constexpr int U = S == 1 ? 4 : (S == 2 ? 2 : 1);
+            int m = mg;
+            for (; m + (U - 1) * NG < mhi; m += U * NG) {
+                double2 sv[U][s2], xv[U][S];
 #pragma unroll
-                for (int b = 0; b < S; b++) xv[b] = xcol[(long)m * s2 + b * S + dd];
+                for (int u = 0; u < U; u++) {
+                    const long mu = m + u * NG;
 #pragma unroll
-                for (int q = 0; q < RM; q++) {
-                    if (!ok[q]) continue;
-                    const double w = greg_w(k, jr[q], m);
-                    const double2 *sm = srow[q] + (long)m * s2;
+                    for (int i = 0; i < s2; i++) sv[u][i] = srow[mu * s2 + i];
+#pragma unroll
+                    for (int b = 0; b < S; b++) xv[u][b] = xcol[mu * s2 + b * S + dd];
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const double w = greg_w(k, j, m + u * NG);
 #pragma unroll
                     for (int a = 0; a < S; a++) {
                         double2 tt = cmk(0, 0);
 #pragma unroll
-                        for (int b = 0; b < S; b++) tt = cfma(sm[a * S + b], xv[b], tt);
-                        a_[q][a] = cfma(cmk(w, 0.0), tt, a_[q][a]);
+                        for (int b = 0; b < S; b++) tt = cfma(sv[u][a * S + b], xv[u][b], tt);
+                        a_[a] = cfma(cmk(w, 0.0), tt, a_[a]);
                     }
+                }
+            }
+            for (; m < mhi; m += NG) {
+                const double w = greg_w(k, j, m);
+                const double2 *sm = srow + (long)m * s2;
+                const double2 *xm = xcol + (long)m * s2;
+#pragma unroll
+                for (int a = 0; a < S; a++) {
+                    double2 tt = cmk(0, 0);
+#pragma unroll
+                    for (int b = 0; b < S; b++) tt = cfma(sm[a * S + b], xm[b * S + dd], tt);
+                    a_[a] = cfma(cmk(w, 0.0), tt, a_[a]);
                 }
             }
         }
+        if constexpr ((S & (S - 1)) == 0) {
 #pragma unroll
-        for (int q = 0; q < RM; q++) {
-            const int r = r0 + q * nw;
-            if (r >= nb) continue;
-            if constexpr ((S & (S - 1)) == 0) {
-#pragma unroll
-                for (int a = 0; a < S; a++) {
-                    double2 v = a_[q][a];
-                    for (int off = LPG; off < 32; off <<= 1) {
-                        v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
-                        v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
-                    }
-                    if (mg == 0) acc[r * s2 + a * S + dd] = v;
+            for (int a = 0; a < S; a++) {
+                double2 v = a_[a];
+                for (int off = LPG; off < 32; off <<= 1) {
+                    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+                    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
                 }
-            } else {
-                double2 *red = redbase + warp * 32 * S;
-                for (int a = 0; a < S; a++) red[lane * S + a] = (mg < NG) ? a_[q][a] : cmk(0, 0);
-                __syncwarp();
-                if (lane < S) {
-                    for (int a = 0; a < S; a++) {
-                        double2 v = cmk(0, 0);
-                        for (int g2 = 0; g2 < NG; g2++) v = cadd(v, red[(g2 * S + lane) * S + a]);
-                        acc[r * s2 + a * S + lane] = v;
-                    }
-                }
-                __syncwarp();
+                a_[a] = v;
             }
+            if (mg == 0)
+                for (int a = 0; a < S; a++) acc[r * s2 + a * S + dd] = a_[a];
+        } else {
+            double2 *red = redbase + warp * 32 * S;
+            for (int a = 0; a < S; a++) red[lane * S + a] = (mg < NG) ? a_[a] : cmk(0, 0);
+            __syncwarp();
+            if (lane < S) {
+                for (int a = 0; a < S; a++) {
+                    double2 v = cmk(0, 0);
+                    for (int g2 = 0; g2 < NG; g2++) v = cadd(v, red[(g2 * S + lane) * S + a]);
+                    acc[r * s2 + a * S + lane] = v;
+                }
+            }
+            __syncwarp();
         }
     }
 }
@@ -380,6 +522,8 @@ __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__res
     double2 ibd[NESSI_K1MAX + 1];
 #pragma unroll
     for (int pp = 0; pp <= NESSI_K1MAX; pp++) ibd[pp] = cmk(0.0, pp <= K1 ? bd_w(k, pp) / h : 0.0);
+    __shared__ double2 ibds[NESSI_K1MAX + 1];
+    if (tid <= NESSI_K1MAX) ibds[tid] = cmk(0.0, tid <= K1 ? bd_w(k, tid) / h : 0.0);
     auto ACC = [&](int bf) { return smem + L::acc + bf * JB * s2; };
     auto SIG = [&](int bf) { return smem + L::sig + bf * L::TRI * s2; };
     auto WBF = [&](int bf) { return (double *)(smem + L::w + bf * L::WB); };
@@ -399,7 +543,10 @@ __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__res
         const int jlo = jstart + b * JB, jhi = jlo + JB - 1 > n ? n : jlo + JB - 1, nb = jhi - jlo + 1;
         const bool has_next = jhi < n;
         const int jlo2 = jhi + 1, jhi2 = jlo2 + JB - 1 > n ? n : jlo2 + JB - 1, nb2 = jhi2 - jlo2 + 1;
-        if (warp == 0) {
+        if (warp == 0 && S <= 2) {
+            les_chain<S>(ACC(cur), SIG(cur), WBF(cur), MNV(cur), GLB(cur), XS(cur), xcol + (long)jlo * s2, nb, K1, ibds,
+                         h, lane);
+        } else if (warp == 0) {
             double2 *acc = ACC(cur), *sig = SIG(cur), *minv = MNV(cur), *glb = GLB(cur), *xs = XS(cur);
             const double *wb = WBF(cur);
             for (int r = 0; r < nb; r++) {
