@@ -261,18 +261,22 @@ def main():
     kernels_per_step = 7  # prep_problem, prep_group, ret, mat_operator, tv, les_operands, les
     gpu_launches = kernels_per_step * (nt - k) * args.steps
 
-    # roofline of the dominant kernel of ours (GEMM is cuBLAS)
+    # roofline of k_tv, the G^tv history stream: the largest single kernel in the serialised ncu
+    # launch list (profiles/launches_config1-ncu.md) and the HBM-bound core of the step
     peak, peak_kind = load_peaks()
-    own = {kname: v for kname, v in prof.items() if kname != "gemm"}
-    dom = max(own, key=lambda x: own[x][0])
-    dms, dl, dbytes = own[dom]
+    dom = "tv"
+    dms, dl, dbytes = prof[dom]
     achieved = (dbytes / dl) / ((dms / dl) / 1000.0) / 1e9 if dl else 0.0
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (dom, args.workload))
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
-    roofline = {"kernel": "k_" + dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    tpath = os.path.join(ROOT, "profiles", "k_tv_config1-ncu.md")
+    if os.path.exists(tpath) and dl:
+        for line in open(tpath):
+            if line.startswith("traffic_ratio:"):
+                traffic = float(line.split(":")[1]) * dbytes / dl
+    roofline = {"kernel": "k_tv", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                "traffic_note": "DRAM bytes per algorithmic byte from one ncu capture at nt=ntau=300, "
+                                "scaled to this launch's algorithmic bytes",
                 "algorithmic_bytes_per_launch": dbytes / dl if dl else None,
                 "avg_launch_ms": dms / dl if dl else None}
     breakdown = {kname: {"ms": v[0] / args.steps, "launches": v[1] // args.steps,

@@ -1,0 +1,135 @@
+// cntr_gpu.hpp - header-only C++ front end of libnessi_gpu.so with libcntr's call signatures.
+//
+// A libcntr program replaces
+//     cntr::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder);
+// by
+//     cntr_gpu::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder);
+// with G, Sigma of type cntr::herm_matrix<double> and H of type cntr::function<double>
+// (libcntr/cntr/cntr_dyson_decl.hpp:78-92).  The templates only need the public accessors of
+// those classes (nt, ntau, size1, sig, retptr, lesptr, tvptr, matptr; function::ptr), so this
+// header does not include libcntr.
+//
+// The single-problem functions copy the whole G and Sigma to the device on every call, which is
+// what a drop-in for one call can do.  Lattice codes advance all k-points of a time step
+// together through cntr_gpu::Batch (the replacement of the per-k loop of
+// examples/programs/gw.cpp:386-420), which keeps every G and the shared Sigma in device memory
+// and moves only time-step slices.
+#pragma once
+
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nessi_gpu.h"
+
+namespace cntr_gpu {
+
+inline void check(int rc) {
+    if (rc != NESSI_OK) throw std::runtime_error(std::string("libnessi_gpu: ") + nessi_gpu_last_error());
+}
+
+// number of complex<double> in one herm_matrix_timestep slice [ret | tv | les] (n >= 0)
+template <class HM> inline long slice_len(const HM &G, int n) {
+    return (2L * (n + 1) + G.ntau() + 1) * G.size1() * G.size1();
+}
+
+// Problems advanced together; problems added with the same sigma_group share one Sigma.
+template <class HM, class FN> class Batch {
+  public:
+    explicit Batch(int precision = NESSI_PREC_FP64) : precision_(precision) {}
+    ~Batch() { if (b_) nessi_gpu_batch_destroy(b_); }
+    Batch(const Batch &) = delete;
+    Batch &operator=(const Batch &) = delete;
+
+    // register problem p (returns its index); call before build()
+    int add(HM &G, FN &H, double mu, double beta, double h, int SolveOrder = 5, int sigma_group = 0) {
+        nessi_problem_desc d;
+        d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+        d.solve_order = SolveOrder; d.sigma_group = sigma_group; d.beta = beta; d.h = h; d.mu = mu;
+        descs_.push_back(d);
+        G_.push_back(&G);
+        H_.push_back(&H);
+        return (int)descs_.size() - 1;
+    }
+    // allocate device storage and upload G (all components), H and the group's Sigma
+    void build(HM &Sigma, int sigma_group = 0) {
+        check(nessi_gpu_batch_create(&b_, descs_.data(), (int)descs_.size(), precision_));
+        for (size_t p = 0; p < G_.size(); p++) {
+            HM &G = *G_[p];
+            check(nessi_gpu_set_G(b_, (int)p, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0)));
+            check(nessi_gpu_set_H(b_, (int)p, H_[p]->ptr(-1)));
+        }
+        set_sigma(Sigma, sigma_group);
+    }
+    void set_sigma(HM &Sigma, int sigma_group = 0) {
+        check(nessi_gpu_set_sigma(b_, sigma_group, Sigma.retptr(0, 0), Sigma.lesptr(0, 0), Sigma.tvptr(0, 0),
+                                  Sigma.matptr(0)));
+    }
+    // one time step of Sigma, in herm_matrix_timestep order (e.g. from a self-energy diagram)
+    void set_sigma_timestep(int n, const std::complex<double> *slice, int sigma_group = 0) {
+        check(nessi_gpu_set_sigma_timestep(b_, sigma_group, n, slice));
+    }
+    void dyson_mat() { check(nessi_gpu_dyson_mat(b_)); }
+    void dyson_start() { check(nessi_gpu_dyson_start(b_)); }
+    void dyson_timestep(int n) { check(nessi_gpu_dyson_timestep(b_, n)); }
+    // copy time step n of problem p back into its herm_matrix
+    void download_timestep(int p, int n) {
+        HM &G = *G_[p];
+        std::vector<std::complex<double>> s(n < 0 ? (long)(G.ntau() + 1) * G.size1() * G.size1() : slice_len(G, n));
+        check(nessi_gpu_get_timestep(b_, p, n, s.data()));
+        const long es = (long)G.size1() * G.size1();
+        if (n < 0) {
+            std::copy(s.begin(), s.end(), G.matptr(0));
+            return;
+        }
+        const long n1 = n + 1, M = G.ntau() + 1;
+        std::copy(s.begin(), s.begin() + n1 * es, G.retptr(n, 0));
+        std::copy(s.begin() + n1 * es, s.begin() + (n1 + M) * es, G.tvptr(n, 0));
+        std::copy(s.begin() + (n1 + M) * es, s.end(), G.lesptr(0, n));
+    }
+    void download_all() {
+        for (size_t p = 0; p < G_.size(); p++) {
+            HM &G = *G_[p];
+            check(nessi_gpu_get_G(b_, (int)p, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0)));
+        }
+    }
+    nessi_batch *handle() { return b_; }
+
+  private:
+    int precision_;
+    nessi_batch *b_ = nullptr;
+    std::vector<nessi_problem_desc> descs_;
+    std::vector<HM *> G_;
+    std::vector<FN *> H_;
+};
+
+// ---- single-problem drop-ins (cntr_dyson_decl.hpp:78-92) -------------------------------
+template <class HM, class FN>
+void dyson_timestep(int n, HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveOrder = 5) {
+    Batch<HM, FN> b;
+    b.add(G, H, mu, beta, h, SolveOrder);
+    b.build(Sigma);
+    b.dyson_timestep(n);
+    b.download_timestep(0, n);
+}
+
+template <class HM, class FN>
+void dyson_start(HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveOrder = 5) {
+    Batch<HM, FN> b;
+    b.add(G, H, mu, beta, h, SolveOrder);
+    b.build(Sigma);
+    b.dyson_start();
+    for (int n = 0; n <= SolveOrder; n++) b.download_timestep(0, n);
+}
+
+template <class HM, class FN>
+void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder = 5) {
+    Batch<HM, FN> b;
+    b.add(G, H, mu, beta, 1.0, SolveOrder);
+    b.build(Sigma);
+    b.dyson_mat();
+    b.download_timestep(0, -1);
+}
+
+}  // namespace cntr_gpu

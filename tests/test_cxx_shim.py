@@ -1,0 +1,55 @@
+"""include/cntr_gpu.hpp (the libcntr-side front end) compiles against a herm_matrix-like class
+with libcntr's public accessors and links against libnessi_gpu.so (no GPU needed)."""
+import os
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+MOCK = r'''
+#include <complex>
+#include <vector>
+#include "cntr_gpu.hpp"
+typedef std::complex<double> cplx;
+struct HM {  // the accessors of cntr::herm_matrix<double> used by cntr_gpu.hpp
+    int nt_, ntau_, s_, sig_;
+    std::vector<cplx> r_, l_, t_, m_;
+    HM(int nt, int ntau, int s, int sig) : nt_(nt), ntau_(ntau), s_(s), sig_(sig),
+        r_((nt + 1) * (nt + 2) / 2 * s * s), l_(r_.size()), t_((nt + 1) * (ntau + 1) * s * s), m_((ntau + 1) * s * s) {}
+    int nt() const { return nt_; }
+    int ntau() const { return ntau_; }
+    int size1() const { return s_; }
+    int sig() const { return sig_; }
+    cplx *retptr(int i, int j) { return r_.data() + ((long)i * (i + 1) / 2 + j) * s_ * s_; }
+    cplx *lesptr(int i, int j) { return l_.data() + ((long)j * (j + 1) / 2 + i) * s_ * s_; }
+    cplx *tvptr(int i, int m) { return t_.data() + ((long)i * (ntau_ + 1) + m) * s_ * s_; }
+    cplx *matptr(int m) { return m_.data() + (long)m * s_ * s_; }
+};
+struct FN {
+    int nt_, s_;
+    std::vector<cplx> d_;
+    FN(int nt, int s) : nt_(nt), s_(s), d_((nt + 2) * s * s) {}
+    cplx *ptr(int t) { return d_.data() + (long)(t + 1) * s_ * s_; }
+};
+int main(int argc, char **argv) {
+    if (argc < 2) return 0;  // link check only
+    HM G(12, 10, 2, -1), S(12, 10, 2, -1);
+    FN H(12, 2);
+    cntr_gpu::dyson_mat(G, 0.0, H, S, 5.0, 5);
+    cntr_gpu::dyson_start(G, 0.0, H, S, 5.0, 0.05, 5);
+    cntr_gpu::dyson_timestep(6, G, 0.0, H, S, 5.0, 0.05, 5);
+    return 0;
+}
+'''
+
+
+def test_cntr_gpu_header_compiles_and_links(tmp_path):
+    from nessi_b200 import build
+    build.build()
+    src = tmp_path / "mock.cpp"
+    src.write_text(MOCK)
+    exe = tmp_path / "mock"
+    libdir = os.path.join(ROOT, "nessi_b200")
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+           "-L", libdir, "-lnessi_gpu", "-Wl,-rpath," + libdir]
+    subprocess.check_call(cmd)
+    assert exe.exists()
