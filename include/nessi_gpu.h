@@ -112,6 +112,23 @@ int nessi_gpu_set_profiling(nessi_batch *b, int on);
  * kernel id since the last read; resets that counter.  No reference counterpart. */
 int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *launches, double *bytes);
 
+/* dyson_mat (fixpoint method) for ONE problem, allocating nothing.  No counterpart in the
+ * reference.  It is meant for callers that cannot let a library call cudaMalloc: code running
+ * while its stream is captured, or applications whose device memory is owned by another
+ * allocator.  Every input and output is a device pointer owned by the caller:
+ *   H          cntr::function data starting at H(-1) (at least one size1 x size1 block)
+ *   sigma_mat  Sigma^mat, (ntau+1) blocks;   gmat  G^mat, (ntau+1) blocks, written
+ * The work is queued on `stream` (a cudaStream_t, NULL = legacy default stream) and the call
+ * returns without waiting.  Scratch is a fixed device array of 131072 complex<double>
+ * (2 MiB) that every GPU loading the library holds until exit; sizes with
+ * 6(ntau+1)size1^2 + 2 ntau size1^2 above that limit are rejected with NESSI_ERR_ARG.  The first
+ * call on a device looks up the array's device address and uploads the integration tables, so
+ * make that first call before any stream capture.  All calls share the one array: calls whose
+ * work overlaps on the GPU race.  Every scratch element is written before it is read, so
+ * nothing left by an earlier call leaks into a result.  ntau must be even. */
+int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int solve_order, double beta, double mu, const void *H,
+                                const void *sigma_mat, void *gmat, void *stream);
+
 /* Wait for all work queued on the batch. */
 int nessi_gpu_synchronize(nessi_batch *b);
 

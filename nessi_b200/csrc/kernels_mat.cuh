@@ -257,14 +257,14 @@ __device__ void vie2_mat_fourier_dev(double2 *G, const double2 *F, const double2
     __syncthreads();
 }
 
+// Body of dyson_mat for one problem (one CTA): reads g.smat, g.k, g.ntau, g.sig, g.beta and
+// p.H, p.mu; writes p.gmat; uses the scratch vectors of w.
 template <int S>
-__global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr) {
+__device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScratch &w) {
     constexpr int s2 = S * S;
     __shared__ double ev[S];
     __shared__ double2 V[S * S], qmasy[S * S];
     extern __shared__ double2 tw[];  // 2 ntau twiddles e^{i pi q / ntau}
-    const ProbDev p = probs[blockIdx.x];
-    const MatScratch w = scr[blockIdx.x];
     const int k = g.k, ntau = g.ntau, M = ntau + 1, sig = g.sig;
     const double beta = g.beta, dtau = beta / ntau;
     for (int q = threadIdx.x; q < 2 * ntau; q += blockDim.x) {
@@ -321,4 +321,9 @@ __global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__
     }
     __syncthreads();
     for (int e = threadIdx.x; e < M * s2; e += blockDim.x) p.gmat[e] = w.dG[e];
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr) {
+    dyson_mat_body<S>(g, probs[blockIdx.x], scr[blockIdx.x]);
 }

@@ -773,3 +773,86 @@ int nessi_gpu_synchronize(nessi_batch *b) {
 }
 
 }  // extern "C"
+
+// =====================================================================================
+// dyson_mat without allocation
+// =====================================================================================
+// Some callers cannot let a library call cudaMalloc: code that runs while its stream is being
+// captured, or a host application whose device memory is owned by another allocator (a
+// framework's memory pool, a preallocated arena).  nessi_gpu_dyson_mat_noalloc serves them:
+// the caller passes every input and output as device pointers and the scratch lives in the
+// fixed array below, which every GPU that loads this library holds until the process exits.
+#define NESSI_NOALLOC_MAX_CPLX (1 << 17)  // 131072 complex<double> = 2 MiB
+static __device__ __align__(256) double2 g_noalloc_scratch[NESSI_NOALLOC_MAX_CPLX];
+
+namespace {
+// device address of g_noalloc_scratch per device, looked up once with that device current
+double2 *g_noalloc_addr[64] = {nullptr};
+
+template <int S>
+__global__ void __launch_bounds__(256) k_dyson_mat_single(GroupDev g, ProbDev p, MatScratch w) {
+    dyson_mat_body<S>(g, p, w);
+}
+
+template <int S>
+int noalloc_launch(const GroupDev &gd, const ProbDev &pd, const MatScratch &w, int ntau, cudaStream_t st) {
+    const size_t sm = 2 * (size_t)ntau * sizeof(double2);
+    CK(cudaFuncSetAttribute(k_dyson_mat_single<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_dyson_mat_single<S><<<1, 256, sm, st>>>(gd, pd, w);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+}  // namespace
+
+extern "C" int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int solve_order, double beta, double mu,
+                                           const void *H, const void *sigma_mat, void *gmat, void *stream) {
+    if (!H || !sigma_mat || !gmat) { set_err("dyson_mat_noalloc: null pointer"); return NESSI_ERR_ARG; }
+    if (size1 < 1 || size1 > NESSI_MAXS || (sig != 1 && sig != -1) || solve_order < 1 || solve_order > CNTR_KMAX ||
+        ntau < solve_order || ntau % 2 || !(beta > 0)) {
+        set_err("dyson_mat_noalloc: bad arguments (ntau=%d size1=%d sig=%d k=%d)", ntau, size1, sig, solve_order);
+        return NESSI_ERR_ARG;
+    }
+    const long s2 = (long)size1 * size1, M = ntau + 1;
+    const long need = 6 * M * s2 + 2L * ntau * s2;
+    if (need > NESSI_NOALLOC_MAX_CPLX) {
+        set_err("dyson_mat_noalloc: 6(ntau+1)s^2 + 2 ntau s^2 = %ld complex exceeds the fixed scratch of %d", need,
+                NESSI_NOALLOC_MAX_CPLX);
+        return NESSI_ERR_ARG;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) { set_err("dyson_mat_noalloc: device index %d unsupported", dev); return NESSI_ERR_ARG; }
+    if (!g_noalloc_addr[dev]) {
+        // set-up on the first call on this device: integration tables and the scratch address
+        CKR(ensure_tables(dev));
+        void *ptr = nullptr;
+        CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_addr[dev] = (double2 *)ptr;
+    }
+    double2 *base = g_noalloc_addr[dev];
+    MatScratch w;
+    w.G0 = base; w.F = base + M * s2; w.Q = base + 2 * M * s2; w.dG = base + 3 * M * s2;
+    w.fdft = base + 4 * M * s2; w.qdft = base + 5 * M * s2; w.Z = base + 6 * M * s2;
+    GroupDev gd;
+    std::memset(&gd, 0, sizeof gd);
+    gd.smat = (const double2 *)sigma_mat;
+    gd.ntau = ntau; gd.s = size1; gd.sig = sig; gd.k = solve_order; gd.beta = beta;
+    ProbDev pd;
+    std::memset(&pd, 0, sizeof pd);
+    pd.H = (const double2 *)H;
+    pd.gmat = (double2 *)gmat;
+    pd.mu = mu;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (size1) {
+        case 1: return noalloc_launch<1>(gd, pd, w, ntau, st);
+        case 2: return noalloc_launch<2>(gd, pd, w, ntau, st);
+        case 3: return noalloc_launch<3>(gd, pd, w, ntau, st);
+        case 4: return noalloc_launch<4>(gd, pd, w, ntau, st);
+        case 5: return noalloc_launch<5>(gd, pd, w, ntau, st);
+        case 6: return noalloc_launch<6>(gd, pd, w, ntau, st);
+        case 7: return noalloc_launch<7>(gd, pd, w, ntau, st);
+        case 8: return noalloc_launch<8>(gd, pd, w, ntau, st);
+    }
+    set_err("dyson_mat_noalloc: size1 %d unsupported", size1);
+    return NESSI_ERR_ARG;
+}

@@ -57,6 +57,9 @@ EXPORTS = {
     "nessi_gpu_dyson_start": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "nessi_gpu_dyson_mat_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
@@ -186,6 +189,14 @@ class Batch:
                                                          ctypes.byref(by)))
             out[name] = (ms.value, nl.value, by.value)
         return out
+
+
+def dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, H_ptr, sigma_mat_ptr, gmat_ptr, stream=0):
+    """nessi_gpu_dyson_mat_noalloc on caller-owned device pointers (integers); allocates
+    nothing.  For callers that cannot let the library allocate device memory."""
+    _check(load_library().nessi_gpu_dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, ctypes.c_void_p(H_ptr),
+                                                       ctypes.c_void_p(sigma_mat_ptr), ctypes.c_void_p(gmat_ptr),
+                                                       ctypes.c_void_p(stream) if stream else None))
 
 
 # ---- cntr-style single-problem entry points ---------------------------------------------
