@@ -113,9 +113,24 @@ def cpu_sample(W, target_s=15.0, max_threads=None):
         Gs.append(G)
     Hs = np.ascontiguousarray(W.H[:P])
     beta, h, mu = d0["beta"], d0["h"], d0["mu"]
+    if W.lattice:
+        # a lattice step needs all of its k-points together: the sample lattice is the first P
+        # k-points (same cost per k-point step; G_loc is their average)
+        Gloc = herm_matrix(nt, ntau, s, d0["sig"])
+        Sig = herm_matrix(nt, ntau, s, d0["sig"])
+        Um = np.zeros((nt + 2, s, s), np.complex128)
+        for i in range(s):
+            Um[:, i, i] = W.U[:, i]
+
+        def steps(a, b_):
+            for n in range(a, b_ + 1):
+                O.lattice2b_timestep(n, Gs, Gloc, Sig, Um, mu, Hs, beta, h, k, ncorr=W.ncorr, nthreads=threads)
+    else:
+        def steps(a, b_):
+            O.dyson_timestep_batch(a, b_, Gs, mu, Hs, W.sigma, beta, h, k, threads)
     # probe one step at the largest n to size the windows
     t0 = time.perf_counter()
-    O.dyson_timestep_batch(nt, nt, Gs, mu, Hs, W.sigma, beta, h, k, threads)
+    steps(nt, nt)
     t1 = time.perf_counter() - t0
     pts = sorted(set([max(k + 1, int(nt * f)) for f in (0.1, 0.3, 0.6, 1.0)]))
     win = int(max(1, min(40, target_s / (len(pts) * max(t1, 1e-6)))))
@@ -123,7 +138,7 @@ def cpu_sample(W, target_s=15.0, max_threads=None):
     for n in pts:
         a = max(k + 1, n - win + 1)
         t0 = time.perf_counter()
-        O.dyson_timestep_batch(a, n, Gs, mu, Hs, W.sigma, beta, h, k, threads)
+        steps(a, n)
         dt = (time.perf_counter() - t0) / (n - a + 1)
         ns.append(0.5 * (a + n) + 1)
         ts.append(dt)
@@ -136,6 +151,8 @@ def cpu_sample(W, target_s=15.0, max_threads=None):
     resid = float(np.max(np.abs(A @ coef - np.array(ts)) / np.array(ts)))
     desc = ("%d problems in parallel on %d threads, windows of %d steps at n=%s, fit t(n)=a+bN+cN^2 "
             "integrated over n=%d..%d (max fit residual %.1f%%)" % (P, threads, win, pts, k + 1, nt, 100 * resid))
+    if W.lattice:
+        desc += "; lattice steps with %d correctors, G_loc over the %d sampled k-points" % (W.ncorr, P)
     return value, threads, desc
 
 
@@ -149,6 +166,10 @@ def build_workload(name, rank, world):
         return workloads.config1(nk=64, nt=200, ntau=100, kshift=shift)
     if name == "config1-ncu":  # config-1 chain at nt=ntau=300: 1.5 GB of G^tv history, > L2
         return workloads.config1(nk=256, nt=300, ntau=300, kshift=shift)
+    if name == "config4":
+        return workloads.config4(kshift=shift)
+    if name == "config4-small":  # 16x16 lattice, nt=400, ntau=200: quick checks of the lattice path
+        return workloads.config4(nkx=16, nky=16, nt=400, ntau=200, kshift=shift)
     raise SystemExit("unknown workload %s" % name)
 
 
@@ -233,9 +254,17 @@ def main():
     k = W.k
     nt = max(d["nt"] for d in W.descs)
 
+    if W.lattice:
+        # set-up (untimed): self-consistent bootstrap of steps 0..k
+        boot_iters, boot_err = b.lattice_2b_start(max_iter=30, tol=1e-12)
+
     def propagate():
-        for n in range(k + 1, nt + 1):
-            b.dyson_timestep(n)
+        if W.lattice:
+            for n in range(k + 1, nt + 1):
+                b.lattice_2b_timestep(n, W.ncorr)
+        else:
+            for n in range(k + 1, nt + 1):
+                b.dyson_timestep(n)
 
     for _ in range(args.warmup):
         propagate()
@@ -259,6 +288,8 @@ def main():
     units = world * W.kpt_steps() * args.steps
     value = units / (ms / 1000.0)
     kernels_per_step = 7  # prep_problem, prep_group, ret, mat_operator, tv, les_operands, les
+    if W.lattice:  # extrapolate + ncorr x (gloc, sigma_2b, Dyson step) + final gloc
+        kernels_per_step = 1 + W.ncorr * (2 + kernels_per_step) + 1
     gpu_launches = kernels_per_step * (nt - k) * args.steps
 
     # roofline of k_tv, the G^tv history stream: the largest single kernel in the serialised ncu
@@ -288,7 +319,7 @@ def main():
     if not args.no_e2e:
         from nessi_b200 import herm_matrix
         host = []
-        for d in W.descs:
+        for d in (W.descs[:1] if W.lattice else W.descs):
             host.append(herm_matrix(d["nt"], d["ntau"], d["size1"], d["sig"]))
         try:
             import torch as _t
@@ -303,22 +334,39 @@ def main():
         sig_bytes = sum(getattr(W.sigma, x).nbytes for x in ("ret", "les", "tv", "mat"))
         h2d = sig_bytes + W.H.nbytes + sum(B.mat.nbytes + sum(B.get_timestep(t).nbytes for t in range(k + 1))
                                            for B in W.boot)
-        d2h = sum(G.ret.nbytes + G.les.nbytes + G.tv.nbytes + G.mat.nbytes for G in host)
+        if W.lattice:
+            h2d += W.U.nbytes
+            # result of a lattice run: G_loc (all components) and the last time step of every G_k
+            d0 = W.descs[0]
+            gloc_host = host[0]
+            last = np.zeros((len(W.descs), 2 * (nt + 1) + d0["ntau"] + 1, d0["size1"], d0["size1"]), np.complex128)
+            d2h = sum(getattr(gloc_host, x).nbytes for x in ("ret", "les", "tv", "mat")) + last.nbytes
+        else:
+            d2h = sum(G.ret.nbytes + G.les.nbytes + G.tv.nbytes + G.mat.nbytes for G in host)
         barrier(world)
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
         for _ in range(args.steps):
             workloads.upload(b, W)
+            if W.lattice:
+                b.lattice_2b_start(max_iter=30, tol=1e-12)
             propagate()
-            for p, G in enumerate(host):
-                b.get_G(p, G)
+            if W.lattice:
+                b.get_gloc(0, gloc_host)
+                for p in range(len(W.descs)):
+                    b.get_timestep(p, nt, last[p])
+            else:
+                for p, G in enumerate(host):
+                    b.get_G(p, G)
         f1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
         ems = allmax(f0.elapsed_time(f1), world)
         e2e = {"value": units / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "pinned_host": pinned, "ms_per_step": ems / args.steps}
+        if W.lattice:
+            e2e["includes"] = "upload, self-consistent bootstrap, propagation, download of G_loc and G_k(nt)"
         # sanity: the downloaded result is finite
         if not all(np.isfinite(G.tv[nt]).all() for G in host[:4]):
             e2e["warning"] = "non-finite values in the result"
@@ -337,7 +385,9 @@ def main():
                 "config": dict(workload=args.workload, precision=args.precision,
                                l2="inputs larger than L2 (G^tv history %.1f GB per GPU)" % (
                                    16.0 * W.nprob * (nt + 1) * (W.descs[0]["ntau"] + 1) * W.descs[0]["size1"] ** 2 / 1e9),
-                               bootstrap="free propagator of H_k(-1) for mat and steps 0..k (set-up, untimed)",
+                               bootstrap=("free propagator of H_k(-1) for mat, then %d self-consistent "
+                                          "dyson_start iterations (set-up, untimed)" % boot_iters) if W.lattice else
+                               "free propagator of H_k(-1) for mat and steps 0..k (set-up, untimed)",
                                **W.info),
                 "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk}

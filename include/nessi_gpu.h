@@ -105,7 +105,8 @@ int nessi_gpu_set_stream(nessi_batch *b, void *stream);
 #define NESSI_KERNEL_GEMM 4          /* K_n G^mat, tv*vt and les*adv products (cuBLAS ZGEMM) */
 #define NESSI_KERNEL_LES 5           /* G^<(., n) Volterra recursion */
 #define NESSI_KERNEL_MATOP 6         /* Matsubara operator K_n of the tv row */
-#define NESSI_KERNEL_COUNT 7
+#define NESSI_KERNEL_LATTICE 7       /* predictor, G_loc and Sigma_2B of the lattice driver */
+#define NESSI_KERNEL_COUNT 8
 /* Turn timing on/off (resets counters).  No reference counterpart. */
 int nessi_gpu_set_profiling(nessi_batch *b, int on);
 /* Total device time (ms), launches and algorithmic bytes (flops for GEMM) recorded for one
@@ -128,6 +129,41 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
  * nothing left by an earlier call leaks into a result.  ntau must be even. */
 int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int solve_order, double beta, double mu, const void *H,
                                 const void *sigma_mat, void *gmat, void *stream);
+
+/* ---- self-consistent lattice (local self-energy recomputed from the k-average) --------
+ * The lattice drivers of the reference (examples/programs/hubbard_chain_2b.cpp:245-324,
+ * gw.cpp:386-420) gather every k-point's time step, form the local G_loc = (1/Nk) sum_k G_k,
+ * recompute the local self-energy from it and solve the Dyson equation of every k-point again,
+ * a few times per step.  Here a sigma_group is the set of k-points, its shared Sigma is the
+ * local self-energy, and all of it stays on the device. */
+
+/* Diagonal local interaction U(t) of a group, (nt+2) x size1 complex values, t = -1 first
+ * (the diagonal of the cntr::function U of hubbard_chain_2b.cpp:170; U(-1) is the value on the
+ * Matsubara branch).  Enables the Sigma_2B functions for the group. */
+int nessi_gpu_set_U(nessi_batch *b, int group, const void *U);
+/* cntr::extrapolate_timestep(n, G, SolveOrder) (cntr_utilities_decl.hpp:23,
+ * cntr_utilities_impl.hpp:22-130) for every problem with nt > n: polynomial extrapolation of
+ * time step n+1 from steps n-k..n.  n >= k. */
+int nessi_gpu_extrapolate_timestep(nessi_batch *b, int n);
+/* G_loc(tstp) = (1/P) sum_p G_p(tstp) over the P problems of the group that reach tstp
+ * (the k-sum of gw_kpoints_impl.cpp:139-180); tstp = -1 averages G^mat. */
+int nessi_gpu_gloc_timestep(nessi_batch *b, int group, int tstp);
+/* Sigma(tstp) = Sigma_2B[G_loc, U](tstp) of the group (hubbard_chain_selfen_impl.cpp:63-75:
+ * Polarization -> U(t) Pol U(t') -> Bubble2, cntr_bubble_impl.hpp:33-150), written into the
+ * group's Sigma; tstp = -1 gives Sigma^mat. */
+int nessi_gpu_sigma_2b_timestep(nessi_batch *b, int group, int tstp);
+/* Download G_loc / Sigma of a group (libcntr layout; NULL skips a component). */
+int nessi_gpu_get_gloc(nessi_batch *b, int group, void *ret, void *les, void *tv, void *mat);
+int nessi_gpu_get_sigma(nessi_batch *b, int group, void *ret, void *les, void *tv, void *mat);
+/* Bootstrap (hubbard_chain_2b.cpp:245-290 with G -> G_loc): iterate
+ *   Sigma(0..k) = Sigma_2B[G_loc];  dyson_start of every problem;  G_loc(0..k)
+ * until sum_t distance_norm2(t) between successive G_loc is below tol after more than 3
+ * iterations, or max_iter+1 iterations.  G must hold mat and an initial guess of steps 0..k. */
+int nessi_gpu_lattice_2b_start(nessi_batch *b, int max_iter, double tol, int *iters, double *err);
+/* One time step n > k (hubbard_chain_2b.cpp:306-324 with G -> G_loc): predictor
+ * extrapolate_timestep(n-1), then corrector_steps x [G_loc(n), Sigma_2B(n), dyson_timestep(n)],
+ * then G_loc(n) of the final G. */
+int nessi_gpu_lattice_2b_timestep(nessi_batch *b, int n, int corrector_steps);
 
 /* Wait for all work queued on the batch. */
 int nessi_gpu_synchronize(nessi_batch *b);

@@ -14,6 +14,7 @@
 #include "kernels_dyson.cuh"
 #include "kernels_start.cuh"
 #include "kernels_mat.cuh"
+#include "kernels_lattice.cuh"
 
 
 
@@ -94,6 +95,8 @@ struct Group {
     int dense_valid = -1, ret_valid = -1, les_valid = -1;
     bool gmat_valid = false;
     MatScratch *d_mat = nullptr;  // per-member scratch of dyson_mat (allocated on first use)
+    LocDev loc{nullptr, nullptr, nullptr, nullptr};  // G_loc of the group (allocated on first use)
+    double2 *U = nullptr;            // diagonal interaction U(t), (ntmax+2) x s, t = -1 first
     std::vector<int> members;        // problem indices, nt descending
     std::vector<ProbDev> h_probs;    // same order; col = position
     ProbDev *d_probs = nullptr;
@@ -349,6 +352,50 @@ template <int S> int mat_group(nessi_batch *b, Group &g) {
     return NESSI_OK;
 }
 
+// ---- lattice pieces: predictor, k-average, local second-order self-energy ---------------
+int active_members(const nessi_batch *b, const Group &g, int tstp) {
+    int nact = 0;
+    for (int i : g.members) nact += b->probs[i].d.nt >= tstp ? 1 : 0;
+    return nact;
+}
+
+template <int S> int extrap_group(nessi_batch *b, Group &g, int n) {
+    const long work = ((long)g.ntau + 1 + 2L * (n + 2)) * S * S;
+    dim3 grid((unsigned)std::min<long>((work + 255) / 256, 64), (unsigned)g.members.size());
+    k_extrapolate<S><<<grid, 256, 0, b->stream>>>(group_dev(g), g.d_probs, n);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+template <int S> int gloc_group(nessi_batch *b, Group &g, int tstp) {
+    const int nact = active_members(b, g, tstp);
+    if (nact == 0) { set_err("gloc: no problem of the group reaches time step %d", tstp); return NESSI_ERR_ARG; }
+    const long M = g.ntau + 1, s2 = (long)S * S;
+    const long total = tstp >= 0 ? (2L * (tstp + 1) + M) * s2 : M * s2;
+    k_gloc<S><<<(unsigned)((total + 31) / 32), dim3(32, 8), 0, b->stream>>>(group_dev(g), g.d_probs, nact, tstp,
+                                                                          g.loc);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+void sigma_changed(Group &g, int tstp) {
+    if (tstp < 0) return;  // Sigma^mat is read only by dyson_mat, which caches nothing
+    g.ret_valid = std::min(g.ret_valid, tstp - 1);
+    g.les_valid = std::min(g.les_valid, tstp - 1);
+    g.dense_valid = std::min(g.dense_valid, tstp - 1);
+}
+
+template <int S> int sigma2b_group(nessi_batch *b, Group &g, int tstp) {
+    const long M = g.ntau + 1, s2 = (long)S * S;
+    const long work = tstp >= 0 ? ((long)tstp + 1 + M) * s2 : M * s2;
+    SigOut o{g.sret, g.sles, g.stv, g.smat};
+    k_sigma_2b<S><<<(unsigned)std::min<long>((work + 255) / 256, 1184), 256, 0, b->stream>>>(group_dev(g), g.loc,
+                                                                                           g.U, tstp, o);
+    CK(cudaGetLastError());
+    sigma_changed(g, tstp);
+    return NESSI_OK;
+}
+
 #define NESSI_SIZE_SWITCH(fn, ...)                 \
     switch (g.s) {                                 \
         case 1: return fn<1>(__VA_ARGS__);         \
@@ -364,6 +411,9 @@ template <int S> int mat_group(nessi_batch *b, Group &g) {
     return NESSI_ERR_ARG;
 
 int start_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(start_group, b, g) }
+int extrap_dispatch(nessi_batch *b, Group &g, int n) { NESSI_SIZE_SWITCH(extrap_group, b, g, n) }
+int gloc_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(gloc_group, b, g, tstp) }
+int sigma2b_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(sigma2b_group, b, g, tstp) }
 int mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(mat_group, b, g) }
 
 int step_dispatch(nessi_batch *b, Group &g, int n, int nact) {
@@ -763,6 +813,194 @@ int nessi_gpu_dyson_start(nessi_batch *b) {
         CKR(refresh32(b, q.gtv32, q.gtv, (b->groups[q.group].k + 1) * row));
     }
     CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+static int find_group_checked(nessi_batch *b, int group, Group **out) {
+    CKR(check_batch(b));
+    int gi = find_group(b, group);
+    if (gi < 0) { set_err("unknown sigma_group %d", group); return NESSI_ERR_ARG; }
+    *out = &b->groups[gi];
+    return NESSI_OK;
+}
+
+static int ensure_loc(nessi_batch *b, Group &g) {
+    if (g.loc.ret) return NESSI_OK;
+    const long s2 = (long)g.s * g.s, N = g.ntmax + 1, M = g.ntau + 1;
+    CKR(b->alloc(&g.loc.ret, tri_h(N) * s2));
+    CKR(b->alloc(&g.loc.les, tri_h(N) * s2));
+    CKR(b->alloc(&g.loc.tv, N * M * s2));
+    CKR(b->alloc(&g.loc.mat, M * s2));
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_U(nessi_batch *b, int group, const void *U) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    if (!U) { set_err("null U"); return NESSI_ERR_ARG; }
+    CKR(ensure_loc(b, *g));
+    if (!g->U) CKR(b->alloc(&g->U, (long)(g->ntmax + 2) * g->s));
+    CKR(copy_cplx(b, g->U, U, (long)(g->ntmax + 2) * g->s, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_extrapolate_timestep(nessi_batch *b, int n) {
+    CKR(check_batch(b));
+    for (Group &g : b->groups)
+        if (n < g.k) { set_err("extrapolate_timestep: n = %d below the solve order %d", n, g.k); return NESSI_ERR_ARG; }
+    b->prof_mark(NESSI_KERNEL_LATTICE);
+    for (Group &g : b->groups) {
+        if (active_members(b, g, n + 1) == 0) continue;
+        CKR(extrap_dispatch(b, g, n));
+    }
+    b->prof_end(NESSI_KERNEL_LATTICE, 0.0);
+    return NESSI_OK;
+}
+
+int nessi_gpu_gloc_timestep(nessi_batch *b, int group, int tstp) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    if (tstp < -1 || tstp > g->ntmax) { set_err("gloc: time step %d out of range", tstp); return NESSI_ERR_ARG; }
+    CKR(ensure_loc(b, *g));
+    b->prof_mark(NESSI_KERNEL_LATTICE);
+    CKR(gloc_dispatch(b, *g, tstp));
+    b->prof_end(NESSI_KERNEL_LATTICE, 0.0);
+    return NESSI_OK;
+}
+
+int nessi_gpu_sigma_2b_timestep(nessi_batch *b, int group, int tstp) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    if (!g->U) { set_err("sigma_2b: nessi_gpu_set_U was not called for group %d", group); return NESSI_ERR_ARG; }
+    if (tstp < -1 || tstp > g->ntmax) { set_err("sigma_2b: time step %d out of range", tstp); return NESSI_ERR_ARG; }
+    b->prof_mark(NESSI_KERNEL_LATTICE);
+    CKR(sigma2b_dispatch(b, *g, tstp));
+    b->prof_end(NESSI_KERNEL_LATTICE, 0.0);
+    return NESSI_OK;
+}
+
+int nessi_gpu_get_gloc(nessi_batch *b, int group, void *ret, void *les, void *tv, void *mat) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    CKR(ensure_loc(b, *g));
+    const long s2 = (long)g->s * g->s, N = g->ntmax + 1, M = g->ntau + 1;
+    CKR(copy_cplx(b, ret, g->loc.ret, tri_h(N) * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, les, g->loc.les, tri_h(N) * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, tv, g->loc.tv, N * M * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, mat, g->loc.mat, M * s2, cudaMemcpyDeviceToHost));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_get_sigma(nessi_batch *b, int group, void *ret, void *les, void *tv, void *mat) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    const long s2 = (long)g->s * g->s, N = g->ntmax + 1, M = g->ntau + 1;
+    CKR(copy_cplx(b, ret, g->sret, tri_h(N) * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, les, g->sles, tri_h(N) * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, tv, g->stv, N * M * s2, cudaMemcpyDeviceToHost));
+    CKR(copy_cplx(b, mat, g->smat, M * s2, cudaMemcpyDeviceToHost));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+// distance_norm2 of time step t between two herm_matrix_timestep-like host buffers (ret row,
+// tv row, les column of t; cntr_utilities_impl.hpp:607-650)
+static double slice_distance(const double2 *a, const double2 *b, long n_elem, int s2) {
+    double err = 0;
+    for (long e = 0; e < n_elem; e++) {
+        double r = 0;
+        for (int i = 0; i < s2; i++) {
+            const double dx = a[e * s2 + i].x - b[e * s2 + i].x, dy = a[e * s2 + i].y - b[e * s2 + i].y;
+            r += dx * dx + dy * dy;
+        }
+        err += std::sqrt(r);
+    }
+    return err;
+}
+
+int nessi_gpu_lattice_2b_start(nessi_batch *b, int max_iter, double tol, int *iters, double *err_out) {
+    CKR(check_batch(b));
+    if (max_iter < 0) { set_err("lattice_2b_start: max_iter < 0"); return NESSI_ERR_ARG; }
+    std::vector<Group *> lat;
+    for (Group &g : b->groups)
+        if (g.U) lat.push_back(&g);
+    if (lat.empty()) { set_err("lattice_2b_start: no group has an interaction (nessi_gpu_set_U)"); return NESSI_ERR_ARG; }
+    // G_loc slices 0..k of every lattice group, downloaded after each iteration
+    auto snapshot = [&](std::vector<std::vector<double2>> &out) -> int {
+        out.resize(lat.size());
+        for (size_t i = 0; i < lat.size(); i++) {
+            Group &g = *lat[i];
+            const long s2 = (long)g.s * g.s, M = g.ntau + 1, tk = tri_h(g.k + 1) * s2;
+            out[i].resize(2 * tk + (g.k + 1) * M * s2);
+            CKR(copy_cplx(b, out[i].data(), g.loc.ret, tk, cudaMemcpyDeviceToHost));
+            CKR(copy_cplx(b, out[i].data() + tk, g.loc.les, tk, cudaMemcpyDeviceToHost));
+            CKR(copy_cplx(b, out[i].data() + 2 * tk, g.loc.tv, (g.k + 1) * M * s2, cudaMemcpyDeviceToHost));
+        }
+        CK(cudaStreamSynchronize(b->stream));
+        return NESSI_OK;
+    };
+    auto distance = [&](const std::vector<std::vector<double2>> &x, const std::vector<std::vector<double2>> &y) {
+        double e = 0;
+        for (size_t i = 0; i < lat.size(); i++) {
+            const Group &g = *lat[i];
+            const int s2 = g.s * g.s;
+            const long M = g.ntau + 1, tk = tri_h(g.k + 1) * s2;
+            for (int t = 0; t <= g.k; t++) {
+                e += slice_distance(x[i].data() + tri_h(t) * s2, y[i].data() + tri_h(t) * s2, t + 1, s2);
+                e += slice_distance(x[i].data() + 2 * tk + t * M * s2, y[i].data() + 2 * tk + t * M * s2, M, s2);
+                e += slice_distance(x[i].data() + tk + tri_h(t) * s2, y[i].data() + tk + tri_h(t) * s2, t + 1, s2);
+            }
+        }
+        return e;
+    };
+    for (Group *g : lat)
+        for (int t = 0; t <= g->k; t++) CKR(gloc_dispatch(b, *g, t));
+    std::vector<std::vector<double2>> prev, cur;
+    CKR(snapshot(prev));
+    int iter = 0;
+    double err = 0;
+    for (iter = 0; iter <= max_iter; iter++) {
+        for (Group *g : lat)
+            for (int t = 0; t <= g->k; t++) CKR(sigma2b_dispatch(b, *g, t));
+        CKR(nessi_gpu_dyson_start(b));
+        for (Group *g : lat)
+            for (int t = 0; t <= g->k; t++) CKR(gloc_dispatch(b, *g, t));
+        CKR(snapshot(cur));
+        err = distance(cur, prev);
+        if (err < tol && iter > 2) break;
+        prev.swap(cur);
+    }
+    if (iters) *iters = iter > max_iter ? max_iter + 1 : iter + 1;
+    if (err_out) *err_out = err;
+    return NESSI_OK;
+}
+
+int nessi_gpu_lattice_2b_timestep(nessi_batch *b, int n, int corrector_steps) {
+    CKR(check_batch(b));
+    if (corrector_steps < 1) { set_err("lattice_2b_timestep: corrector_steps must be >= 1"); return NESSI_ERR_ARG; }
+    bool any = false;
+    for (Group &g : b->groups) {
+        if (n <= g.k) { set_err("lattice_2b_timestep: n = %d must exceed the solve order %d", n, g.k); return NESSI_ERR_ARG; }
+        any = any || g.U != nullptr;
+    }
+    if (!any) { set_err("lattice_2b_timestep: no group has an interaction (nessi_gpu_set_U)"); return NESSI_ERR_ARG; }
+    CKR(nessi_gpu_extrapolate_timestep(b, n - 1));
+    for (int it = 0; it < corrector_steps; it++) {
+        b->prof_mark(NESSI_KERNEL_LATTICE);
+        for (Group &g : b->groups) {
+            if (!g.U || active_members(b, g, n) == 0) continue;
+            CKR(gloc_dispatch(b, g, n));
+            CKR(sigma2b_dispatch(b, g, n));
+        }
+        b->prof_end(NESSI_KERNEL_LATTICE, 0.0);
+        CKR(nessi_gpu_dyson_timestep(b, n));
+    }
+    b->prof_mark(NESSI_KERNEL_LATTICE);
+    for (Group &g : b->groups)
+        if (g.U && active_members(b, g, n) > 0) CKR(gloc_dispatch(b, g, n));
+    b->prof_end(NESSI_KERNEL_LATTICE, 0.0);
     return NESSI_OK;
 }
 

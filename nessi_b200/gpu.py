@@ -60,12 +60,21 @@ EXPORTS = {
     "nessi_gpu_dyson_mat_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p]),
+    "nessi_gpu_set_U": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "nessi_gpu_extrapolate_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "nessi_gpu_gloc_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "nessi_gpu_sigma_2b_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "nessi_gpu_get_gloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_get_sigma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_lattice_2b_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    "nessi_gpu_lattice_2b_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
 }
 
-KERNELS = ["prep", "ret", "tv", "les_operands", "gemm", "les", "matop"]
+KERNELS = ["prep", "ret", "tv", "les_operands", "gemm", "les", "matop", "lattice"]
 
 
 def load_library(path=None):
@@ -172,6 +181,36 @@ class Batch:
 
     def synchronize(self):
         _check(load_library().nessi_gpu_synchronize(self._h))
+
+    # ---- self-consistent lattice ----------------------------------------------------
+    def set_U(self, group, U):
+        """Diagonal local interaction of a group: array (nt+2, size1), t = -1 first."""
+        _check(load_library().nessi_gpu_set_U(self._h, group, _ptr(np.ascontiguousarray(U, np.complex128))))
+
+    def extrapolate_timestep(self, n):
+        """cntr::extrapolate_timestep(n, G, SolveOrder) of every problem: step n+1 from n-k..n."""
+        _check(load_library().nessi_gpu_extrapolate_timestep(self._h, n))
+
+    def gloc_timestep(self, group, tstp):
+        _check(load_library().nessi_gpu_gloc_timestep(self._h, group, tstp))
+
+    def sigma_2b_timestep(self, group, tstp):
+        _check(load_library().nessi_gpu_sigma_2b_timestep(self._h, group, tstp))
+
+    def get_gloc(self, group, G):
+        _check(load_library().nessi_gpu_get_gloc(self._h, group, _ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
+
+    def get_sigma(self, group, S):
+        _check(load_library().nessi_gpu_get_sigma(self._h, group, _ptr(S.ret), _ptr(S.les), _ptr(S.tv), _ptr(S.mat)))
+
+    def lattice_2b_start(self, max_iter=20, tol=1e-12):
+        """Bootstrap of the lattice; returns (iterations, last distance)."""
+        it, err = ctypes.c_int(), ctypes.c_double()
+        _check(load_library().nessi_gpu_lattice_2b_start(self._h, max_iter, tol, ctypes.byref(it), ctypes.byref(err)))
+        return it.value, err.value
+
+    def lattice_2b_timestep(self, n, corrector_steps=3):
+        _check(load_library().nessi_gpu_lattice_2b_timestep(self._h, n, corrector_steps))
 
     def set_stream(self, stream_handle):
         """Use a caller-owned cudaStream_t (an int handle, e.g. torch.cuda.Stream().cuda_stream)."""

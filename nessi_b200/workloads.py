@@ -12,6 +12,10 @@ chain2 (2-band chain, size1 = 2, Nk k-points in [-pi, pi)):
     201 levels), shared by all k.
 chain4 (4-band chain, size1 = 4): diagonal -2cos(k - A) + eps_a, eps = (-1.5, -0.5, 0.5, 1.5),
     nearest-band hoppings 0.3, same Sigma (x) 1_4.
+lattice2b (square lattice, size1 = 1, nkx x nky k-points in [-pi, pi)^2):
+    eps_k = -2(cos kx + cos ky), mu = 0 (half filling), free equilibrium (U = 0 on the Matsubara
+    branch), U(t) = min(t, 2) switched on at t = 0; Sigma = Sigma_2B[G_loc, U] recomputed from the
+    k-average every corrector iteration.
 """
 import numpy as np
 
@@ -20,6 +24,10 @@ from .herm_matrix import herm_matrix
 
 
 class Workload:
+    lattice = False  # True: Sigma_2B of G_loc, recomputed each step (U, ncorr set)
+    U = None
+    ncorr = 0
+
     def __init__(self, name, descs, sigma, H, boot, k, info):
         self.name = name
         self.descs = descs          # list of batch descriptors
@@ -102,6 +110,41 @@ def config2(nk=512, nt=4000, ntau=800, kshift=0.0):
     return chain(nk, nt, ntau, 20.0, 0.01, 4, kshift=kshift)
 
 
+def lattice2b(nkx, nky, nt, ntau, beta, h, u_max=2.0, t_ramp=2.0, ncorr=3, k=5, kshift=0.0):
+    """Self-consistent square lattice with the local second-order self-energy."""
+    kx = -np.pi + 2 * np.pi * np.arange(nkx) / nkx + kshift
+    ky = -np.pi + 2 * np.pi * np.arange(nky) / nky
+    eps = np.array([-2.0 * (np.cos(a) + np.cos(b)) for a in kx for b in ky])
+    nk = len(eps)
+    H = np.zeros((nk, nt + 2, 1, 1), np.complex128)
+    H[:, :, 0, 0] = eps[:, None]
+    sigma = herm_matrix(nt, ntau, 1, -1)
+    boot, cache = [], {}
+    for i in range(nk):
+        key = round(float(eps[i]), 14)
+        if key not in cache:
+            cache[key] = bootstrap_free(H[i, 0], 0.0, beta, h, k, ntau)
+        boot.append(cache[key])
+    descs = [dict(nt=nt, ntau=ntau, size1=1, sig=-1, solve_order=k, sigma_group=0, beta=beta, h=h, mu=0.0)
+             for _ in range(nk)]
+    info = dict(model="square lattice, local Sigma_2B[G_loc]", size1=1, nk=nk, nkx=nkx, nky=nky, nt=nt, ntau=ntau,
+                beta=beta, h=h, solve_order=k, correctors=ncorr,
+                sigma="U(t)U(t') G_loc(t,t')^2 G_loc(t',t), U(t) = %g min(t/%g, 1), U = 0 on the Matsubara branch"
+                      % (u_max, t_ramp))
+    W = Workload("lattice2b", descs, sigma, H, boot, k, info)
+    W.lattice = True
+    W.ncorr = ncorr
+    U = np.zeros((nt + 2, 1), np.complex128)
+    U[1:, 0] = u_max * np.minimum(np.arange(nt + 1) * h / t_ramp, 1.0)
+    W.U = U
+    return W
+
+
+def config4(nkx=32, nky=32, nt=2000, ntau=800, kshift=0.0):
+    """32x32 square lattice, size1 = 1, nt = 2000, ntau = 800, beta = 20, h = 0.01, 3 correctors."""
+    return lattice2b(nkx, nky, nt, ntau, 20.0, 0.01, kshift=kshift)
+
+
 def upload(batch, W):
     """Copy Sigma, H and the bootstrap steps of a workload into a gpu.Batch."""
     batch.set_sigma(0, W.sigma)
@@ -111,3 +154,5 @@ def upload(batch, W):
         batch.set_timestep(p, -1, B.mat)
         for t in range(W.k + 1):
             batch.set_timestep(p, t, B.get_timestep(t))
+    if W.lattice:
+        batch.set_U(0, W.U)

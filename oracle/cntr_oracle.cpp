@@ -1696,4 +1696,188 @@ void orc_dyson_timestep_batch(int n0, int n1, int nprob, orc_hm *G, double mu, c
     (void)nthreads;
 }
 
+// ------------------------------------------------------------------------------------
+// Self-consistent lattice with a local second-order self-energy
+// ------------------------------------------------------------------------------------
+// Sigma_2B at one time step (examples/programs/hubbard_chain_selfen_impl.cpp:63-75):
+//   Pol_ij = -Bubble1(G_ij, G_ij)              (Polarization, :25-34)
+//   Pol   <- U(t) Pol U(t')                    (herm_matrix_timestep::right_multiply then
+//                                               left_multiply, cntr_herm_matrix_timestep_impl.hpp:1570-1860)
+//   Sigma_ij = Bubble2(G_ij, Pol_ij)           (cntr_bubble_impl.hpp:100-150)
+// with Bubble1(c,a,b) = i A_{a1a2}(t,t') B_{b2b1}(t',t), Bubble2 = i A_{a1a2}(t,t') B_{b1b2}(t,t')
+// (get_bubble_1_timestep / get_bubble_2_timestep, cntr_bubble_impl.hpp:33-150).  U holds (nt+2)
+// s x s blocks, U(-1) first (cntr::function layout); tstp = -1 gives Sigma^mat.
+void orc_sigma_2b_timestep(int tstp, orc_hm *Sh, orc_hm *Gh, const cplx *U) {
+    HM S(Sh), G(Gh);
+    const int s = G.s, es = G.es, ntau = G.ntau();
+    const cplx ii(0.0, 1.0);
+    const cplx *U0 = U;           // U(-1)
+    auto Ut = [&](int t) { return U + (long)(t + 1) * es; };
+    auto mm = [&](const cplx *a, const cplx *b, cplx *c) {  // c = a b (element_mult)
+        for (int i = 0; i < s; i++)
+            for (int j = 0; j < s; j++) {
+                cplx x = 0;
+                for (int l = 0; l < s; l++) x += a[i * s + l] * b[l * s + j];
+                c[i * s + j] = x;
+            }
+    };
+    std::vector<cplx> tmp(es);
+    if (tstp == -1) {
+        std::vector<cplx> pm((long)(ntau + 1) * es);
+        const double sg = -1.0 * G.sig();
+        for (int i = 0; i < s; i++)
+            for (int j = 0; j < s; j++)
+                for (int m = 0; m <= ntau; m++)
+                    pm[(long)m * es + i * s + j] = -(sg * G.matptr(m)[i * s + j] * G.matptr(ntau - m)[j * s + i]);
+        for (int m = 0; m <= ntau; m++) {
+            mm(pm.data() + (long)m * es, U0, tmp.data());
+            mm(U0, tmp.data(), pm.data() + (long)m * es);
+        }
+        for (int i = 0; i < s; i++)
+            for (int j = 0; j < s; j++)
+                for (int m = 0; m <= ntau; m++)
+                    S.matptr(m)[i * s + j] = -G.matptr(m)[i * s + j] * pm[(long)m * es + i * s + j];
+        return;
+    }
+    const int n = tstp;
+    std::vector<cplx> pret((long)(n + 1) * es), ples((long)(n + 1) * es), ptv((long)(ntau + 1) * es);
+    for (int i = 0; i < s; i++)
+        for (int j = 0; j < s; j++) {
+            const int a12 = i * s + j, a21 = j * s + i;
+            for (int m = 0; m <= n; m++) {
+                const cplx *gr = G.retptr(n, m), *gl = G.lesptr(m, n);
+                cplx bles21_tt1 = -std::conj(gl[a12]);
+                cplx bgtr21_tt1 = gr[a21] + bles21_tt1;
+                cplx bles21_t1t = gl[a21];
+                cplx bgtr21_t1t = -std::conj(gr[a12]) + bles21_t1t;
+                cplx ales12_tt1 = -std::conj(gl[a21]);
+                cplx agtr12_tt1 = gr[a12] + ales12_tt1;
+                cplx cgtr = ii * agtr12_tt1 * bles21_t1t;
+                cplx cles = ii * ales12_tt1 * bgtr21_t1t;
+                pret[(long)m * es + a12] = -(cgtr - cles);
+                ples[(long)m * es + a12] = -(ii * gl[a12] * bgtr21_tt1);
+            }
+            const cplx msigb = -1.0 * G.sig();
+            for (int m = 0; m <= ntau; m++) {
+                cplx bvt21 = msigb * std::conj(G.tvptr(n, ntau - m)[a12]);
+                ptv[(long)m * es + a12] = -(ii * G.tvptr(n, m)[a12] * bvt21);
+            }
+        }
+    // right_multiply(tstp, U): ret(n,m) U(m), tv U(-1), les(m,n) U(n); then left_multiply:
+    // U(n) ret(n,m), U(n) tv, U(m) les(m,n)
+    for (int m = 0; m <= n; m++) {
+        mm(pret.data() + (long)m * es, Ut(m), tmp.data());
+        mm(Ut(n), tmp.data(), pret.data() + (long)m * es);
+        mm(ples.data() + (long)m * es, Ut(n), tmp.data());
+        mm(Ut(m), tmp.data(), ples.data() + (long)m * es);
+    }
+    for (int m = 0; m <= ntau; m++) {
+        mm(ptv.data() + (long)m * es, U0, tmp.data());
+        mm(Ut(n), tmp.data(), ptv.data() + (long)m * es);
+    }
+    for (int i = 0; i < s; i++)
+        for (int j = 0; j < s; j++) {
+            const int a12 = i * s + j, a21 = j * s + i;
+            for (int m = 0; m <= n; m++) {
+                const cplx *gr = G.retptr(n, m), *gl = G.lesptr(m, n);
+                const cplx *br = pret.data() + (long)m * es, *bl = ples.data() + (long)m * es;
+                cplx bgtr12 = br[a12] - std::conj(bl[a21]);
+                cplx agtr12 = gr[a12] - std::conj(gl[a21]);
+                cplx cgtr = ii * agtr12 * bgtr12;
+                cplx cles = ii * std::conj(gl[a21]) * std::conj(bl[a21]);
+                S.retptr(n, m)[a12] = cgtr - cles;
+                S.lesptr(m, n)[a12] = ii * gl[a12] * bl[a12];
+            }
+            for (int m = 0; m <= ntau; m++) S.tvptr(n, m)[a12] = ii * G.tvptr(n, m)[a12] * ptv[(long)m * es + a12];
+        }
+}
+
+// G_loc(tstp) = (1/nprob) sum_p G_p(tstp): the k-average of the lattice drivers
+// (examples/programs/gw_kpoints_impl.cpp:139-180 gathers the k slices and sums them).
+void orc_gloc_timestep(int tstp, int nprob, orc_hm *G, orc_hm *Gloch) {
+    HM L(Gloch);
+    const int es = L.es, ntau = L.ntau();
+    const double w = 1.0 / nprob;
+    auto avg = [&](auto ptr_of) {
+        cplx *dst = ptr_of(L);
+        for (int e = 0; e < es; e++) {
+            cplx acc = 0;
+            for (int p = 0; p < nprob; p++) {
+                HM Gp(&G[p]);
+                acc += ptr_of(Gp)[e];
+            }
+            dst[e] = acc * w;
+        }
+    };
+    if (tstp == -1) {
+        for (int m = 0; m <= ntau; m++) avg([&](const HM &X) { return X.matptr(m); });
+        return;
+    }
+    for (int m = 0; m <= tstp; m++) {
+        avg([&](const HM &X) { return X.retptr(tstp, m); });
+        avg([&](const HM &X) { return X.lesptr(m, tstp); });
+    }
+    for (int m = 0; m <= ntau; m++) avg([&](const HM &X) { return X.tvptr(tstp, m); });
+}
+
+// Bootstrap of the lattice (examples/programs/hubbard_chain_2b.cpp:245-290 with G -> G_loc):
+// per iteration Sigma(0..k) = Sigma_2B[G_loc, U], dyson_start of every problem, G_loc(0..k),
+// err = sum_t distance_norm2(t, G_loc, previous G_loc); stop once err < tol and iter > 2.
+// Returns the number of iterations run; *err_out is the last err.
+int orc_lattice2b_start(int nprob, orc_hm *G, orc_hm *Gloc, orc_hm *Sigma, const cplx *U, double mu,
+                        const cplx *H, long h_stride, int k, double beta, double h, int max_iter, double tol,
+                        double *err_out, int nthreads) {
+    integ_init_all();
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    HM L(Gloc);
+    for (int t = 0; t <= k; t++) orc_gloc_timestep(t, nprob, G, Gloc);
+    // previous G_loc slices 0..k, in a herm_matrix of nt = k
+    std::vector<cplx> pr((long)(k + 1) * (k + 2) / 2 * L.es), pl(pr.size()), ptv((long)(k + 1) * (L.ntau() + 1) * L.es);
+    orc_hm prev = {k, L.ntau(), L.s, L.sig(), pr.data(), pl.data(), ptv.data(), nullptr};
+    auto save = [&]() {
+        std::memcpy(pr.data(), Gloc->ret, pr.size() * sizeof(cplx));
+        std::memcpy(pl.data(), Gloc->les, pl.size() * sizeof(cplx));
+        std::memcpy(ptv.data(), Gloc->tv, ptv.size() * sizeof(cplx));
+    };
+    save();
+    int iter = 0;
+    double err = 0;
+    for (iter = 0; iter <= max_iter; iter++) {
+        for (int t = 0; t <= k; t++) orc_sigma_2b_timestep(t, Sigma, Gloc, U);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+        for (int p = 0; p < nprob; p++) orc_dyson_start(&G[p], mu, H + (long)p * h_stride, Sigma, k, beta, h);
+        for (int t = 0; t <= k; t++) orc_gloc_timestep(t, nprob, G, Gloc);
+        err = 0;
+        for (int t = 0; t <= k; t++) err += orc_distance_norm2(t, Gloc, &prev);
+        if (err < tol && iter > 2) break;
+        save();
+    }
+    if (err_out) *err_out = err;
+    (void)nthreads;
+    return iter > max_iter ? max_iter + 1 : iter + 1;
+}
+
+// One time step of the lattice (examples/programs/hubbard_chain_2b.cpp:306-324 with G -> G_loc):
+// predictor extrapolate_timestep(n-1) of every problem, then ncorr x [G_loc(n), Sigma_2B(n),
+// dyson_timestep(n) of every problem], then G_loc(n) of the final G.
+void orc_lattice2b_timestep(int n, int nprob, orc_hm *G, orc_hm *Gloc, orc_hm *Sigma, const cplx *U, double mu,
+                            const cplx *H, long h_stride, int k, double beta, double h, int ncorr, int nthreads) {
+    integ_init_all();
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int p = 0; p < nprob; p++) orc_extrapolate_timestep(n - 1, &G[p], k);
+    for (int it = 0; it < ncorr; it++) {
+        orc_gloc_timestep(n, nprob, G, Gloc);
+        orc_sigma_2b_timestep(n, Sigma, Gloc, U);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+        for (int p = 0; p < nprob; p++) orc_dyson_timestep(n, &G[p], mu, H + (long)p * h_stride, Sigma, k, beta, h);
+    }
+    orc_gloc_timestep(n, nprob, G, Gloc);
+    (void)nthreads;
+}
+
 }  // extern "C"

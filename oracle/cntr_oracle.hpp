@@ -73,6 +73,17 @@ void orc_force_matsubara_hermitian(orc_hm *G);
 void orc_bubble1_scalar(int tstp, orc_hm *C, orc_hm *A, orc_hm *Acc, orc_hm *B, orc_hm *Bcc);
 void orc_bubble2_scalar(int tstp, orc_hm *C, orc_hm *A, orc_hm *Acc, orc_hm *B, orc_hm *Bcc);
 
+// Self-consistent lattice with a local second-order self-energy (examples/programs/
+// hubbard_chain_selfen_impl.cpp:63-75, hubbard_chain_2b.cpp:245-324, with G -> G_loc, the
+// k-average of the problems' G).  U holds (nt+2) s x s blocks, U(-1) first.
+void orc_sigma_2b_timestep(int tstp, orc_hm *Sigma, orc_hm *G, const ocplx *U);
+void orc_gloc_timestep(int tstp, int nprob, orc_hm *G, orc_hm *Gloc);
+int orc_lattice2b_start(int nprob, orc_hm *G, orc_hm *Gloc, orc_hm *Sigma, const ocplx *U, double mu,
+                        const ocplx *H, long h_stride, int k, double beta, double h, int max_iter, double tol,
+                        double *err_out, int nthreads);
+void orc_lattice2b_timestep(int n, int nprob, orc_hm *G, orc_hm *Gloc, orc_hm *Sigma, const ocplx *U, double mu,
+                            const ocplx *H, long h_stride, int k, double beta, double h, int ncorr, int nthreads);
+
 // Batched driver used as the CPU baseline: Dyson time steps n0..n1 (inclusive) for
 // nprob problems that share one Sigma, distributed over nthreads OpenMP threads
 // (the "OpenMP over k" harness of the reference's lattice driver, gw.cpp:386-420).

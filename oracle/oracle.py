@@ -64,6 +64,11 @@ def lib():
             "orc_bubble1_scalar": (None, [i, P, P, P, P, P]),
             "orc_bubble2_scalar": (None, [i, P, P, P, P, P]),
             "orc_dyson_timestep_batch": (None, [i, i, i, P, d, vp, ctypes.c_long, P, i, d, d, i]),
+            "orc_sigma_2b_timestep": (None, [i, P, P, vp]),
+            "orc_gloc_timestep": (None, [i, i, P, P]),
+            "orc_lattice2b_start": (i, [i, P, P, P, vp, d, vp, ctypes.c_long, i, d, d, i, d,
+                                        ctypes.POINTER(ctypes.c_double), i]),
+            "orc_lattice2b_timestep": (None, [i, i, P, P, P, vp, d, vp, ctypes.c_long, i, d, d, i, i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -218,3 +223,45 @@ def dyson_timestep_batch(n0, n1, Gs, mu, Hs, Sigma, beta, h, k=5, nthreads=0):
     s = hm(Sigma)
     lib().orc_dyson_timestep_batch(n0, n1, len(Gs), arr, mu, Ha.ctypes.data, stride, ctypes.byref(s), k, beta, h,
                                    nthreads)
+
+
+def _U(U):
+    a = np.ascontiguousarray(U, np.complex128)
+    return a, a.ctypes.data
+
+
+def sigma_2b_timestep(tstp, Sigma, G, U):
+    """Sigma(tstp) = Sigma_2B[G, U] (hubbard_chain_selfen_impl.cpp:63-75).  ``U`` is an
+    (nt+2, s, s) array, U(-1) first."""
+    s, g = hm(Sigma), hm(G)
+    Ua, up = _U(U)
+    lib().orc_sigma_2b_timestep(tstp, ctypes.byref(s), ctypes.byref(g), up)
+
+
+def gloc_timestep(tstp, Gs, Gloc):
+    arr = (_OrcHM * len(Gs))(*[hm(G) for G in Gs])
+    l = hm(Gloc)
+    lib().orc_gloc_timestep(tstp, len(Gs), arr, ctypes.byref(l))
+
+
+def lattice2b_start(Gs, Gloc, Sigma, U, mu, Hs, beta, h, k=5, max_iter=20, tol=1e-12, nthreads=0):
+    """Bootstrap of the lattice (hubbard_chain_2b.cpp:245-290 with G -> G_loc).
+    Returns (iterations, last error)."""
+    arr = (_OrcHM * len(Gs))(*[hm(G) for G in Gs])
+    Ha = np.ascontiguousarray(Hs, np.complex128)
+    Ua, up = _U(U)
+    l, s = hm(Gloc), hm(Sigma)
+    err = ctypes.c_double()
+    it = lib().orc_lattice2b_start(len(Gs), arr, ctypes.byref(l), ctypes.byref(s), up, mu, Ha.ctypes.data,
+                                   Ha[0].size, k, beta, h, max_iter, tol, ctypes.byref(err), nthreads)
+    return it, err.value
+
+
+def lattice2b_timestep(n, Gs, Gloc, Sigma, U, mu, Hs, beta, h, k=5, ncorr=3, nthreads=0):
+    """One lattice time step: predictor + ncorr x [G_loc, Sigma_2B, dyson_timestep]."""
+    arr = (_OrcHM * len(Gs))(*[hm(G) for G in Gs])
+    Ha = np.ascontiguousarray(Hs, np.complex128)
+    Ua, up = _U(U)
+    l, s = hm(Gloc), hm(Sigma)
+    lib().orc_lattice2b_timestep(n, len(Gs), arr, ctypes.byref(l), ctypes.byref(s), up, mu, Ha.ctypes.data,
+                                 Ha[0].size, k, beta, h, ncorr, nthreads)

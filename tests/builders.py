@@ -63,3 +63,31 @@ def component_errors(Gg, Go, n0, n1):
     out["les"] = rel_err(np.concatenate(lr), np.concatenate(lo))
     out["tv"] = rel_err(Gg.tv[n0:n1 + 1], Go.tv[n0:n1 + 1])
     return out
+
+
+def make_lattice(O, nkx, nky, nt, ntau, beta, h, u_max, t_ramp, u_mat=0.0, mu=0.0):
+    """Square-lattice k-points eps_k = -2(cos kx + cos ky) (size1 = 1) with free initial G_k
+    (green_from_H) and a linear ramp U(t) = u_max min(t h / t_ramp, 1), U(-1) = u_mat.
+    Returns (Gs, Hs, U) with Hs of shape (nk, nt+2, 1, 1) and U of shape (nt+2, 1)."""
+    ks = [(2 * np.pi * i / nkx - np.pi, 2 * np.pi * j / nky - np.pi) for i in range(nkx) for j in range(nky)]
+    Gs, Hs = [], []
+    for kx, ky in ks:
+        e = -2.0 * (np.cos(kx) + np.cos(ky))
+        G = herm_matrix(nt, ntau, 1, -1)
+        O.green_from_H(G, mu, np.array([[e]]), beta, h)
+        Gs.append(G)
+        Hs.append(np.full((nt + 2, 1, 1), e, np.complex128))
+    U = np.zeros((nt + 2, 1), np.complex128)
+    U[0, 0] = u_mat
+    for t in range(nt + 1):
+        U[t + 1, 0] = u_max * min(t * h / t_ramp, 1.0)
+    return Gs, np.array(Hs), U
+
+
+def u_matrices(U):
+    """(nt+2, s) diagonal values -> (nt+2, s, s) cntr::function blocks for the oracle."""
+    nt2, s = U.shape
+    out = np.zeros((nt2, s, s), np.complex128)
+    for i in range(s):
+        out[:, i, i] = U[:, i]
+    return out
