@@ -93,6 +93,27 @@ int nessi_gpu_dyson_start(nessi_batch *b);
  * G must hold time steps 0..n-1 and mat; Sigma and H must hold 0..n. */
 int nessi_gpu_dyson_timestep(nessi_batch *b, int n);
 
+/* ---- VIE2: [1 + F] G = Q (cntr_vie2_decl.hpp:63-90) ---------------------------------------
+ * A group becomes a VIE2 group when its kernel F is set: F (and its hermitian-conjugate partner
+ * Fcc, which the retarded and lesser parts need where F is not hermitian) are shared by the
+ * group, Q is per problem.  dyson_* calls act on Dyson groups only and vie2_* calls on VIE2
+ * groups only, so one batch may hold both kinds.  G^mat of a VIE2 problem is the caller's
+ * (set_G / set_timestep(-1)). */
+/* F and Fcc of a group (herm_matrix layout; Fcc's ret and les only). */
+int nessi_gpu_set_F(nessi_batch *b, int group, const void *ret, const void *les, const void *tv, const void *mat,
+                    const void *cc_ret, const void *cc_les);
+/* One time step of F and Fcc (herm_matrix_timestep slices; tstp = -1: F^mat, cc_slice unused). */
+int nessi_gpu_set_F_timestep(nessi_batch *b, int group, int tstp, const void *slice, const void *cc_slice);
+/* The source term Q of problem p, whole or one time step. */
+int nessi_gpu_set_Q(nessi_batch *b, int p, const void *ret, const void *les, const void *tv, const void *mat);
+int nessi_gpu_set_Q_timestep(nessi_batch *b, int p, int tstp, const void *slice);
+/* cntr::vie2_start(G, F, Fcc, Q, SolveOrder, beta, h) (cntr_vie2_decl.hpp:67,
+ * cntr_vie2_impl.hpp:1338-1420): time steps 0..k of every VIE2 problem from G^mat. */
+int nessi_gpu_vie2_start(nessi_batch *b);
+/* cntr::vie2_timestep(n, G, F, Fcc, Q, SolveOrder, beta, h) (cntr_vie2_decl.hpp:72,
+ * cntr_vie2_impl.hpp:1505-1560) for every VIE2 problem with nt >= n; n > k. */
+int nessi_gpu_vie2_timestep(nessi_batch *b, int n);
+
 /* Run the batch's work on the caller's cudaStream_t (NULL: a private stream again).
  * libcntr has no streams; this lets a caller order the batch with its own work. */
 int nessi_gpu_set_stream(nessi_batch *b, void *stream);

@@ -15,6 +15,7 @@
 
 struct ProbDev {
     double2 *gret, *gles, *gtv, *gmat;  // this problem's G (libcntr layout)
+    const double2 *qret, *qles, *qtv;   // VIE2: the source term Q (tv in plane layout); else null
     const double2 *H;                   // (nt+2) s^2 blocks, H(-1) first
     double2 *minv_ret, *minv_les;       // (nt+1) s^2: inverses of the ret / les+tv step matrices
     float2 *gtv32;                      // mixed precision: FP32 copy of G^tv (plane layout) or null
@@ -25,7 +26,9 @@ struct ProbDev {
 };
 
 struct GroupDev {
-    const double2 *sret, *sles, *stv, *smat;  // Sigma (libcntr layout, shared by the group)
+    const double2 *sret, *sles, *stv, *smat;  // Sigma, or F of a VIE2 group (libcntr layout, shared)
+    const double2 *rret;  // triangle of the retarded recursion: Sigma^R, or Fcc^R for VIE2
+    const double2 *lcc;   // lesser triangle for t' < t of the les*adv operand: Sigma^<, or Fcc^<
     double2 *Ldense;   // ((ntmax+1)s) x ((ntmax+1)s) row-major: Sigma^<(j,m), full (anti-hermitian)
     double2 *Tdense;   // ((ntmax+1)s) x ((ntau+1)s) row-major: Sigma^tv(j,m) reordered (s>1)
     double2 *tvcoef;   // (ntmax+1) s^2: coefficients of the tv history sum at the current step
@@ -45,7 +48,9 @@ __device__ __forceinline__ long tri(long t) { return t * (t + 1) / 2; }
 //   tv/les:  mm = i/h bd0 + mu - H(n) - h w0 Sigma^R(n,n)        (dyson_impl :693-699, :983-1004)
 //   ret:     mm = i/h bd0 + mu - H(j)^dagger - h w0 Sigma^R(j,j) (dyson_impl :188-199)
 // ---------------------------------------------------------------------------------------
-template <int S>
+// VIE2 ([1 + F] G = Q, cntr_vie2_impl.hpp:60-140, 645-725, 847-990): the step matrices are
+//   tv/les:  mm = 1 + h w0 F^R(j,j);   ret: mm = 1 + h w0 Fcc^R(j,j)
+template <int S, bool VIE = false>
 __global__ void k_prep_problem(GroupDev g, const ProbDev *__restrict__ probs, int n, int les_lo, int r0, int r1) {
     const ProbDev p = probs[blockIdx.x];
     const int k = g.k, s2 = S * S;
@@ -60,15 +65,20 @@ __global__ void k_prep_problem(GroupDev g, const ProbDev *__restrict__ probs, in
         int j = is_ret ? r0 + (t - nles) : les_lo + t;
         if (j > p.nt) continue;
         double2 M[S * S];
-        const double2 *Hj = p.H + (long)(j + 1) * s2;
-        const double2 *Sjj = g.sret + (tri(j) + j) * s2;
-        for (int a = 0; a < S; a++)
-            for (int b = 0; b < S; b++) {
-                double2 hv = is_ret ? cconj(Hj[b * S + a]) : Hj[a * S + b];
-                double2 v = csub(cscale(Sjj[a * S + b], -w0), hv);
-                if (a == b) v = cadd(v, cadd(ibd0, cmk(p.mu, 0.0)));
-                M[a * S + b] = v;
-            }
+        if (VIE) {
+            const double2 *Fjj = (is_ret ? g.rret : g.sret) + (tri(j) + j) * s2;
+            for (int e = 0; e < s2; e++) M[e] = cadd(cscale(Fjj[e], w0), cmk(e / S == e % S ? 1.0 : 0.0, 0.0));
+        } else {
+            const double2 *Hj = p.H + (long)(j + 1) * s2;
+            const double2 *Sjj = g.sret + (tri(j) + j) * s2;
+            for (int a = 0; a < S; a++)
+                for (int b = 0; b < S; b++) {
+                    double2 hv = is_ret ? cconj(Hj[b * S + a]) : Hj[a * S + b];
+                    double2 v = csub(cscale(Sjj[a * S + b], -w0), hv);
+                    if (a == b) v = cadd(v, cadd(ibd0, cmk(p.mu, 0.0)));
+                    M[a * S + b] = v;
+                }
+        }
         double2 *dst = (is_ret ? p.minv_ret : p.minv_les) + (long)j * s2;
         small_inverse<S>(M, dst);
     }
@@ -79,7 +89,8 @@ __global__ void k_prep_problem(GroupDev g, const ProbDev *__restrict__ probs, in
 // (conv_impl :942-972 with the BDF terms of dyson_impl :681-692 folded in), and the dense
 // copies of Sigma^< (rows/columns d_lo..n) and Sigma^tv (rows d_lo..n).
 // ---------------------------------------------------------------------------------------
-template <int S>
+// VIE2: a_j = -h w(n,j) F^R(n,j) (conv_tv with A = F, moved to the right-hand side).
+template <int S, bool VIE = false>
 __global__ void k_prep_group(GroupDev g, int n, int d_lo) {
     const int k = g.k, s2 = S * S;
     const double h = g.h;
@@ -88,8 +99,9 @@ __global__ void k_prep_group(GroupDev g, int n, int d_lo) {
     // tv coefficients, j = 0..n-1
     for (long e = tid; e < (long)n * s2; e += nth) {
         int j = (int)(e / s2), ab = (int)(e % s2), a = ab / S, b = ab % S;
-        double2 v = cscale(g.sret[(tri(n) + j) * s2 + ab], h * greg_w(k, n, j));
-        if (j >= n - k - 1 && a == b) v = csub(v, cmk(0.0, bd_w(k, n - j) / h));
+        (void)a; (void)b;
+        double2 v = cscale(g.sret[(tri(n) + j) * s2 + ab], (VIE ? -h : h) * greg_w(k, n, j));
+        if (!VIE && j >= n - k - 1 && a == b) v = csub(v, cmk(0.0, bd_w(k, n - j) / h));
         g.tvcoef[(long)j * s2 + ab] = v;
     }
     // dense Sigma^<: for every t in [d_lo, n]: column t (rows 0..t) and row t (cols 0..t-1)
@@ -100,8 +112,8 @@ __global__ void k_prep_group(GroupDev g, int n, int d_lo) {
             // L(j,t) = Sigma^<(j,t), j <= t
             double2 v = g.sles[(tri(t) + j) * s2 + ab];
             g.Ldense[((long)j * S + a) * ldL + (long)t * S + b] = v;
-            // L(t,j) = -Sigma^<(j,t)^dagger, j < t   [element (b,a) of the block]
-            if (j < t) g.Ldense[((long)t * S + b) * ldL + (long)j * S + a] = cneg(cconj(v));
+            // L(t,j) = -Sigma^<(j,t)^dagger (-Fcc^<(j,t)^dagger for VIE2), j < t  [element (b,a)]
+            if (j < t) g.Ldense[((long)t * S + b) * ldL + (long)j * S + a] = cneg(cconj(g.lcc[(tri(t) + j) * s2 + ab]));
         }
     }
     if (S > 1) {
@@ -193,6 +205,105 @@ __device__ void ret_start_block(const GroupDev &g, const ProbDev &p, int n, doub
     __syncthreads();
 }
 
+// VIE2 ret (vie2_timestep_ret, cntr_vie2_impl.hpp:60-140, called with F and Fcc swapped):
+// unknowns X_q = G(n, n-q-1), q = 0..k-1, with G(n,n) = Q(n,n) set;
+//   sum_q X_q mm(p,q) = qq(p),  mm(p,q) = 1 delta_pq + h w(j,l) F'(n-l, n-j) [l = q+1]
+//   qq(p) = Q(n, n-j) - h w(j,0) G(n,n) F'(n, n-j),  j = p+1,
+// F'(t,t') = Fcc^R(t,t') for t >= t' and F^R(t',t)^dagger otherwise (sign folded into w).
+template <int S>
+__device__ void ret_start_block_vie(const GroupDev &g, const ProbDev &p, int n, double2 *smem) {
+    const int k = g.k, s2 = S * S, KS = k * S;
+    const double h = g.h;
+    double2 *mm = smem;
+    double2 *qq = mm + k * k * s2;
+    double2 *A = qq + k * s2;
+    double2 *R = A + KS * KS;
+    int *ipiv = (int *)(R + KS * S);
+    int *status = ipiv + 1;
+    double2 *grow = p.gret + tri(n) * s2;
+    for (int e = threadIdx.x; e < k * k * s2; e += blockDim.x) mm[e] = cmk(0, 0);
+    if (threadIdx.x == 0) *status = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+        const int pr = e / s2, ab = e % s2, a = ab / S, b = ab % S, j = pr + 1;
+        double2 q = p.qret[(tri(n) + n - j) * s2 + ab];
+        if (a == b) mm[(pr * k + pr) * s2 + ab] = cadd(mm[(pr * k + pr) * s2 + ab], cmk(1.0, 0.0));
+        for (int l = 0; l <= k; l++) {
+            double w = -h * greg_w(k, j, l);
+            if (l == 0) {
+                // qq += w G(n,n) F'(n, n-j)
+                const double2 *fr = g.rret + (tri(n) + n - j) * s2;
+                double2 t = cmk(0, 0);
+                for (int c = 0; c < S; c++) t = cfma(grow[(long)n * s2 + a * S + c], fr[c * S + b], t);
+                q = cfma(cmk(w, 0.0), t, q);
+            } else {
+                double2 st;
+                if (l <= j) st = g.rret[(tri(n - l) + n - j) * s2 + ab];
+                else { st = cconj(g.sret[(tri(n - j) + n - l) * s2 + b * S + a]); w = -w; }
+                const int idx = (pr * k + l - 1) * s2 + ab;
+                mm[idx] = csub(mm[idx], cscale(st, w));
+            }
+        }
+        qq[pr * s2 + ab] = q;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < KS * KS; e += blockDim.x) {
+        int r = e / KS, c = e % KS, pr = r / S, a = r % S, q = c / S, b = c % S;
+        A[e] = cconj(mm[(pr * k + q) * s2 + b * S + a]);
+    }
+    for (int e = threadIdx.x; e < KS * S; e += blockDim.x) {
+        int r = e / S, c = e % S, pr = r / S, a = r % S;
+        R[e] = cconj(qq[pr * s2 + c * S + a]);
+    }
+    __syncthreads();
+    cta_solve(A, R, KS, S, ipiv, status);
+    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+        int q = e / s2, ac = e % s2, a = ac / S, c = ac % S;
+        grow[(long)(n - q - 1) * s2 + ac] = cconj(R[(q * S + c) * S + a]);
+    }
+    __syncthreads();
+}
+
+// VIE2 les (vie2_timestep_les, cntr_vie2_impl.hpp:847-990): unknowns x_j = G^<(j,n), j = 0..k;
+//   sum_m mm(j,m) x_m = gl(j) + Q^<(j,n),  mm(j,m) = 1 delta_jm + h w(j,m) F'(j,m),
+// F'(j,m) = F^R(j,m) for j >= m and -Fcc^R(m,j)^dagger otherwise (right solve).
+template <int S>
+__device__ void les_start_block_vie(const GroupDev &g, const ProbDev &p, int n, const double2 *gl, long ldc,
+                                    double2 *xcol, double2 *smem) {
+    const int k = g.k, K1 = k + 1, s2 = S * S, KS = K1 * S;
+    const double h = g.h;
+    double2 *A = smem;
+    double2 *R = A + KS * KS;
+    int *ipiv = (int *)(R + KS * S);
+    int *status = ipiv + 1;
+    if (threadIdx.x == 0) *status = 0;
+    for (int e = threadIdx.x; e < K1 * s2; e += blockDim.x) {
+        const int j = e / s2, ad = e % s2, a = ad / S, d = ad % S;
+        double2 q = gl[((long)j * S + a) * ldc + d];
+        q = cadd(q, j <= n ? p.qles[(tri(n) + j) * s2 + ad] : cneg(cconj(p.qles[(tri(j) + n) * s2 + d * S + a])));
+        R[(j * S + a) * S + d] = q;
+        if (d == 0) {
+            for (int m = 0; m <= k; m++) {
+                const double w = h * greg_w(k, j, m);
+                for (int b = 0; b < S; b++) {
+                    double2 st = j >= m ? g.sret[(tri(j) + m) * s2 + a * S + b]
+                                        : cneg(cconj(g.rret[(tri(m) + j) * s2 + b * S + a]));
+                    double2 v = cscale(st, w);
+                    if (m == j && a == b) v = cadd(v, cmk(1.0, 0.0));
+                    A[(j * S + a) * KS + m * S + b] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    cta_solve(A, R, KS, S, ipiv, status);
+    for (int e = threadIdx.x; e < K1 * s2; e += blockDim.x) {
+        const int j = e / s2, ad = e % s2, a = ad / S, d = ad % S;
+        xcol[(long)j * s2 + ad] = R[(j * S + a) * S + d];
+    }
+    __syncthreads();
+}
+
 // les: unknowns x_j = G^<(j,n), j = 1..k; sum_q mm(p,q) x_{q+1} = qq(p)  (right solve)
 template <int S>
 __device__ void les_start_block(const GroupDev &g, const ProbDev &p, int n, const double2 *gl, long ldc,
@@ -268,7 +379,9 @@ template <int S> struct TvCfg {
 
 // MIXED: history rows j < n-k-1 are read from the FP32 copy (half the bytes); the k+1 rows
 // that carry the backward-difference terms, and all sums, stay in FP64.
-template <int S, bool MIXED>
+// VIE2 (vie2_timestep_tv, cntr_vie2_impl.hpp:645-725): a_j and Cmat carry the minus sign of
+// the convolution and Q^tv(n, tau) is added before the solve with (1 + h w0 F^R(n,n))^-1.
+template <int S, bool MIXED, bool VIE = false>
 __global__ void __launch_bounds__(256) k_tv(GroupDev g, const ProbDev *__restrict__ probs, int n) {
     constexpr int s2 = S * S, DCH = TvCfg<S>::DCH, NW = TvCfg<S>::NW;
     __shared__ double2 red[NW * 32 * S * DCH];
@@ -354,6 +467,14 @@ __global__ void __launch_bounds__(256) k_tv(GroupDev g, const ProbDev *__restric
 #pragma unroll
                 for (int c = 0; c < DCH; c++)
                     if (c0 + c < S) acc[a][c] = cadd(acc[a][c], cm[(long)a * g.ldc + c]);
+            if (VIE) {
+                const double2 *qt = p.qtv + (long)n * rowstride + tau;
+#pragma unroll
+                for (int a = 0; a < S; a++)
+#pragma unroll
+                    for (int c = 0; c < DCH; c++)
+                        if (c0 + c < S) acc[a][c] = cadd(acc[a][c], qt[(long)(a * S + c0 + c) * M]);
+            }
             // solve: G^tv(n,tau)[a][d] = sum_b Minv[a][b] Q[b][d]
             const double2 *mi = p.minv_les + (long)n * s2;
             double2 *out = p.gtv + (long)n * rowstride + tau;
@@ -400,8 +521,9 @@ __global__ void k_tv_relayout(double2 *__restrict__ dst, const double2 *__restri
 //   c2 = sum_{l=0}^{r} w(r,l) A(m+l) B(l)           (r = ntau-m >= k; rcorr for 0<r<k)
 //   c1 = sum_{l=0}^{m} w(m,l) A(m-l) B(ntau-l)      (m >= k; rcorr for 0<m<k),  C = c2 + sig c1
 // ---------------------------------------------------------------------------------------
+// sgn = -1 for VIE2, whose Matsubara convolution enters the right-hand side with a minus sign.
 template <int S>
-__global__ void k_mat_operator(GroupDev g, int n) {
+__global__ void k_mat_operator(GroupDev g, int n, double sgn) {
     const int k = g.k, s2 = S * S, ntau = g.ntau, M = ntau + 1;
     const long KS = (long)M * S;
     const double2 *A = g.stv + (long)n * M * s2;
@@ -423,7 +545,7 @@ __global__ void k_mat_operator(GroupDev g, int n) {
         } else if (m > 0 && l >= 0 && l <= k) {
             for (int jj = 0; jj <= k; jj++) v = cfma(cmk(sg * rcorr_w(k, m, l, jj), 0), A[(long)jj * s2 + ac], v);
         }
-        g.Kmat[((long)m * S + a) * KS + (long)x * S + c] = cscale(v, dtau);
+        g.Kmat[((long)m * S + a) * KS + (long)x * S + c] = cscale(v, dtau * sgn);
     }
 }
 

@@ -73,7 +73,7 @@ __device__ void ret_phaseA(const GroupDev &g, const double2 *grow, int n, int jl
             for (int d = 0; d < S; d++) sum[i][d] = cmk(0, 0);
         if (r < nb) {
             const int j = jlo + r;
-            const double2 *sj = g.sret + (long)j * s2;  // Sigma(m,j) at sj + tri(m) s2
+            const double2 *sj = g.rret + (long)j * s2;  // Sigma(m,j) at sj + tri(m) s2
             const double2 *ga = grow + a0 * S;          // G(n,m)[a0+i][b] at ga + m s2 + i S + b
             int m = mlo + gi;
             for (; m + (U - 1) * G <= n; m += U * G) {
@@ -127,9 +127,9 @@ __device__ void ret_phaseA(const GroupDev &g, const double2 *grow, int n, int jl
     }
 }
 
-template <int S>
+template <int S, bool VIE>
 __device__ void ret_stage(const GroupDev &g, const ProbDev &p, int n, int jlo, int nb, double2 *sig, double *wb,
-                          double2 *minv, int t, int nthr) {
+                          double2 *minv, double2 *qb, int t, int nthr) {
     constexpr int s2 = S * S;
     const int k = g.k;
     for (int e = t; e < RetCfg<S>::TRI * s2; e += nthr) {
@@ -137,11 +137,14 @@ __device__ void ret_stage(const GroupDev &g, const ProbDev &p, int n, int jlo, i
         int r, r2;
         pk_inv(q, r, r2);
         if (r < nb) {
-            sig[e] = g.sret[(tri(jlo + r) + jlo + r2) * s2 + ab];
+            sig[e] = g.rret[(tri(jlo + r) + jlo + r2) * s2 + ab];
             if (ab == 0) wb[q] = greg_w(k, n - (jlo + r2), n - (jlo + r));
         }
     }
-    for (int e = t; e < nb * s2; e += nthr) minv[e] = p.minv_ret[(long)jlo * s2 + e];
+    for (int e = t; e < nb * s2; e += nthr) {
+        minv[e] = p.minv_ret[(long)jlo * s2 + e];
+        if (VIE) qb[e] = p.qret[(tri(n) + jlo) * s2 + e];  // Q(n, jlo + r)
+    }
 }
 
 // Register-resident solve of one block for S <= 2 (warp 0): lane r owns block row r and keeps
@@ -158,10 +161,12 @@ __device__ __forceinline__ void shfl_blk(double2 *x, int src) {
     }
 }
 
-// ret: rows solved from r = nb-1 down to 0; x_r = (h acc_r - bdf_r) Minv_r (left solve)
-template <int S>
-__device__ void ret_chain(const double2 *acc, const double2 *sig, const double *wb, const double2 *minv, double2 *xs,
-                          double2 *gout, int nb, int K1, const double2 *ibd, double h, int lane) {
+// ret: rows solved from r = nb-1 down to 0; x_r = (h acc_r - bdf_r) Minv_r (left solve);
+// VIE2: x_r = (Q_r - h acc_r) Minv_r
+template <int S, bool VIE>
+__device__ void ret_chain(const double2 *acc, const double2 *sig, const double *wb, const double2 *minv,
+                          const double2 *qb, double2 *xs, double2 *gout, int nb, int K1, const double2 *ibd, double h,
+                          int lane) {
     constexpr int s2 = S * S;
     const int r = lane;
     const bool own = r < nb;
@@ -170,9 +175,9 @@ __device__ void ret_chain(const double2 *acc, const double2 *sig, const double *
     for (int e = 0; e < s2; e++) {
         a_[e] = own ? acc[r * s2 + e] : cmk(0, 0);
         mi[e] = own ? minv[r * s2 + e] : cmk(0, 0);
-        bd[e] = cmk(0, 0);
+        bd[e] = (VIE && own) ? qb[r * s2 + e] : cmk(0, 0);  // VIE2: bd holds Q_r
     }
-    if (own)
+    if (own && !VIE)
         for (int pp = 1; pp <= K1; pp++)
             if (r + pp >= nb)
 #pragma unroll
@@ -182,7 +187,7 @@ __device__ void ret_chain(const double2 *acc, const double2 *sig, const double *
         if (r == rr) {
             double2 q[s2];
 #pragma unroll
-            for (int e = 0; e < s2; e++) q[e] = csub(cscale(a_[e], h), bd[e]);
+            for (int e = 0; e < s2; e++) q[e] = VIE ? csub(bd[e], cscale(a_[e], h)) : csub(cscale(a_[e], h), bd[e]);
 #pragma unroll
             for (int aa = 0; aa < S; aa++)
 #pragma unroll
@@ -211,7 +216,7 @@ __device__ void ret_chain(const double2 *acc, const double2 *sig, const double *
                     for (int bb = 0; bb < S; bb++) t = cfma(x[aa * S + bb], sg[bb * S + d], t);
                     a_[aa * S + d] = cfma(cmk(w, 0.0), t, a_[aa * S + d]);
                 }
-            if (rr - r <= K1)
+            if (!VIE && rr - r <= K1)
 #pragma unroll
                 for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[rr - r], x[e], bd[e]);
         }
@@ -219,8 +224,9 @@ __device__ void ret_chain(const double2 *acc, const double2 *sig, const double *
 }
 
 // les: rows solved from r = 0 up; x_r = Minv_r (gl_r + h acc_r - bdf_r) (right solve);
+// VIE2: x_r = Minv_r (gl_r - h acc_r) with gl_r including Q^<(j,n).
 // xs holds x(jlo - K1 + i) at index i
-template <int S>
+template <int S, bool VIE>
 __device__ void les_chain(const double2 *acc, const double2 *sig, const double *wb, const double2 *minv,
                           const double2 *glb, double2 *xs, double2 *gout, int nb, int K1, const double2 *ibd, double h,
                           int lane) {
@@ -235,7 +241,7 @@ __device__ void les_chain(const double2 *acc, const double2 *sig, const double *
         gv[e] = own ? glb[r * s2 + e] : cmk(0, 0);
         bd[e] = cmk(0, 0);
     }
-    if (own)
+    if (own && !VIE)
         for (int pp = 1; pp <= K1; pp++)
             if (r - pp < 0)
 #pragma unroll
@@ -245,7 +251,7 @@ __device__ void les_chain(const double2 *acc, const double2 *sig, const double *
         if (r == rr) {
             double2 q[s2];
 #pragma unroll
-            for (int e = 0; e < s2; e++) q[e] = csub(cfma(cmk(h, 0.0), a_[e], gv[e]), bd[e]);
+            for (int e = 0; e < s2; e++) q[e] = VIE ? cfma(cmk(-h, 0.0), a_[e], gv[e]) : csub(cfma(cmk(h, 0.0), a_[e], gv[e]), bd[e]);
 #pragma unroll
             for (int aa = 0; aa < S; aa++)
 #pragma unroll
@@ -274,14 +280,14 @@ __device__ void les_chain(const double2 *acc, const double2 *sig, const double *
                     for (int bb = 0; bb < S; bb++) t = cfma(sg[aa * S + bb], x[bb * S + d], t);
                     a_[aa * S + d] = cfma(cmk(w, 0.0), t, a_[aa * S + d]);
                 }
-            if (r - rr <= K1)
+            if (!VIE && r - rr <= K1)
 #pragma unroll
                 for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[r - rr], x[e], bd[e]);
         }
     }
 }
 
-template <int S>
+template <int S, bool VIE = false>
 __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__restrict__ probs, int n) {
     extern __shared__ double2 smem[];
     const ProbDev p = probs[blockIdx.x];
@@ -292,10 +298,12 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
     double2 *grow = p.gret + tri(n) * s2;  // G(n, 0..n)
     for (long e = tid; e < (long)(n + 1) * s2; e += blockDim.x) {
         int ab = (int)(e % s2);
-        grow[e] = (e / s2 == n && (ab / S == ab % S)) ? cmk(0.0, -1.0) : cmk(0, 0);
+        if (VIE) grow[e] = e / s2 == n ? p.qret[(tri(n) + n) * s2 + ab] : cmk(0, 0);  // G(n,n) = Q(n,n)
+        else grow[e] = (e / s2 == n && (ab / S == ab % S)) ? cmk(0.0, -1.0) : cmk(0, 0);
     }
     __syncthreads();
-    ret_start_block<S>(g, p, n, smem);
+    if (VIE) ret_start_block_vie<S>(g, p, n, smem);
+    else ret_start_block<S>(g, p, n, smem);
     double2 *part = smem + L::part, *qv = smem + L::qv;
     double2 ibd[NESSI_K1MAX + 1];
 #pragma unroll
@@ -307,12 +315,13 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
     auto SIG = [&](int bf) { return smem + L::sig + bf * L::TRI * s2; };
     auto WBF = [&](int bf) { return (double *)(smem + L::w + bf * L::WB); };
     auto MNV = [&](int bf) { return smem + L::minv + bf * JB * s2; };
+    auto QB = [&](int bf) { return smem + L::gl + bf * JB * s2; };  // VIE2: Q(n, j) of the block
     auto XS = [&](int bf) { return smem + L::xs + bf * L::XS * s2; };
     // prologue: block 0 with all threads
     {
         const int jhi = jtop, jlo = jhi - JB + 1 < 0 ? 0 : jhi - JB + 1, nb = jhi - jlo + 1;
         ret_phaseA<S, false>(g, grow, n, jlo, nb, jhi + 1, part, ACC(0), tid, 256);
-        ret_stage<S>(g, p, n, jlo, nb, SIG(0), WBF(0), MNV(0), tid, 256);
+        ret_stage<S, VIE>(g, p, n, jlo, nb, SIG(0), WBF(0), MNV(0), QB(0), tid, 256);
         for (int e = tid; e < K1 * s2; e += 256) XS(0)[nb * s2 + e] = grow[(long)(jhi + 1) * s2 + e];
         __syncthreads();
     }
@@ -322,17 +331,22 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
         const bool has_next = jlo > 0;
         const int jhi2 = jlo - 1, jlo2 = jhi2 - JB + 1 < 0 ? 0 : jhi2 - JB + 1, nb2 = jhi2 - jlo2 + 1;
         if (warp == 0 && S <= 2) {
-            ret_chain<S>(ACC(cur), SIG(cur), WBF(cur), MNV(cur), XS(cur), grow + (long)jlo * s2, nb, K1, ibds, h, lane);
+            ret_chain<S, VIE>(ACC(cur), SIG(cur), WBF(cur), MNV(cur), QB(cur), XS(cur), grow + (long)jlo * s2, nb, K1,
+                              ibds, h, lane);
         } else if (warp == 0) {
             // ---- phase B: solve j = jhi .. jlo
-            double2 *acc = ACC(cur), *sig = SIG(cur), *minv = MNV(cur), *xs = XS(cur);
+            double2 *acc = ACC(cur), *sig = SIG(cur), *minv = MNV(cur), *xs = XS(cur), *qb = QB(cur);
             const double *wb = WBF(cur);
             for (int r = nb - 1; r >= 0; r--) {
                 for (int e = lane; e < s2; e += 32) {
                     double2 q = cscale(acc[r * s2 + e], h);
+                    if (VIE) {
+                        q = csub(qb[r * s2 + e], q);
+                    } else {
 #pragma unroll
-                    for (int pp = 1; pp <= NESSI_K1MAX; pp++)
-                        if (pp <= K1) q = csub(q, cmul(ibd[pp], xs[(r + pp) * s2 + e]));
+                        for (int pp = 1; pp <= NESSI_K1MAX; pp++)
+                            if (pp <= K1) q = csub(q, cmul(ibd[pp], xs[(r + pp) * s2 + e]));
+                    }
                     qv[e] = q;
                 }
                 __syncwarp();
@@ -358,7 +372,7 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
         } else if (has_next) {
             // ---- look-ahead: phase A of block b+1 over m > jhi, and its staging
             ret_phaseA<S, true>(g, grow, n, jlo2, nb2, jhi + 1, part, ACC(nxt), tid - 32, 224);
-            ret_stage<S>(g, p, n, jlo2, nb2, SIG(nxt), WBF(nxt), MNV(nxt), tid - 32, 224);
+            ret_stage<S, VIE>(g, p, n, jlo2, nb2, SIG(nxt), WBF(nxt), MNV(nxt), QB(nxt), tid - 32, 224);
         }
         __syncthreads();
         if (!has_next) break;
@@ -374,7 +388,7 @@ __global__ void __launch_bounds__(256, 2) k_ret(GroupDev g, const ProbDev *__res
 #pragma unroll 4
                     for (int mm = gi; mm < nb; mm += GC) {
                         const int m = jlo + mm;
-                        const double2 *sm = g.sret + (tri(m) + j) * s2 + d;
+                        const double2 *sm = g.rret + (tri(m) + j) * s2 + d;
                         double2 tt = cmk(0, 0);
 #pragma unroll
                         for (int bb = 0; bb < S; bb++) tt = cfma(xs[mm * s2 + a * S + bb], sm[bb * S], tt);
@@ -479,8 +493,8 @@ __device__ void les_phaseA(const GroupDev &g, const double2 *xcol, int jlo, int 
     }
 }
 
-template <int S>
-__device__ void les_stage(const GroupDev &g, const ProbDev &p, const double2 *gl, long ldc, int jlo, int nb,
+template <int S, bool VIE>
+__device__ void les_stage(const GroupDev &g, const ProbDev &p, int n, const double2 *gl, long ldc, int jlo, int nb,
                           double2 *sig, double *wb, double2 *minv, double2 *glb, int t, int nthr) {
     constexpr int s2 = S * S;
     const int k = g.k;
@@ -497,10 +511,11 @@ __device__ void les_stage(const GroupDev &g, const ProbDev &p, const double2 *gl
         minv[e] = p.minv_les[(long)jlo * s2 + e];
         const int r = e / s2, ad = e % s2, a = ad / S, d = ad % S;
         glb[e] = gl[((long)(jlo + r) * S + a) * ldc + d];
+        if (VIE) glb[e] = cadd(glb[e], p.qles[(tri(n) + jlo + r) * s2 + ad]);  // + Q^<(j,n), j <= n
     }
 }
 
-template <int S>
+template <int S, bool VIE = false>
 __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__restrict__ probs, int n) {
     extern __shared__ double2 smem[];
     const ProbDev p = probs[blockIdx.x];
@@ -511,12 +526,16 @@ __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__res
     const long ldc = g.ldc;
     const double2 *gl = g.gles + (long)p.col * S;   // gles(j)[a][d] at gl[(j*S+a)*ldc + d]
     double2 *xcol = p.gles + tri(n) * s2;           // G^<(0..n, n)
-    for (int ad = tid; ad < s2; ad += blockDim.x) {
-        int a = ad / S, d = ad % S;
-        xcol[ad] = cneg(cconj(p.gtv[((long)n * s2 + d * S + a) * (g.ntau + 1) + 0]));
+    if (VIE) {
+        les_start_block_vie<S>(g, p, n, gl, ldc, xcol, smem);
+    } else {
+        for (int ad = tid; ad < s2; ad += blockDim.x) {
+            int a = ad / S, d = ad % S;
+            xcol[ad] = cneg(cconj(p.gtv[((long)n * s2 + d * S + a) * (g.ntau + 1) + 0]));
+        }
+        __syncthreads();
+        les_start_block<S>(g, p, n, gl, ldc, xcol, smem);
     }
-    __syncthreads();
-    les_start_block<S>(g, p, n, gl, ldc, xcol, smem);
     if (n <= k) return;
     double2 *part = smem + L::part, *qv = smem + L::qv, *red = smem + L::red;
     double2 ibd[NESSI_K1MAX + 1];
@@ -534,7 +553,7 @@ __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__res
     {
         const int jlo = jstart, jhi = jlo + JB - 1 > n ? n : jlo + JB - 1, nb = jhi - jlo + 1;
         les_phaseA<S>(g, xcol, jlo, nb, jlo, ACC(0), red, warp, 8, lane, warp);
-        les_stage<S>(g, p, gl, ldc, jlo, nb, SIG(0), WBF(0), MNV(0), GLB(0), tid, 256);
+        les_stage<S, VIE>(g, p, n, gl, ldc, jlo, nb, SIG(0), WBF(0), MNV(0), GLB(0), tid, 256);
         for (int e = tid; e < K1 * s2; e += 256) XS(0)[e] = xcol[(long)(jlo - K1) * s2 + e];
         __syncthreads();
     }
@@ -544,17 +563,19 @@ __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__res
         const bool has_next = jhi < n;
         const int jlo2 = jhi + 1, jhi2 = jlo2 + JB - 1 > n ? n : jlo2 + JB - 1, nb2 = jhi2 - jlo2 + 1;
         if (warp == 0 && S <= 2) {
-            les_chain<S>(ACC(cur), SIG(cur), WBF(cur), MNV(cur), GLB(cur), XS(cur), xcol + (long)jlo * s2, nb, K1, ibds,
-                         h, lane);
+            les_chain<S, VIE>(ACC(cur), SIG(cur), WBF(cur), MNV(cur), GLB(cur), XS(cur), xcol + (long)jlo * s2, nb, K1,
+                              ibds, h, lane);
         } else if (warp == 0) {
             double2 *acc = ACC(cur), *sig = SIG(cur), *minv = MNV(cur), *glb = GLB(cur), *xs = XS(cur);
             const double *wb = WBF(cur);
             for (int r = 0; r < nb; r++) {
                 for (int e = lane; e < s2; e += 32) {
-                    double2 q = cfma(cmk(h, 0.0), acc[r * s2 + e], glb[r * s2 + e]);
+                    double2 q = cfma(cmk(VIE ? -h : h, 0.0), acc[r * s2 + e], glb[r * s2 + e]);
+                    if (!VIE) {
 #pragma unroll
-                    for (int pp = 1; pp <= NESSI_K1MAX; pp++)
-                        if (pp <= K1) q = csub(q, cmul(ibd[pp], xs[(r + K1 - pp) * s2 + e]));
+                        for (int pp = 1; pp <= NESSI_K1MAX; pp++)
+                            if (pp <= K1) q = csub(q, cmul(ibd[pp], xs[(r + K1 - pp) * s2 + e]));
+                    }
                     qv[e] = q;
                 }
                 __syncwarp();
@@ -579,7 +600,7 @@ __global__ void __launch_bounds__(256, 2) k_les(GroupDev g, const ProbDev *__res
             }
         } else if (has_next) {
             les_phaseA<S>(g, xcol, jlo2, nb2, jlo, ACC(nxt), red, warp - 1, 7, lane, warp);
-            les_stage<S>(g, p, gl, ldc, jlo2, nb2, SIG(nxt), WBF(nxt), MNV(nxt), GLB(nxt), tid - 32, 224);
+            les_stage<S, VIE>(g, p, n, gl, ldc, jlo2, nb2, SIG(nxt), WBF(nxt), MNV(nxt), GLB(nxt), tid - 32, 224);
         }
         __syncthreads();
         if (!has_next) break;

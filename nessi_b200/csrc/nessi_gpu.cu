@@ -81,6 +81,7 @@ struct Prob {
     double2 *gret = nullptr, *gles = nullptr, *gtv = nullptr, *gmat = nullptr;
     double2 *H = nullptr, *minv_ret = nullptr, *minv_les = nullptr;
     float2 *gtv32 = nullptr;
+    double2 *qret = nullptr, *qles = nullptr, *qtv = nullptr, *qmat = nullptr;  // VIE2 source term
 };
 
 struct Group {
@@ -96,6 +97,8 @@ struct Group {
     bool gmat_valid = false;
     MatScratch *d_mat = nullptr;  // per-member scratch of dyson_mat (allocated on first use)
     LocDev loc{nullptr, nullptr, nullptr, nullptr};  // G_loc of the group (allocated on first use)
+    bool vie = false;                // VIE2 group: s* hold F, fcc* hold Fcc (nessi_gpu_set_F)
+    double2 *fccret = nullptr, *fccles = nullptr;
     double2 *U = nullptr;            // diagonal interaction U(t), (ntmax+2) x s, t = -1 first
     std::vector<int> members;        // problem indices, nt descending
     std::vector<ProbDev> h_probs;    // same order; col = position
@@ -168,6 +171,8 @@ namespace {
 GroupDev group_dev(const Group &g) {
     GroupDev d;
     d.sret = g.sret; d.sles = g.sles; d.stv = g.stv; d.smat = g.smat;
+    d.rret = g.vie ? g.fccret : g.sret;
+    d.lcc = g.vie ? g.fccles : g.sles;
     d.Ldense = g.Ldense; d.Tdense = g.Tdense; d.tvcoef = g.tvcoef;
     d.badv = g.badv; d.btv = g.btv; d.gles = g.gles;
     d.Kmat = g.Kmat; d.Gmat_all = g.Gmat_all; d.Cmat = g.Cmat;
@@ -201,12 +206,13 @@ template <int S> size_t ret_smem(int k) {
     return std::max(start, phase);
 }
 template <int S> size_t les_smem(int k) {
-    size_t start = (size_t)((k * S) * (k * S) + k * S * S) * 16 + 16;
+    const int K1 = k + 1;  // the VIE2 start block has k+1 unknowns
+    size_t start = (size_t)((K1 * S) * (K1 * S) + K1 * S * S) * 16 + 16;
     size_t phase = (size_t)VolLayout<S>::total * 16;
     return std::max(start, phase);
 }
 
-template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
+template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     const GroupDev gd = group_dev(g);
     cudaStream_t st = b->stream;
     const int k = g.k;
@@ -214,7 +220,7 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     int les_lo = std::min(n, std::max(k + 1, g.les_valid + 1));
     int r0 = g.ret_valid + 1, r1 = n - k - 1;
     b->prof_mark(NESSI_KERNEL_PREP);
-    k_prep_problem<S><<<nact, 64, 0, st>>>(gd, g.d_probs, n, les_lo, r0, r1);
+    k_prep_problem<S, VIE><<<nact, 64, 0, st>>>(gd, g.d_probs, n, les_lo, r0, r1);
     CK(cudaGetLastError());
     g.les_valid = n - 1;
     if (r1 >= r0) g.ret_valid = r1;
@@ -222,12 +228,14 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     {
         long work = (long)(n + 1) * S * S * (n - d_lo + 1) + (long)n * S * S;
         int blocks = (int)std::min<long>(std::max<long>(1, (work + 255) / 256), 1184);
-        k_prep_group<S><<<blocks, 256, 0, st>>>(gd, n, d_lo);
+        k_prep_group<S, VIE><<<blocks, 256, 0, st>>>(gd, n, d_lo);
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_PREP, 0.0);
         g.dense_valid = n - 1;
     }
     const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    // VIE2 moves the convolution to the right-hand side: gles = -(tv*vt + les*adv)
+    const cuDoubleComplex alpha = make_cuDoubleComplex(VIE ? -1.0 : 1.0, 0.0);
     // Matsubara part of the tv row: Cmat = K_n Gmat_all (one GEMM for the group)
     {
         const long M = g.ntau + 1;
@@ -239,7 +247,7 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
         }
         b->prof_mark(NESSI_KERNEL_MATOP);
         long work = M * M * S * S;
-        k_mat_operator<S><<<(unsigned)std::min<long>((work + 255) / 256, 4736), 256, 0, st>>>(gd, n);
+        k_mat_operator<S><<<(unsigned)std::min<long>((work + 255) / 256, 4736), 256, 0, st>>>(gd, n, VIE ? -1.0 : 1.0);
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_MATOP, 16.0 * (double)work + 16.0 * M * S * S);
         b->prof_mark(NESSI_KERNEL_GEMM);
@@ -255,9 +263,9 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     {
         size_t sm = ret_smem<S>(k);
-        CK(cudaFuncSetAttribute(k_ret<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(cudaFuncSetAttribute(k_ret<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         b->prof_mark(NESSI_KERNEL_RET, b->side);
-        k_ret<S><<<nact, 256, sm, b->side>>>(gd, g.d_probs, n);
+        k_ret<S, VIE><<<nact, 256, sm, b->side>>>(gd, g.d_probs, n);
         CK(cudaGetLastError());
         // G^R row n written; Sigma^R triangle rows <= n read (shared by the group)
         b->prof_end(NESSI_KERNEL_RET, 16.0 * S * S * ((double)nact * (n + 1) + tri_h(n + 1)), b->side);
@@ -268,7 +276,7 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_LES_OPERANDS, 32.0 * S * S * (double)nact * (n + 1), b->side);
         b->prof_mark(NESSI_KERNEL_GEMM, b->side);
-        CKB(cublasZgemm(b->cublas_side, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (n + 1) * S, &one,
+        CKB(cublasZgemm(b->cublas_side, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (n + 1) * S, &alpha,
                         (const cuDoubleComplex *)g.badv, g.ldc, (const cuDoubleComplex *)g.Ldense, (int)ldL, &zero,
                         (cuDoubleComplex *)g.gles, g.ldc));
         b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)m * nn * ((n + 1) * S), b->side);
@@ -279,8 +287,8 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
         dim3 grid((g.ntau + 1 + 31) / 32, nact);
         b->prof_mark(NESSI_KERNEL_TV);
         const bool mixed = b->precision == NESSI_PREC_MIXED;
-        if (mixed) k_tv<S, true><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
-        else k_tv<S, false><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+        if (mixed) k_tv<S, true, VIE><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+        else k_tv<S, false, VIE><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
         CK(cudaGetLastError());
         // per problem: G^tv history rows 0..n-1 read (FP32 below the k+1 BDF rows when mixed),
         // row n written, Cmat column read; shared: the n coefficient blocks
@@ -300,7 +308,7 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     {
         b->prof_mark(NESSI_KERNEL_GEMM);
         const double2 *T = S == 1 ? g.stv : g.Tdense;
-        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (g.ntau + 1) * S, &one,
+        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (g.ntau + 1) * S, &alpha,
                         (const cuDoubleComplex *)g.btv, g.ldc, (const cuDoubleComplex *)T, (int)ldT, &one,
                         (cuDoubleComplex *)g.gles, g.ldc));
         b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)m * nn * ((g.ntau + 1) * S));
@@ -308,9 +316,9 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     // lesser column
     {
         size_t sm = les_smem<S>(k);
-        CK(cudaFuncSetAttribute(k_les<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(cudaFuncSetAttribute(k_les<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         b->prof_mark(NESSI_KERNEL_LES);
-        k_les<S><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+        k_les<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_LES, 16.0 * S * S * ((double)nact * 2.0 * (n + 1) + tri_h(n + 1)));
     }
@@ -320,8 +328,13 @@ template <int S> int step_group(nessi_batch *b, Group &g, int n, int nact) {
 template <int S> int start_group(nessi_batch *b, Group &g) {
     const GroupDev gd = group_dev(g);
     const size_t sm = NESSI_START_SMEM * sizeof(double2);
-    CK(cudaFuncSetAttribute(k_dyson_start<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_dyson_start<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs);
+    if (g.vie) {
+        CK(cudaFuncSetAttribute(k_vie2_start<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_vie2_start<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs);
+    } else {
+        CK(cudaFuncSetAttribute(k_dyson_start<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_dyson_start<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs);
+    }
     CK(cudaGetLastError());
     return NESSI_OK;
 }
@@ -416,16 +429,20 @@ int gloc_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(gloc_g
 int sigma2b_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(sigma2b_group, b, g, tstp) }
 int mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(mat_group, b, g) }
 
+template <int S> int step_group_any(nessi_batch *b, Group &g, int n, int nact) {
+    return g.vie ? step_group<S, true>(b, g, n, nact) : step_group<S, false>(b, g, n, nact);
+}
+
 int step_dispatch(nessi_batch *b, Group &g, int n, int nact) {
     switch (g.s) {
-        case 1: return step_group<1>(b, g, n, nact);
-        case 2: return step_group<2>(b, g, n, nact);
-        case 3: return step_group<3>(b, g, n, nact);
-        case 4: return step_group<4>(b, g, n, nact);
-        case 5: return step_group<5>(b, g, n, nact);
-        case 6: return step_group<6>(b, g, n, nact);
-        case 7: return step_group<7>(b, g, n, nact);
-        case 8: return step_group<8>(b, g, n, nact);
+        case 1: return step_group_any<1>(b, g, n, nact);
+        case 2: return step_group_any<2>(b, g, n, nact);
+        case 3: return step_group_any<3>(b, g, n, nact);
+        case 4: return step_group_any<4>(b, g, n, nact);
+        case 5: return step_group_any<5>(b, g, n, nact);
+        case 6: return step_group_any<6>(b, g, n, nact);
+        case 7: return step_group_any<7>(b, g, n, nact);
+        case 8: return step_group_any<8>(b, g, n, nact);
     }
     set_err("size1 = %d not supported (1..8)", g.s);
     return NESSI_ERR_ARG;
@@ -552,6 +569,7 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
             ProbDev pd;
             pd.gret = p.gret; pd.gles = p.gles; pd.gtv = p.gtv; pd.gmat = p.gmat;
             pd.H = p.H; pd.minv_ret = p.minv_ret; pd.minv_les = p.minv_les; pd.gtv32 = p.gtv32;
+            pd.qret = p.qret; pd.qles = p.qles; pd.qtv = p.qtv;
             pd.mu = p.d.mu; pd.nt = p.d.nt; pd.col = (int)c; pd.pad = 0;
             g.h_probs.push_back(pd);
         }
@@ -739,17 +757,39 @@ int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void
     return NESSI_OK;
 }
 
-int nessi_gpu_dyson_timestep(nessi_batch *b, int n) {
+static int find_group_checked(nessi_batch *b, int group, Group **out) {
     CKR(check_batch(b));
+    int gi = find_group(b, group);
+    if (gi < 0) { set_err("unknown sigma_group %d", group); return NESSI_ERR_ARG; }
+    *out = &b->groups[gi];
+    return NESSI_OK;
+}
+
+static int timestep_kind(nessi_batch *b, int n, bool vie, const char *name) {
+    CKR(check_batch(b));
+    bool any = false;
     for (Group &g : b->groups) {
-        if (n <= g.k) { set_err("dyson_timestep: n = %d must exceed the solve order %d", n, g.k); return NESSI_ERR_ARG; }
+        if (g.vie != vie) continue;
+        any = true;
+        if (n <= g.k) { set_err("%s: n = %d must exceed the solve order %d", name, n, g.k); return NESSI_ERR_ARG; }
+    }
+    if (!any) { set_err("%s: the batch has no %s group", name, vie ? "VIE2 (nessi_gpu_set_F)" : "Dyson"); return NESSI_ERR_ARG; }
+    for (Group &g : b->groups) {
+        if (g.vie != vie) continue;
         int nact = 0;
         for (int i : g.members) nact += b->probs[i].d.nt >= n ? 1 : 0;
         if (nact == 0) continue;
+        if (vie)
+            for (int i = 0; i < nact; i++)
+                if (!b->probs[g.members[i]].qret) { set_err("%s: Q of problem %d not set", name, g.members[i]); return NESSI_ERR_ARG; }
         CKR(step_dispatch(b, g, n, nact));
     }
     return NESSI_OK;
 }
+
+int nessi_gpu_dyson_timestep(nessi_batch *b, int n) { return timestep_kind(b, n, false, "dyson_timestep"); }
+
+int nessi_gpu_vie2_timestep(nessi_batch *b, int n) { return timestep_kind(b, n, true, "vie2_timestep"); }
 
 int nessi_gpu_set_stream(nessi_batch *b, void *stream) {
     CKR(check_batch(b));
@@ -794,6 +834,7 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
 int nessi_gpu_dyson_mat(nessi_batch *b) {
     CKR(check_batch(b));
     for (Group &g : b->groups) {
+        if (g.vie) continue;  // VIE2 groups take G^mat from the caller
         if (g.ntau % 2) { set_err("dyson_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
         CKR(mat_dispatch(b, g));
     }
@@ -801,14 +842,22 @@ int nessi_gpu_dyson_mat(nessi_batch *b) {
     return NESSI_OK;
 }
 
-int nessi_gpu_dyson_start(nessi_batch *b) {
+static int start_kind(nessi_batch *b, bool vie, const char *name) {
     CKR(check_batch(b));
+    bool any = false;
     for (Group &g : b->groups) {
-        for (int i : g.members)
-            if (b->probs[i].d.nt < g.k) { set_err("dyson_start: nt must be >= SolveOrder"); return NESSI_ERR_ARG; }
-        CKR(start_dispatch(b, g));
+        if (g.vie != vie) continue;
+        any = true;
+        for (int i : g.members) {
+            if (b->probs[i].d.nt < g.k) { set_err("%s: nt must be >= SolveOrder", name); return NESSI_ERR_ARG; }
+            if (vie && !b->probs[i].qret) { set_err("%s: Q of problem %d not set", name, i); return NESSI_ERR_ARG; }
+        }
     }
+    if (!any) { set_err("%s: the batch has no %s group", name, vie ? "VIE2 (nessi_gpu_set_F)" : "Dyson"); return NESSI_ERR_ARG; }
+    for (Group &g : b->groups)
+        if (g.vie == vie) CKR(start_dispatch(b, g));
     for (Prob &q : b->probs) {
+        if (b->groups[q.group].vie != vie) continue;
         const long row = (long)(q.d.ntau + 1) * q.d.size1 * q.d.size1;
         CKR(refresh32(b, q.gtv32, q.gtv, (b->groups[q.group].k + 1) * row));
     }
@@ -816,13 +865,100 @@ int nessi_gpu_dyson_start(nessi_batch *b) {
     return NESSI_OK;
 }
 
-static int find_group_checked(nessi_batch *b, int group, Group **out) {
-    CKR(check_batch(b));
-    int gi = find_group(b, group);
-    if (gi < 0) { set_err("unknown sigma_group %d", group); return NESSI_ERR_ARG; }
-    *out = &b->groups[gi];
+int nessi_gpu_dyson_start(nessi_batch *b) { return start_kind(b, false, "dyson_start"); }
+
+int nessi_gpu_vie2_start(nessi_batch *b) { return start_kind(b, true, "vie2_start"); }
+
+static int sync_probdev(nessi_batch *b, int p) {
+    Prob &q = b->probs[p];
+    Group &g = b->groups[q.group];
+    for (size_t c = 0; c < g.members.size(); c++) {
+        if (g.members[c] != p) continue;
+        ProbDev &pd = g.h_probs[c];
+        pd.qret = q.qret; pd.qles = q.qles; pd.qtv = q.qtv;
+        CK(cudaMemcpyAsync(g.d_probs + c, &pd, sizeof(ProbDev), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+    }
     return NESSI_OK;
 }
+
+static int ensure_q(nessi_batch *b, int p) {
+    Prob &q = b->probs[p];
+    if (q.qret) return NESSI_OK;
+    const long s2 = (long)q.d.size1 * q.d.size1, nt = q.d.nt, M = q.d.ntau + 1;
+    CKR(b->alloc(&q.qret, tri_h(nt + 1) * s2));
+    CKR(b->alloc(&q.qles, tri_h(nt + 1) * s2));
+    CKR(b->alloc(&q.qtv, (nt + 1) * M * s2));
+    CKR(b->alloc(&q.qmat, M * s2));
+    return sync_probdev(b, p);
+}
+
+int nessi_gpu_set_Q(nessi_batch *b, int p, const void *ret, const void *les, const void *tv, const void *mat) {
+    CKR(check_prob(b, p));
+    CKR(ensure_q(b, p));
+    Prob &q = b->probs[p];
+    const long s2 = (long)q.d.size1 * q.d.size1, nt = q.d.nt, M = q.d.ntau + 1;
+    CKR(copy_cplx(b, q.qret, ret, tri_h(nt + 1) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, q.qles, les, tri_h(nt + 1) * s2, cudaMemcpyHostToDevice));
+    CKR(tv_transfer(b, q.qtv, (void *)tv, 0, nt + 1, (int)M, q.d.size1, true));
+    CKR(copy_cplx(b, q.qmat, mat, M * s2, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_Q_timestep(nessi_batch *b, int p, int tstp, const void *slice) {
+    CKR(check_prob(b, p));
+    CKR(ensure_q(b, p));
+    Prob &q = b->probs[p];
+    return slice_copy(b, q.qret, q.qtv, q.qles, q.qmat, q.d.nt, q.d.ntau, q.d.size1, tstp, (void *)slice, true, true);
+}
+
+static int ensure_fcc(nessi_batch *b, Group &g) {
+    g.vie = true;
+    if (g.fccret) return NESSI_OK;
+    const long s2 = (long)g.s * g.s, N = g.ntmax + 1;
+    CKR(b->alloc(&g.fccret, tri_h(N) * s2));
+    CKR(b->alloc(&g.fccles, tri_h(N) * s2));
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_F(nessi_batch *b, int group, const void *ret, const void *les, const void *tv, const void *mat,
+                    const void *cc_ret, const void *cc_les) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    if (g->U) { set_err("set_F: group %d is a lattice (Dyson) group", group); return NESSI_ERR_ARG; }
+    CKR(ensure_fcc(b, *g));
+    const long s2 = (long)g->s * g->s, N = g->ntmax + 1, M = g->ntau + 1;
+    CKR(copy_cplx(b, g->sret, ret, tri_h(N) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g->sles, les, tri_h(N) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g->stv, tv, N * M * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g->smat, mat, M * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g->fccret, cc_ret, tri_h(N) * s2, cudaMemcpyHostToDevice));
+    CKR(copy_cplx(b, g->fccles, cc_les, tri_h(N) * s2, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
+    g->ret_valid = g->les_valid = g->dense_valid = -1;
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_F_timestep(nessi_batch *b, int group, int tstp, const void *slice, const void *cc_slice) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    if (g->U) { set_err("set_F_timestep: group %d is a lattice (Dyson) group", group); return NESSI_ERR_ARG; }
+    CKR(ensure_fcc(b, *g));
+    CKR(slice_copy(b, g->sret, g->stv, g->sles, g->smat, g->ntmax, g->ntau, g->s, tstp, (void *)slice, true, false));
+    if (tstp >= 0) {
+        // the ret and les parts of the Fcc slice; its tv part is not used by the VIE2 step
+        if (!cc_slice) { set_err("set_F_timestep: null Fcc slice"); return NESSI_ERR_ARG; }
+        const long s2 = (long)g->s * g->s, n1 = tstp + 1, M = g->ntau + 1;
+        const double2 *h = (const double2 *)cc_slice;
+        CKR(copy_cplx(b, g->fccret + tri_h(tstp) * s2, h, n1 * s2, cudaMemcpyHostToDevice));
+        CKR(copy_cplx(b, g->fccles + tri_h(tstp) * s2, h + (n1 + M) * s2, n1 * s2, cudaMemcpyHostToDevice));
+        CK(cudaStreamSynchronize(b->stream));
+        sigma_changed(*g, tstp);
+    }
+    return NESSI_OK;
+}
+
 
 static int ensure_loc(nessi_batch *b, Group &g) {
     if (g.loc.ret) return NESSI_OK;
@@ -838,6 +974,7 @@ int nessi_gpu_set_U(nessi_batch *b, int group, const void *U) {
     Group *g;
     CKR(find_group_checked(b, group, &g));
     if (!U) { set_err("null U"); return NESSI_ERR_ARG; }
+    if (g->vie) { set_err("set_U: group %d is a VIE2 group", group); return NESSI_ERR_ARG; }
     CKR(ensure_loc(b, *g));
     if (!g->U) CKR(b->alloc(&g->U, (long)(g->ntmax + 2) * g->s));
     CKR(copy_cplx(b, g->U, U, (long)(g->ntmax + 2) * g->s, cudaMemcpyHostToDevice));

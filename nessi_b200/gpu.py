@@ -60,6 +60,13 @@ EXPORTS = {
     "nessi_gpu_dyson_mat_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p]),
+    "nessi_gpu_set_F": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 6),
+    "nessi_gpu_set_F_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
+    "nessi_gpu_set_Q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_set_Q_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "nessi_gpu_vie2_start": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_vie2_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_set_U": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "nessi_gpu_extrapolate_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_gloc_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
@@ -181,6 +188,32 @@ class Batch:
 
     def synchronize(self):
         _check(load_library().nessi_gpu_synchronize(self._h))
+
+    # ---- VIE2: [1 + F] G = Q ---------------------------------------------------------
+    def set_F(self, group, F, Fcc):
+        """Kernel F of a group (and its partner Fcc); makes the group a VIE2 group."""
+        _check(load_library().nessi_gpu_set_F(self._h, group, _ptr(F.ret), _ptr(F.les), _ptr(F.tv), _ptr(F.mat),
+                                              _ptr(Fcc.ret), _ptr(Fcc.les)))
+
+    def set_F_timestep(self, group, tstp, F_slice, Fcc_slice=None):
+        fs = np.ascontiguousarray(F_slice, np.complex128)
+        cs = None if Fcc_slice is None else np.ascontiguousarray(Fcc_slice, np.complex128)
+        _check(load_library().nessi_gpu_set_F_timestep(self._h, group, tstp, _ptr(fs), _ptr(cs)))
+
+    def set_Q(self, p, Q):
+        _check(load_library().nessi_gpu_set_Q(self._h, p, _ptr(Q.ret), _ptr(Q.les), _ptr(Q.tv), _ptr(Q.mat)))
+
+    def set_Q_timestep(self, p, tstp, data):
+        _check(load_library().nessi_gpu_set_Q_timestep(self._h, p, tstp, _ptr(np.ascontiguousarray(data,
+                                                                                                    np.complex128))))
+
+    def vie2_start(self):
+        """Time steps 0..k of every VIE2 problem (cntr::vie2_start)."""
+        _check(load_library().nessi_gpu_vie2_start(self._h))
+
+    def vie2_timestep(self, n):
+        """cntr::vie2_timestep(n, ...) for every VIE2 problem."""
+        _check(load_library().nessi_gpu_vie2_timestep(self._h, n))
 
     # ---- self-consistent lattice ----------------------------------------------------
     def set_U(self, group, U):
