@@ -186,6 +186,23 @@ int nessi_gpu_lattice_2b_start(nessi_batch *b, int max_iter, double tol, int *it
  * then G_loc(n) of the final G. */
 int nessi_gpu_lattice_2b_timestep(nessi_batch *b, int n, int corrector_steps);
 
+/* ---- convolution on device-resident herm_matrix data ----------------------------------------
+ * cntr::convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder)
+ * (cntr_convolution_decl.hpp:61, cntr_convolution_impl.hpp:1582-1803): time step n of C = A * B,
+ * for `count` independent problems at once; n = -1 gives cntr::convolution_matsubara
+ * (C^mat = A^mat * B^mat, :560-605).  Every pointer is a caller-owned DEVICE pointer to a
+ * herm_matrix component in libcntr's layout (tv as (t(ntau+1)+tau) s^2, not the batch's planes);
+ * all problems have the same nt, ntau, size1.  Acc and Bcc are the hermitian-conjugate partners
+ * (pass A and B again for hermitian functions).  Writes C's time step n only; queued on `stream`
+ * (NULL = legacy default stream), the call returns without waiting and allocates nothing. */
+typedef struct {
+    void *ret, *les, *tv, *mat;
+} nessi_hm_ptrs;
+int nessi_gpu_convolution_timestep(int n, int count, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                   const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc,
+                                   int nt, int ntau, int size1, int sig_a, int sig_b, int solve_order, double beta,
+                                   double h, void *stream);
+
 /* Wait for all work queued on the batch. */
 int nessi_gpu_synchronize(nessi_batch *b);
 

@@ -15,6 +15,7 @@
 #include "kernels_start.cuh"
 #include "kernels_mat.cuh"
 #include "kernels_lattice.cuh"
+#include "kernels_conv.cuh"
 
 
 
@@ -1230,4 +1231,82 @@ extern "C" int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int sol
     }
     set_err("dyson_mat_noalloc: size1 %d unsupported", size1);
     return NESSI_ERR_ARG;
+}
+
+// =====================================================================================
+// convolution_timestep on device-resident herm_matrix data
+// =====================================================================================
+namespace {
+template <int S> int conv_launch(const ConvBatch &cb, int n, cudaStream_t st) {
+    const long s2 = (long)S * S, M = cb.ntau + 1;
+    auto blocks = [](long items) { return (unsigned)std::min<long>(std::max<long>(1, (items + 127) / 128), 1024); };
+    if (n < 0) {
+        k_conv_mat<S><<<dim3(blocks(M * s2), cb.count), 128, 0, st>>>(cb);
+        CK(cudaGetLastError());
+        return NESSI_OK;
+    }
+    k_conv_ret<S><<<dim3(blocks((n + 1) * s2), cb.count), 128, 0, st>>>(cb, n);
+    CK(cudaGetLastError());
+    k_conv_tv<S><<<dim3(blocks(M * s2), cb.count), 128, 0, st>>>(cb, n);
+    CK(cudaGetLastError());
+    k_conv_les<S><<<dim3(blocks((n + 1) * s2), cb.count), 128, 0, st>>>(cb, n);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+}  // namespace
+
+extern "C" int nessi_gpu_convolution_timestep(int n, int count, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                              const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B,
+                                              const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a,
+                                              int sig_b, int solve_order, double beta, double h, void *stream) {
+    if (count < 0 || !C || !A || !Acc || !B || !Bcc) { set_err("convolution_timestep: bad arguments"); return NESSI_ERR_ARG; }
+    if (size1 < 1 || size1 > NESSI_MAXS || solve_order < 1 || solve_order > CNTR_KMAX || nt < solve_order ||
+        ntau < solve_order || n < -1 || n > nt || (sig_a != 1 && sig_a != -1) || (sig_b != 1 && sig_b != -1) ||
+        !(beta > 0) || !(h > 0)) {
+        set_err("convolution_timestep: bad dimensions (n=%d nt=%d ntau=%d size1=%d k=%d)", n, nt, ntau, size1,
+                solve_order);
+        return NESSI_ERR_ARG;
+    }
+    for (int i = 0; i < count; i++) {
+        const nessi_hm_ptrs *all[5] = {&C[i], &A[i], &Acc[i], &B[i], &Bcc[i]};
+        bool ok = B[i].mat != nullptr;  // B^mat enters C^tv and C^mat
+        if (n >= 0)
+            for (const nessi_hm_ptrs *x : all) ok = ok && x->ret && x->les && x->tv;
+        else
+            ok = ok && A[i].mat && C[i].mat;
+        if (!ok) { set_err("convolution_timestep: problem %d has a null pointer it needs", i); return NESSI_ERR_ARG; }
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) { set_err("convolution_timestep: device index %d unsupported", dev); return NESSI_ERR_ARG; }
+    CKR(ensure_tables(dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    auto conv = [](const nessi_hm_ptrs &x) {
+        ConvHM y;
+        y.ret = (double2 *)x.ret; y.les = (double2 *)x.les; y.tv = (double2 *)x.tv; y.mat = (double2 *)x.mat;
+        return y;
+    };
+    for (int i0 = 0; i0 < count; i0 += NESSI_CONV_MAXP) {
+        ConvBatch cb;
+        std::memset(&cb, 0, sizeof cb);
+        cb.count = std::min(NESSI_CONV_MAXP, count - i0);
+        for (int i = 0; i < cb.count; i++) {
+            cb.p[i].C = conv(C[i0 + i]); cb.p[i].A = conv(A[i0 + i]); cb.p[i].Acc = conv(Acc[i0 + i]);
+            cb.p[i].B = conv(B[i0 + i]); cb.p[i].Bcc = conv(Bcc[i0 + i]);
+        }
+        cb.ntau = ntau; cb.sig_a = sig_a; cb.sig_b = sig_b; cb.k = solve_order; cb.h = h; cb.beta = beta;
+        int r = NESSI_ERR_ARG;
+        switch (size1) {
+            case 1: r = conv_launch<1>(cb, n, st); break;
+            case 2: r = conv_launch<2>(cb, n, st); break;
+            case 3: r = conv_launch<3>(cb, n, st); break;
+            case 4: r = conv_launch<4>(cb, n, st); break;
+            case 5: r = conv_launch<5>(cb, n, st); break;
+            case 6: r = conv_launch<6>(cb, n, st); break;
+            case 7: r = conv_launch<7>(cb, n, st); break;
+            case 8: r = conv_launch<8>(cb, n, st); break;
+        }
+        if (r != NESSI_OK) return r;
+    }
+    return NESSI_OK;
 }

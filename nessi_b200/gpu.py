@@ -38,6 +38,11 @@ class ProblemDesc(ctypes.Structure):
                 ("beta", ctypes.c_double), ("h", ctypes.c_double), ("mu", ctypes.c_double)]
 
 
+class HmPtrs(ctypes.Structure):
+    """Device pointers of one herm_matrix (nessi_hm_ptrs)."""
+    _fields_ = [("ret", ctypes.c_void_p), ("les", ctypes.c_void_p), ("tv", ctypes.c_void_p), ("mat", ctypes.c_void_p)]
+
+
 EXPORTS = {
     "nessi_gpu_init": (ctypes.c_int, [ctypes.c_int]),
     "nessi_gpu_last_error": (ctypes.c_char_p, []),
@@ -76,6 +81,8 @@ EXPORTS = {
     "nessi_gpu_lattice_2b_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "nessi_gpu_lattice_2b_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "nessi_gpu_convolution_timestep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 5 +
+                                       [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
@@ -269,6 +276,24 @@ def dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, H_ptr, sigma_mat_
     _check(load_library().nessi_gpu_dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, ctypes.c_void_p(H_ptr),
                                                        ctypes.c_void_p(sigma_mat_ptr), ctypes.c_void_p(gmat_ptr),
                                                        ctypes.c_void_p(stream) if stream else None))
+
+
+def convolution_timestep_dev(n, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, stream=0):
+    """cntr::convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder) for len(C) problems on
+    device memory.  Each of C, A, Acc, B, Bcc is a list of (ret, les, tv, mat) device pointers
+    (integers, libcntr layout).  Queued on ``stream``; allocates nothing."""
+    if not _inited:
+        init(0)
+    cnt = len(C)
+
+    def arr(lst):
+        a = (HmPtrs * max(cnt, 1))()
+        for i, t in enumerate(lst):
+            a[i] = HmPtrs(*[ctypes.c_void_p(x) if x else None for x in t])
+        return a
+    _check(load_library().nessi_gpu_convolution_timestep(n, cnt, arr(C), arr(A), arr(Acc), arr(B), arr(Bcc), nt, ntau,
+                                                         size1, sig_a, sig_b, solve_order, beta, h,
+                                                         ctypes.c_void_p(stream) if stream else None))
 
 
 # ---- cntr-style single-problem entry points ---------------------------------------------
