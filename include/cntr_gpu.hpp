@@ -70,6 +70,25 @@ template <class HM, class FN> class Batch {
     void set_sigma_timestep(int n, const std::complex<double> *slice, int sigma_group = 0) {
         check(nessi_gpu_set_sigma_timestep(b_, sigma_group, n, slice));
     }
+    // VIE2 groups: kernel F (with partner Fcc) shared by the group, source Q per problem
+    void set_F(HM &F, HM &Fcc, int group = 0) {
+        check(nessi_gpu_set_F(b_, group, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0),
+                              Fcc.retptr(0, 0), Fcc.lesptr(0, 0)));
+    }
+    void set_Q(int p, HM &Q) {
+        check(nessi_gpu_set_Q(b_, p, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0)));
+    }
+    void vie2_start() { check(nessi_gpu_vie2_start(b_)); }
+    void vie2_timestep(int n) { check(nessi_gpu_vie2_timestep(b_, n)); }
+    // self-consistent lattice with the local second-order self-energy of G_loc
+    void set_U(const std::complex<double> *udiag, int group = 0) { check(nessi_gpu_set_U(b_, group, udiag)); }
+    void extrapolate_timestep(int n) { check(nessi_gpu_extrapolate_timestep(b_, n)); }
+    int lattice_2b_start(int max_iter, double tol, double *err = nullptr) {
+        int it = 0;
+        check(nessi_gpu_lattice_2b_start(b_, max_iter, tol, &it, err));
+        return it;
+    }
+    void lattice_2b_timestep(int n, int corrector_steps) { check(nessi_gpu_lattice_2b_timestep(b_, n, corrector_steps)); }
     void dyson_mat() { check(nessi_gpu_dyson_mat(b_)); }
     void dyson_start() { check(nessi_gpu_dyson_start(b_)); }
     void dyson_timestep(int n) { check(nessi_gpu_dyson_timestep(b_, n)); }
@@ -130,6 +149,59 @@ void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder =
     b.build(Sigma);
     b.dyson_mat();
     b.download_timestep(0, -1);
+}
+
+// ---- VIE2 single-problem drop-ins (cntr_vie2_decl.hpp:67-72) --------------------------------
+template <class HM>
+void vie2_start(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5) {
+    nessi_problem_desc d;
+    d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = h; d.mu = 0.0;
+    nessi_batch *b = nullptr;
+    check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
+    int rc = nessi_gpu_set_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
+    if (!rc) rc = nessi_gpu_set_F(b, 0, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0), Fcc.retptr(0, 0),
+                                  Fcc.lesptr(0, 0));
+    if (!rc) rc = nessi_gpu_set_Q(b, 0, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0));
+    if (!rc) rc = nessi_gpu_vie2_start(b);
+    if (!rc) rc = nessi_gpu_get_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), nullptr);
+    nessi_gpu_batch_destroy(b);
+    check(rc);
+}
+
+template <class HM>
+void vie2_timestep(int n, HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5) {
+    nessi_problem_desc d;
+    d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = h; d.mu = 0.0;
+    nessi_batch *b = nullptr;
+    check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
+    int rc = nessi_gpu_set_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0));
+    if (!rc) rc = nessi_gpu_set_F(b, 0, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0), Fcc.retptr(0, 0),
+                                  Fcc.lesptr(0, 0));
+    if (!rc) rc = nessi_gpu_set_Q(b, 0, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0));
+    if (!rc) rc = nessi_gpu_vie2_timestep(b, n);
+    std::vector<std::complex<double>> s(slice_len(G, n));
+    if (!rc) rc = nessi_gpu_get_timestep(b, 0, n, s.data());
+    nessi_gpu_batch_destroy(b);
+    check(rc);
+    const long es = (long)G.size1() * G.size1(), n1 = n + 1, M = G.ntau() + 1;
+    std::copy(s.begin(), s.begin() + n1 * es, G.retptr(n, 0));
+    std::copy(s.begin() + n1 * es, s.begin() + (n1 + M) * es, G.tvptr(n, 0));
+    std::copy(s.begin() + (n1 + M) * es, s.end(), G.lesptr(0, n));
+}
+
+// ---- convolution_timestep (cntr_convolution_decl.hpp:61) --------------------------------
+template <class HM>
+void convolution_timestep(int n, HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta, double h, int SolveOrder = 5) {
+    auto p = [](HM &X) {
+        nessi_hm_ptrs q;
+        q.ret = X.retptr(0, 0); q.les = X.lesptr(0, 0); q.tv = X.tvptr(0, 0); q.mat = X.matptr(0);
+        return q;
+    };
+    nessi_hm_ptrs c = p(C), a = p(A), acc = p(Acc), b = p(B), bcc = p(Bcc);
+    check(nessi_gpu_convolution_timestep_host(n, &c, &a, &acc, &b, &bcc, C.nt(), C.ntau(), C.size1(), A.sig(), B.sig(),
+                                              SolveOrder, beta, h));
 }
 
 }  // namespace cntr_gpu

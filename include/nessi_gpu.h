@@ -203,6 +203,14 @@ int nessi_gpu_convolution_timestep(int n, int count, const nessi_hm_ptrs *C, con
                                    int nt, int ntau, int size1, int sig_a, int sig_b, int solve_order, double beta,
                                    double h, void *stream);
 
+/* The same on HOST herm_matrix data (libcntr layout): copies A, Acc, B, Bcc and C to the device,
+ * computes time step n and writes C's time step n back; allocates and frees device memory and
+ * waits for completion.  For single calls with libcntr's signature (cntr_gpu.hpp). */
+int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                        const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc,
+                                        int nt, int ntau, int size1, int sig_a, int sig_b, int solve_order,
+                                        double beta, double h);
+
 /* Wait for all work queued on the batch. */
 int nessi_gpu_synchronize(nessi_batch *b);
 

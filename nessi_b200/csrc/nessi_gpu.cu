@@ -1310,3 +1310,57 @@ extern "C" int nessi_gpu_convolution_timestep(int n, int count, const nessi_hm_p
     }
     return NESSI_OK;
 }
+
+// Host-data convenience for single calls with libcntr's signature: copies the five herm_matrix
+// objects to the device, runs the convolution for time step n and copies C's time step back.
+extern "C" int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                                   const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B,
+                                                   const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a,
+                                                   int sig_b, int solve_order, double beta, double h) {
+    if (!C || !A || !Acc || !B || !Bcc || nt < 0 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS) {
+        set_err("convolution_timestep_host: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    CK(cudaSetDevice(g_device));
+    const long s2 = (long)size1 * size1, M = ntau + 1;
+    const long len[4] = {tri_h(nt + 1) * s2, tri_h(nt + 1) * s2, (long)(nt + 1) * M * s2, M * s2};
+    const nessi_hm_ptrs *hs[5] = {C, A, Acc, B, Bcc};
+    nessi_hm_ptrs ds[5];
+    std::vector<void *> owned;
+    int rc = NESSI_OK;
+    for (int i = 0; i < 5 && rc == NESSI_OK; i++) {
+        void **dst[4] = {&ds[i].ret, &ds[i].les, &ds[i].tv, &ds[i].mat};
+        void *const src[4] = {hs[i]->ret, hs[i]->les, hs[i]->tv, hs[i]->mat};
+        for (int c = 0; c < 4; c++) {
+            *dst[c] = nullptr;
+            if (!src[c]) continue;
+            if (cudaMalloc(dst[c], (size_t)len[c] * 16) != cudaSuccess) { set_err("cudaMalloc failed"); rc = NESSI_ERR_OOM; break; }
+            owned.push_back(*dst[c]);
+            if (cudaMemcpy(*dst[c], src[c], (size_t)len[c] * 16, cudaMemcpyHostToDevice) != cudaSuccess) {
+                set_err("upload failed");
+                rc = NESSI_ERR_CUDA;
+                break;
+            }
+        }
+    }
+    if (rc == NESSI_OK)
+        rc = nessi_gpu_convolution_timestep(n, 1, &ds[0], &ds[1], &ds[2], &ds[3], &ds[4], nt, ntau, size1, sig_a, sig_b,
+                                            solve_order, beta, h, nullptr);
+    if (rc == NESSI_OK && cudaDeviceSynchronize() != cudaSuccess) { set_err("convolution failed"); rc = NESSI_ERR_CUDA; }
+    if (rc == NESSI_OK) {
+        // C's time step n: ret row, tv row, les column (or mat)
+        auto back = [&](void *h, const void *d, long off, long cnt) {
+            return cudaMemcpy((char *)h + off * 16, (const char *)d + off * 16, (size_t)cnt * 16, cudaMemcpyDeviceToHost);
+        };
+        cudaError_t e = cudaSuccess;
+        if (n < 0) e = back(C->mat, ds[0].mat, 0, M * s2);
+        else {
+            e = back(C->ret, ds[0].ret, tri_h(n) * s2, (n + 1) * s2);
+            if (e == cudaSuccess) e = back(C->tv, ds[0].tv, (long)n * M * s2, M * s2);
+            if (e == cudaSuccess) e = back(C->les, ds[0].les, tri_h(n) * s2, (n + 1) * s2);
+        }
+        if (e != cudaSuccess) { set_err("download failed"); rc = NESSI_ERR_CUDA; }
+    }
+    for (void *q : owned) cudaFree(q);
+    return rc;
+}

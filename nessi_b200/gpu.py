@@ -83,6 +83,8 @@ EXPORTS = {
     "nessi_gpu_lattice_2b_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "nessi_gpu_convolution_timestep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 5 +
                                        [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    "nessi_gpu_convolution_timestep_host": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 5 +
+                                            [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
@@ -297,6 +299,18 @@ def convolution_timestep_dev(n, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b
 
 
 # ---- cntr-style single-problem entry points ---------------------------------------------
+def convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder=5):
+    """cntr::convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder) on host herm_matrix
+    objects (cntr_convolution_decl.hpp:61): writes C's time step n (mat for n = -1) in place."""
+    if not _inited:
+        init(0)
+
+    def hp(G):
+        return ctypes.byref(HmPtrs(_ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
+    _check(load_library().nessi_gpu_convolution_timestep_host(n, hp(C), hp(A), hp(Acc), hp(B), hp(Bcc), C.nt, C.ntau,
+                                                              C.size1, A.sig, B.sig, SolveOrder, beta, h))
+
+
 def dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder=5):
     """cntr::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder) on the GPU
     (cntr_dyson_decl.hpp:92): writes G's time step n in place."""

@@ -37,6 +37,10 @@ int main(int argc, char **argv) {
     cntr_gpu::dyson_mat(G, 0.0, H, S, 5.0, 5);
     cntr_gpu::dyson_start(G, 0.0, H, S, 5.0, 0.05, 5);
     cntr_gpu::dyson_timestep(6, G, 0.0, H, S, 5.0, 0.05, 5);
+    HM F(12, 10, 2, -1), Q(12, 10, 2, -1), C(12, 10, 2, -1);
+    cntr_gpu::vie2_start(G, F, F, Q, 5.0, 0.05, 5);
+    cntr_gpu::vie2_timestep(6, G, F, F, Q, 5.0, 0.05, 5);
+    cntr_gpu::convolution_timestep(6, C, G, G, S, S, 5.0, 0.05, 5);
     return 0;
 }
 '''

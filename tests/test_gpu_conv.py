@@ -112,3 +112,18 @@ def test_convolution_rejects_bad_arguments():
                                      [(0, 0, 0, 0)], 10, 8, 1, -1, -1, 5, 3.0, 0.05)
     with pytest.raises(gpu.NessiGpuError):
         gpu.convolution_timestep_dev(11, [], [], [], [], [], 10, 8, 1, -1, -1, 5, 3.0, 0.05)
+
+
+def test_convolution_host_dropin(oracle):
+    """gpu.convolution_timestep with libcntr's signature on host herm_matrix objects."""
+    from nessi_b200 import gpu
+    rng = np.random.default_rng(9)
+    nt, ntau, beta, h, k, s = 10, 8, 2.0, 0.05, 5, 2
+    A, Acc = _pair(oracle, rng, nt, ntau, s, -1, beta, h, k)
+    B = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.8)
+    C, R = herm_matrix(nt, ntau, s, -1), herm_matrix(nt, ntau, s, -1)
+    for n in range(-1, nt + 1):
+        gpu.convolution_timestep(n, C, A, Acc, B, B, beta, h, k)
+        oracle.convolution_timestep(n, R, A, Acc, B, B, beta, h, k)
+    for comp in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(C, comp), getattr(R, comp)) < TOL, comp
