@@ -166,6 +166,10 @@ def build_workload(name, rank, world):
         return workloads.config1(nk=64, nt=200, ntau=100, kshift=shift)
     if name == "config1-ncu":  # config-1 chain at nt=ntau=300: 1.5 GB of G^tv history, > L2
         return workloads.config1(nk=256, nt=300, ntau=300, kshift=shift)
+    if name == "config3":  # 96 uneven problems; ranks draw their own problems (seed + rank)
+        return workloads.config3(seed=20261203 + rank)
+    if name == "config3-small":
+        return workloads.uneven(nprob=24, nt_range=(100, 400), ntau=100, seed=20261203 + rank)
     if name == "config4":
         return workloads.config4(kshift=shift)
     if name == "config4-small":  # 16x16 lattice, nt=400, ntau=200: quick checks of the lattice path
@@ -235,6 +239,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="launch every step eagerly instead of replaying "
+                    "a CUDA graph of the propagation")
     args = ap.parse_args()
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
@@ -269,7 +275,22 @@ def main():
     for _ in range(args.warmup):
         propagate()
     b.synchronize()
-    b.set_profiling(True)
+    use_graph = not args.no_graph
+    if use_graph:
+        # per-kernel device times from one eager propagation (untimed); then the propagation is
+        # recorded once as a CUDA graph and every timed step replays it
+        b.set_profiling(True)
+        propagate()
+        b.synchronize()
+        prof = b.read_profile()
+        b.set_profiling(False)
+        b.graph_record(b.GRAPH_LATTICE if W.lattice else b.GRAPH_DYSON, k + 1, nt, W.ncorr or 3)
+        run_step = b.graph_launch
+        run_step()  # first replay outside the timed region
+        b.synchronize()
+    else:
+        b.set_profiling(True)
+        run_step = propagate
     clocks = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -277,14 +298,16 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        propagate()
+        run_step()
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
     ms = allmax(e0.elapsed_time(e1), world)
-    prof = b.read_profile()
-    b.set_profiling(False)
+    if not use_graph:
+        prof = b.read_profile()
+        b.set_profiling(False)
+    prof_steps = 1 if use_graph else args.steps
     units = world * W.kpt_steps() * args.steps
     value = units / (ms / 1000.0)
     kernels_per_step = 7  # prep_problem, prep_group, ret, mat_operator, tv, les_operands, les
@@ -310,7 +333,7 @@ def main():
                                 "scaled to this launch's algorithmic bytes",
                 "algorithmic_bytes_per_launch": dbytes / dl if dl else None,
                 "avg_launch_ms": dms / dl if dl else None}
-    breakdown = {kname: {"ms": v[0] / args.steps, "launches": v[1] // args.steps,
+    breakdown = {kname: {"ms": v[0] / prof_steps, "launches": v[1] // prof_steps,
                          "share": v[0] / max(1e-9, sum(x[0] for x in prof.values()))}
                  for kname, v in prof.items()}
 
@@ -318,8 +341,10 @@ def main():
     e2e = None
     if not args.no_e2e:
         from nessi_b200 import herm_matrix
+        # the uneven batch holds ~135 GB of G: its result is the last time step of every problem
+        last_only = W.name == "uneven"
         host = []
-        for d in (W.descs[:1] if W.lattice else W.descs):
+        for d in (W.descs[:1] if (W.lattice or last_only) else W.descs):
             host.append(herm_matrix(d["nt"], d["ntau"], d["size1"], d["sig"]))
         try:
             import torch as _t
@@ -341,6 +366,10 @@ def main():
             gloc_host = host[0]
             last = np.zeros((len(W.descs), 2 * (nt + 1) + d0["ntau"] + 1, d0["size1"], d0["size1"]), np.complex128)
             d2h = sum(getattr(gloc_host, x).nbytes for x in ("ret", "les", "tv", "mat")) + last.nbytes
+        elif last_only:
+            lasts = [np.zeros((2 * (d["nt"] + 1) + d["ntau"] + 1, d["size1"], d["size1"]), np.complex128)
+                     for d in W.descs]
+            d2h = sum(a.nbytes for a in lasts)
         else:
             d2h = sum(G.ret.nbytes + G.les.nbytes + G.tv.nbytes + G.mat.nbytes for G in host)
         barrier(world)
@@ -351,11 +380,14 @@ def main():
             workloads.upload(b, W)
             if W.lattice:
                 b.lattice_2b_start(max_iter=30, tol=1e-12)
-            propagate()
+            run_step()
             if W.lattice:
                 b.get_gloc(0, gloc_host)
                 for p in range(len(W.descs)):
                     b.get_timestep(p, nt, last[p])
+            elif last_only:
+                for p, d in enumerate(W.descs):
+                    b.get_timestep(p, d["nt"], lasts[p])
             else:
                 for p, G in enumerate(host):
                     b.get_G(p, G)
@@ -367,12 +399,16 @@ def main():
                "d2h_bytes_per_step": int(d2h), "pinned_host": pinned, "ms_per_step": ems / args.steps}
         if W.lattice:
             e2e["includes"] = "upload, self-consistent bootstrap, propagation, download of G_loc and G_k(nt)"
+        elif last_only:
+            e2e["includes"] = "upload of Sigma, H and bootstrap steps, propagation, download of each G_p(nt_p)"
         # sanity: the downloaded result is finite
-        if not all(np.isfinite(G.tv[nt]).all() for G in host[:4]):
+        if not last_only and not all(np.isfinite(G.tv[nt]).all() for G in host[:4]):
             e2e["warning"] = "non-finite values in the result"
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if isinstance(W.sigma, dict):
+        cpu = {"value": None, "note": "not sampled for the multi-size batch; see the config-1 and config-4 lines"}
+    elif rank == 0 and world == 1 and not args.no_cpu:
         v, thr, desc = cpu_sample(W, target_s=args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
 
@@ -384,13 +420,14 @@ def main():
                 "data": "synthetic",
                 "config": dict(workload=args.workload, precision=args.precision,
                                l2="inputs larger than L2 (G^tv history %.1f GB per GPU)" % (
-                                   16.0 * W.nprob * (nt + 1) * (W.descs[0]["ntau"] + 1) * W.descs[0]["size1"] ** 2 / 1e9),
+                                   sum(16.0 * (d["nt"] + 1) * (d["ntau"] + 1) * d["size1"] ** 2 for d in W.descs) / 1e9),
                                bootstrap=("free propagator of H_k(-1) for mat, then %d self-consistent "
                                           "dyson_start iterations (set-up, untimed)" % boot_iters) if W.lattice else
                                "free propagator of H_k(-1) for mat and steps 0..k (set-up, untimed)",
                                **W.info),
                 "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": gpu_launches, "clocks": clk}
+                "gpu_launches": gpu_launches, "clocks": clk,
+                "launch": "CUDA graph of the whole propagation, replayed each step" if use_graph else "eager"}
         print(json.dumps(line), flush=True)
     b.close()
     if world > 1:

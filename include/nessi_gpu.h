@@ -211,6 +211,17 @@ int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nes
                                         int nt, int ntau, int size1, int sig_a, int sig_b, int solve_order,
                                         double beta, double h);
 
+/* ---- CUDA graphs of the per-step launch sequence ---------------------------------------------
+ * Record the launches of time steps n0..n1 (kind 0: dyson_timestep, 1: vie2_timestep,
+ * 2: lattice_2b_timestep with corrector_steps) into a CUDA graph held by the batch, without
+ * executing them; nessi_gpu_graph_launch replays the recording on the batch stream.  A replay
+ * repeats exactly the recorded launches, so it reproduces the steps as long as the inputs they
+ * read (H, a fixed Sigma, the bootstrap steps) are unchanged; record after the batch has run
+ * the same steps once (as a warm-up), so that nothing is set up during the recording.  A new
+ * recording replaces the previous one.  No reference counterpart (libcntr has no streams). */
+int nessi_gpu_graph_record(nessi_batch *b, int kind, int n0, int n1, int corrector_steps);
+int nessi_gpu_graph_launch(nessi_batch *b);
+
 /* Wait for all work queued on the batch. */
 int nessi_gpu_synchronize(nessi_batch *b);
 

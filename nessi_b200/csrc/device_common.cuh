@@ -70,12 +70,27 @@ __device__ __forceinline__ double rcorr_w(int k, int m, int j, int l) {
     return c_tab.rcorr[k][((m - 1) * NESSI_K1MAX + j) * NESSI_K1MAX + l];
 }
 
-// ---- CTA-wide dense solve A X = B (n x n, nrhs columns), partial pivoting ------------
+// ---- execution groups for the small dense block solves --------------------------------------
+// CtaExec: all threads of the block; WarpExec: the 32 lanes of one warp.
+struct CtaExec {
+    __device__ __forceinline__ int t() const { return threadIdx.x; }
+    __device__ __forceinline__ int n() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct WarpExec {
+    int lane;
+    __device__ __forceinline__ int t() const { return lane; }
+    __device__ __forceinline__ int n() const { return 32; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+
+// ---- dense solve A X = B (n x n, nrhs columns), partial pivoting, by an execution group ------
 // A (n x n, row-major, lda = n) and B (n x nrhs, row-major) live in shared memory and
-// are overwritten; on return B holds X.  All threads of the block must call it.
+// are overwritten; on return B holds X.  Every member of the group must call it.
 // Returns nonzero in *status (shared) if a zero pivot was met.
-__device__ inline void cta_solve(double2 *A, double2 *B, int n, int nrhs, int *s_piv, int *status) {
-    const int tid = threadIdx.x, nth = blockDim.x;
+template <class X>
+__device__ inline void grp_solve(const X &x, double2 *A, double2 *B, int n, int nrhs, int *s_piv, int *status) {
+    const int tid = x.t(), nth = x.n();
     for (int c = 0; c < n; c++) {
         if (tid == 0) {
             int p = c;
@@ -87,7 +102,7 @@ __device__ inline void cta_solve(double2 *A, double2 *B, int n, int nrhs, int *s
             *s_piv = p;
             if (best == 0.0) *status = 1;
         }
-        __syncthreads();
+        x.sync();
         int p = *s_piv;
         if (p != c) {
             for (int j = tid; j < n + nrhs; j += nth) {
@@ -99,7 +114,7 @@ __device__ inline void cta_solve(double2 *A, double2 *B, int n, int nrhs, int *s
                 }
             }
         }
-        __syncthreads();
+        x.sync();
         double2 piv = A[c * n + c];
         if (piv.x == 0.0 && piv.y == 0.0) piv = cmk(1.0, 0.0);  // status already flagged
         // eliminate rows below c
@@ -115,18 +130,22 @@ __device__ inline void cta_solve(double2 *A, double2 *B, int n, int nrhs, int *s
                 B[i * nrhs + jj] = csub(B[i * nrhs + jj], cmul(f, B[c * nrhs + jj]));
             }
         }
-        __syncthreads();
+        x.sync();
         // column c below the pivot is no longer needed (implicit zeros)
     }
-    // back substitution, one rhs column per thread group
+    // back substitution, one rhs column per thread
     for (int i = n - 1; i >= 0; i--) {
         for (int j = tid; j < nrhs; j += nth) {
             double2 acc = B[i * nrhs + j];
             for (int l = i + 1; l < n; l++) acc = csub(acc, cmul(A[i * n + l], B[l * nrhs + j]));
             B[i * nrhs + j] = cdiv(acc, A[i * n + i].x == 0.0 && A[i * n + i].y == 0.0 ? cmk(1, 0) : A[i * n + i]);
         }
-        __syncthreads();
+        x.sync();
     }
+}
+
+__device__ inline void cta_solve(double2 *A, double2 *B, int n, int nrhs, int *s_piv, int *status) {
+    grp_solve(CtaExec{}, A, B, n, nrhs, s_piv, status);
 }
 
 // Invert an s x s complex matrix held by one thread (Gauss-Jordan, partial pivoting).

@@ -132,8 +132,8 @@ __global__ void k_prep_group(GroupDev g, int n, int d_lo) {
 // dyson_timestep_les (:926-982), solved by the whole CTA in shared memory.
 // ---------------------------------------------------------------------------------------
 // ret: unknowns X_q = G(n, n-q-1); equations sum_q X_q mm(p,q) = qq(p)  (left solve)
-template <int S>
-__device__ void ret_start_block(const GroupDev &g, const ProbDev &p, int n, double2 *smem) {
+template <int S, class X = CtaExec>
+__device__ void ret_start_block(const GroupDev &g, const ProbDev &p, int n, double2 *smem, const X &x = X()) {
     const int k = g.k, s2 = S * S, KS = k * S;
     const double h = g.h;
     double2 *mm = smem;                 // k*k blocks (block (p,q) at (p*k+q)*s2)
@@ -143,12 +143,12 @@ __device__ void ret_start_block(const GroupDev &g, const ProbDev &p, int n, doub
     int *ipiv = (int *)(R + KS * S);
     int *status = ipiv + 1;
     double2 *grow = p.gret + tri(n) * s2;  // G(n, .)
-    for (int e = threadIdx.x; e < k * k * s2; e += blockDim.x) mm[e] = cmk(0, 0);
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) qq[e] = cmk(0, 0);
-    if (threadIdx.x == 0) *status = 0;
-    __syncthreads();
+    for (int e = x.t(); e < k * k * s2; e += x.n()) mm[e] = cmk(0, 0);
+    for (int e = x.t(); e < k * s2; e += x.n()) qq[e] = cmk(0, 0);
+    if (x.t() == 0) *status = 0;
+    x.sync();
     // thread per (row-block pr, element ab): fills block row pr of mm and qq(pr)
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+    for (int e = x.t(); e < k * s2; e += x.n()) {
         int pr = e / s2, ab = e % s2, a = ab / S, b = ab % S;
         int j = pr + 1;
         double2 q = cmk(0, 0);
@@ -184,25 +184,25 @@ __device__ void ret_start_block(const GroupDev &g, const ProbDev &p, int n, doub
         }
         qq[pr * s2 + ab] = q;
     }
-    __syncthreads();
+    x.sync();
     // conjugate-transpose to a right solve: A[(pr,a),(q,b)] = conj(mm(pr,q)[b][a]),
     // R[(pr,a),c] = conj(qq(pr)[c][a])
-    for (int e = threadIdx.x; e < KS * KS; e += blockDim.x) {
+    for (int e = x.t(); e < KS * KS; e += x.n()) {
         int r = e / KS, c = e % KS, pr = r / S, a = r % S, q = c / S, b = c % S;
         A[e] = cconj(mm[(pr * k + q) * s2 + b * S + a]);
     }
-    for (int e = threadIdx.x; e < KS * S; e += blockDim.x) {
+    for (int e = x.t(); e < KS * S; e += x.n()) {
         int r = e / S, c = e % S, pr = r / S, a = r % S;
         R[e] = cconj(qq[pr * s2 + c * S + a]);
     }
-    __syncthreads();
-    cta_solve(A, R, KS, S, ipiv, status);
+    x.sync();
+    grp_solve(x, A, R, KS, S, ipiv, status);
     // X_q[a][c] = conj(Y[(q,c), a]) -> G(n, n-q-1)
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+    for (int e = x.t(); e < k * s2; e += x.n()) {
         int q = e / s2, ac = e % s2, a = ac / S, c = ac % S;
         grow[(long)(n - q - 1) * s2 + ac] = cconj(R[(q * S + c) * S + a]);
     }
-    __syncthreads();
+    x.sync();
 }
 
 // VIE2 ret (vie2_timestep_ret, cntr_vie2_impl.hpp:60-140, called with F and Fcc swapped):
@@ -210,8 +210,8 @@ __device__ void ret_start_block(const GroupDev &g, const ProbDev &p, int n, doub
 //   sum_q X_q mm(p,q) = qq(p),  mm(p,q) = 1 delta_pq + h w(j,l) F'(n-l, n-j) [l = q+1]
 //   qq(p) = Q(n, n-j) - h w(j,0) G(n,n) F'(n, n-j),  j = p+1,
 // F'(t,t') = Fcc^R(t,t') for t >= t' and F^R(t',t)^dagger otherwise (sign folded into w).
-template <int S>
-__device__ void ret_start_block_vie(const GroupDev &g, const ProbDev &p, int n, double2 *smem) {
+template <int S, class X = CtaExec>
+__device__ void ret_start_block_vie(const GroupDev &g, const ProbDev &p, int n, double2 *smem, const X &x = X()) {
     const int k = g.k, s2 = S * S, KS = k * S;
     const double h = g.h;
     double2 *mm = smem;
@@ -221,10 +221,10 @@ __device__ void ret_start_block_vie(const GroupDev &g, const ProbDev &p, int n, 
     int *ipiv = (int *)(R + KS * S);
     int *status = ipiv + 1;
     double2 *grow = p.gret + tri(n) * s2;
-    for (int e = threadIdx.x; e < k * k * s2; e += blockDim.x) mm[e] = cmk(0, 0);
-    if (threadIdx.x == 0) *status = 0;
-    __syncthreads();
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+    for (int e = x.t(); e < k * k * s2; e += x.n()) mm[e] = cmk(0, 0);
+    if (x.t() == 0) *status = 0;
+    x.sync();
+    for (int e = x.t(); e < k * s2; e += x.n()) {
         const int pr = e / s2, ab = e % s2, a = ab / S, b = ab % S, j = pr + 1;
         double2 q = p.qret[(tri(n) + n - j) * s2 + ab];
         if (a == b) mm[(pr * k + pr) * s2 + ab] = cadd(mm[(pr * k + pr) * s2 + ab], cmk(1.0, 0.0));
@@ -246,38 +246,38 @@ __device__ void ret_start_block_vie(const GroupDev &g, const ProbDev &p, int n, 
         }
         qq[pr * s2 + ab] = q;
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < KS * KS; e += blockDim.x) {
+    x.sync();
+    for (int e = x.t(); e < KS * KS; e += x.n()) {
         int r = e / KS, c = e % KS, pr = r / S, a = r % S, q = c / S, b = c % S;
         A[e] = cconj(mm[(pr * k + q) * s2 + b * S + a]);
     }
-    for (int e = threadIdx.x; e < KS * S; e += blockDim.x) {
+    for (int e = x.t(); e < KS * S; e += x.n()) {
         int r = e / S, c = e % S, pr = r / S, a = r % S;
         R[e] = cconj(qq[pr * s2 + c * S + a]);
     }
-    __syncthreads();
-    cta_solve(A, R, KS, S, ipiv, status);
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+    x.sync();
+    grp_solve(x, A, R, KS, S, ipiv, status);
+    for (int e = x.t(); e < k * s2; e += x.n()) {
         int q = e / s2, ac = e % s2, a = ac / S, c = ac % S;
         grow[(long)(n - q - 1) * s2 + ac] = cconj(R[(q * S + c) * S + a]);
     }
-    __syncthreads();
+    x.sync();
 }
 
 // VIE2 les (vie2_timestep_les, cntr_vie2_impl.hpp:847-990): unknowns x_j = G^<(j,n), j = 0..k;
 //   sum_m mm(j,m) x_m = gl(j) + Q^<(j,n),  mm(j,m) = 1 delta_jm + h w(j,m) F'(j,m),
 // F'(j,m) = F^R(j,m) for j >= m and -Fcc^R(m,j)^dagger otherwise (right solve).
-template <int S>
+template <int S, class X = CtaExec>
 __device__ void les_start_block_vie(const GroupDev &g, const ProbDev &p, int n, const double2 *gl, long ldc,
-                                    double2 *xcol, double2 *smem) {
+                                    double2 *xcol, double2 *smem, const X &x = X()) {
     const int k = g.k, K1 = k + 1, s2 = S * S, KS = K1 * S;
     const double h = g.h;
     double2 *A = smem;
     double2 *R = A + KS * KS;
     int *ipiv = (int *)(R + KS * S);
     int *status = ipiv + 1;
-    if (threadIdx.x == 0) *status = 0;
-    for (int e = threadIdx.x; e < K1 * s2; e += blockDim.x) {
+    if (x.t() == 0) *status = 0;
+    for (int e = x.t(); e < K1 * s2; e += x.n()) {
         const int j = e / s2, ad = e % s2, a = ad / S, d = ad % S;
         double2 q = gl[((long)j * S + a) * ldc + d];
         q = cadd(q, j <= n ? p.qles[(tri(n) + j) * s2 + ad] : cneg(cconj(p.qles[(tri(j) + n) * s2 + d * S + a])));
@@ -295,30 +295,30 @@ __device__ void les_start_block_vie(const GroupDev &g, const ProbDev &p, int n, 
             }
         }
     }
-    __syncthreads();
-    cta_solve(A, R, KS, S, ipiv, status);
-    for (int e = threadIdx.x; e < K1 * s2; e += blockDim.x) {
+    x.sync();
+    grp_solve(x, A, R, KS, S, ipiv, status);
+    for (int e = x.t(); e < K1 * s2; e += x.n()) {
         const int j = e / s2, ad = e % s2, a = ad / S, d = ad % S;
         xcol[(long)j * s2 + ad] = R[(j * S + a) * S + d];
     }
-    __syncthreads();
+    x.sync();
 }
 
 // les: unknowns x_j = G^<(j,n), j = 1..k; sum_q mm(p,q) x_{q+1} = qq(p)  (right solve)
-template <int S>
+template <int S, class X = CtaExec>
 __device__ void les_start_block(const GroupDev &g, const ProbDev &p, int n, const double2 *gl, long ldc,
-                                double2 *xcol, double2 *smem) {
+                                double2 *xcol, double2 *smem, const X &x = X()) {
     const int k = g.k, s2 = S * S, KS = k * S;
     const double h = g.h;
     double2 *A = smem;           // (KS x KS)
     double2 *R = A + KS * KS;    // (KS x S)
     int *ipiv = (int *)(R + KS * S);
     int *status = ipiv + 1;
-    if (threadIdx.x == 0) *status = 0;
-    for (int e = threadIdx.x; e < KS * KS; e += blockDim.x) A[e] = cmk(0, 0);
-    __syncthreads();
+    if (x.t() == 0) *status = 0;
+    for (int e = x.t(); e < KS * KS; e += x.n()) A[e] = cmk(0, 0);
+    x.sync();
     // thread per (pr, a, d): qq(pr)[a][d] and the row (pr,a) of A
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+    for (int e = x.t(); e < k * s2; e += x.n()) {
         int pr = e / s2, ad = e % s2, a = ad / S, d = ad % S;
         int j = pr + 1;
         double2 q = gl[((long)j * S + a) * ldc + d];  // gles(j)
@@ -352,13 +352,13 @@ __device__ void les_start_block(const GroupDev &g, const ProbDev &p, int n, cons
             }
         }
     }
-    __syncthreads();
-    cta_solve(A, R, KS, S, ipiv, status);
-    for (int e = threadIdx.x; e < k * s2; e += blockDim.x) {
+    x.sync();
+    grp_solve(x, A, R, KS, S, ipiv, status);
+    for (int e = x.t(); e < k * s2; e += x.n()) {
         int q = e / s2, ad = e % s2, a = ad / S, d = ad % S;
         xcol[(long)(q + 1) * s2 + ad] = R[(q * S + a) * S + d];
     }
-    __syncthreads();
+    x.sync();
 }
 
 // ---------------------------------------------------------------------------------------
@@ -403,7 +403,8 @@ __global__ void __launch_bounds__(256) k_tv(GroupDev g, const ProbDev *__restric
             const int j64 = MIXED ? (n - g.k - 1 > 0 ? n - g.k - 1 : 0) : 0;  // first FP64 row
             if (MIXED) {
                 const float2 *gb32 = p.gtv32 + tau;
-#pragma unroll 4
+                // 8-byte loads: twice the rows in flight of the FP64 loop keep as many bytes in flight
+#pragma unroll 8
                 for (int j = warp; j < j64; j += NW) {
                     const float2 *gj = gb32 + (long)j * rowstride;
                     double2 bv[S][DCH];
@@ -589,4 +590,58 @@ __global__ void k_les_operands(GroupDev g, const ProbDev *__restrict__ probs, in
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// k_les_operands_t: the same operands as k_les_operands, written row by row.  badv / btv are
+// row-major with the problems side by side in a row, so one problem's column is a strided
+// write; here a CTA takes a tile of LOT problems x LOR time indices, reads each problem's
+// contiguous slice into shared memory and writes whole row segments (coalesced).
+//   which = 1: badv rows m = 0..n (from G^R(n, m)); which = 2: btv rows m = 0..ntau (from G^tv(n, .))
+// ---------------------------------------------------------------------------------------
+#define LOT 32
+template <int S> struct LoCfg {
+    static constexpr int LOR = S == 1 ? 32 : (S == 2 ? 16 : (S <= 4 ? 4 : 1));  // time indices per tile
+};
+
+template <int S>
+__global__ void __launch_bounds__(256) k_les_operands_t(GroupDev g, const ProbDev *__restrict__ probs, int n,
+                                                        int which, int nact) {
+    constexpr int s2 = S * S, LOR = LoCfg<S>::LOR;
+    __shared__ double2 buf[LOT * LOR * s2 + LOT];
+    __shared__ const double2 *src[LOT];
+    __shared__ int colid[LOT];
+    const int k = g.k, ntau = g.ntau, M = ntau + 1;
+    const double h = g.h, dtau = g.beta / ntau;
+    const long ldc = g.ldc;
+    const int q0 = blockIdx.y * LOT, nq = min(LOT, nact - q0);
+    const int m0 = blockIdx.x * LOR, rows = which == 1 ? n + 1 : M, nm = min(LOR, rows - m0);
+    if (threadIdx.x < LOT) {
+        const int q = threadIdx.x;
+        src[q] = q < nq ? (which == 1 ? probs[q0 + q].gret + tri(n) * s2 : probs[q0 + q].gtv + (long)n * s2 * M)
+                        : nullptr;
+        colid[q] = q < nq ? probs[q0 + q].col : 0;
+    }
+    __syncthreads();
+    // gather: buf[(q*LOR + mm)*s2 + e] = G element e of problem q at time index m0+mm
+    for (int i = threadIdx.x; i < nq * nm * s2; i += blockDim.x) {
+        if (which == 1) {
+            const int q = i / (nm * s2), rem = i % (nm * s2), mm = rem / s2, e = rem % s2;
+            buf[(q * LOR + mm) * s2 + e] = src[q][(long)(m0 + mm) * s2 + e];     // ret row n, contiguous
+        } else {
+            const int q = i / (nm * s2), rem = i % (nm * s2), e = rem / nm, mm = rem % nm;
+            buf[(q * LOR + mm) * s2 + e] = src[q][(long)e * M + (ntau - (m0 + mm))];  // tv planes
+        }
+    }
+    __syncthreads();
+    // scatter: row (m, c), columns (col, d) of this tile
+    for (int i = threadIdx.x; i < nm * S * nq * S; i += blockDim.x) {
+        const int r = i / (nq * S), cc = i % (nq * S), mm = r / S, c = r % S, q = cc / S, d = cc % S;
+        const int m = m0 + mm;
+        const double2 v = cconj(buf[(q * LOR + mm) * s2 + d * S + c]);
+        const long dst = ((long)m * S + c) * ldc + (long)colid[q] * S + d;
+        if (which == 1) g.badv[dst] = cscale(v, h * greg_w(k, n, m));
+        else g.btv[dst] = cmul(cmk(0.0, dtau * (double)g.sig * greg_w(k, ntau, m)), v);
+    }
+}
+
 #include "kernels_volterra.cuh"
+#include "kernels_volterra_mp.cuh"

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -99,6 +100,7 @@ struct Group {
     MatScratch *d_mat = nullptr;  // per-member scratch of dyson_mat (allocated on first use)
     LocDev loc{nullptr, nullptr, nullptr, nullptr};  // G_loc of the group (allocated on first use)
     bool vie = false;                // VIE2 group: s* hold F, fcc* hold Fcc (nessi_gpu_set_F)
+    int pp_ret = 0, pp_les = 0;      // Volterra kernel chosen by the autotuner (0: not yet)
     double2 *fccret = nullptr, *fccles = nullptr;
     double2 *U = nullptr;            // diagonal interaction U(t), (ntmax+2) x s, t = -1 first
     std::vector<int> members;        // problem indices, nt descending
@@ -126,10 +128,17 @@ struct nessi_batch {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool own_stream = true;
     cublasHandle_t cublas = nullptr, cublas_side = nullptr;
+    void *cublas_ws = nullptr, *cublas_ws_side = nullptr;  // fixed cuBLAS workspaces (capture-safe)
+    cudaGraphExec_t graph = nullptr;                     // recorded time steps (nessi_gpu_graph_record)
     std::vector<Prob> probs;
     std::vector<Group> groups;
     std::vector<void *> allocs;
     long long bytes = 0;
+    // Volterra kernels for size1 <= 2: 0 (default) = chosen per group by the autotuner in
+    // volterra_step; -1 = the one-problem-per-CTA kernels k_ret / k_les, which overlap the next
+    // block's sums with the current block's solve; 1, 2, 4, 8 = problems per CTA of the tensor-core
+    // kernels k_ret_mp / k_les_mp, which read each shared Sigma tile once for all of them.
+    int volterra_pp = 0;
     double2 *scratch = nullptr;  // G^tv in libcntr layout during layout conversion (size1 > 1)
     long scratch_n = 0;
 
@@ -213,6 +222,75 @@ template <int S> size_t les_smem(int k) {
     return std::max(start, phase);
 }
 
+// One Volterra recursion (ret or les) of a step: the one-problem kernels (pp = -1) or the
+// multi-problem tensor-core kernels with pp problems per CTA (size1 <= 2).
+template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret, int pp,
+                                               cudaStream_t st) {
+    if constexpr (S <= 2) {
+        if (pp > 0) {
+            const size_t sm = (size_t)MpCfg<S>::total * sizeof(double2);
+            const unsigned grid = (unsigned)((nact + pp - 1) / pp);
+            if (ret) {
+                CK(cudaFuncSetAttribute(k_ret_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_ret_mp<S, VIE><<<grid, 256, sm, st>>>(gd, g.d_probs, n, nact, pp);
+            } else {
+                CK(cudaFuncSetAttribute(k_les_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_les_mp<S, VIE><<<grid, 256, sm, st>>>(gd, g.d_probs, n, nact, pp);
+            }
+            CK(cudaGetLastError());
+            return NESSI_OK;
+        }
+    }
+    const size_t sm = ret ? ret_smem<S>(gd.k) : les_smem<S>(gd.k);
+    if (ret) {
+        CK(cudaFuncSetAttribute(k_ret<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_ret<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+    } else {
+        CK(cudaFuncSetAttribute(k_les<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_les<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+    }
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+// Autotuner of the Volterra kernels.  With volterra_pp = 0 (default), the first eager step of a
+// group with n >= min(128, ntmax) launches every candidate (one-problem kernels, and for
+// size1 <= 2 the multi-problem kernels with 2, 4, 8 problems per CTA) on the step itself --
+// each launch recomputes the same row / column from the same inputs, so the last one leaves
+// the step's result -- times them with CUDA events and keeps the fastest for the group.  Until
+// then, and while a graph is being recorded, the one-problem kernels run.
+template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const GroupDev &gd, int n, int nact, bool ret,
+                                             cudaStream_t st) {
+    int &choice = ret ? g.pp_ret : g.pp_les;
+    if (b->volterra_pp != 0) return volterra_launch<S, VIE>(gd, g, n, nact, ret, b->volterra_pp, st);
+    if (choice != 0) return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cap));
+    if (S > 2) choice = -1;
+    if (S > 2 || cap != cudaStreamCaptureStatusNone || n < std::min(128, g.ntmax))
+        return volterra_launch<S, VIE>(gd, g, n, nact, ret, -1, st);
+    const int cand[4] = {-1, 2, 4, 8};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bestc = -1;
+    for (int pass = 0; pass < 2; pass++)  // the first pass warms up every variant
+        for (int c : cand) {
+            CK(cudaEventRecord(e0, st));
+            CKR((volterra_launch<S, VIE>(gd, g, n, nact, ret, c, st)));
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (pass == 1 && ms < best) { best = ms; bestc = c; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    choice = bestc;
+    return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);  // the kept variant writes last
+}
+
 template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     const GroupDev gd = group_dev(g);
     cudaStream_t st = b->stream;
@@ -263,17 +341,13 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
     CK(cudaEventRecord(b->ev_fork, st));
     CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     {
-        size_t sm = ret_smem<S>(k);
-        CK(cudaFuncSetAttribute(k_ret<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         b->prof_mark(NESSI_KERNEL_RET, b->side);
-        k_ret<S, VIE><<<nact, 256, sm, b->side>>>(gd, g.d_probs, n);
-        CK(cudaGetLastError());
+        CKR((volterra_step<S, VIE>(b, g, gd, n, nact, true, b->side)));
         // G^R row n written; Sigma^R triangle rows <= n read (shared by the group)
         b->prof_end(NESSI_KERNEL_RET, 16.0 * S * S * ((double)nact * (n + 1) + tri_h(n + 1)), b->side);
-        long rows = (long)(n + 1) * S * S;
-        dim3 grid((unsigned)std::min<long>((rows + 255) / 256, 64), nact);
         b->prof_mark(NESSI_KERNEL_LES_OPERANDS, b->side);
-        k_les_operands<S><<<grid, 256, 0, b->side>>>(gd, g.d_probs, n, 1);
+        dim3 grid((unsigned)((n + 1 + LoCfg<S>::LOR - 1) / LoCfg<S>::LOR), (unsigned)((nact + LOT - 1) / LOT));
+        k_les_operands_t<S><<<grid, 256, 0, b->side>>>(gd, g.d_probs, n, 1, nact);
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_LES_OPERANDS, 32.0 * S * S * (double)nact * (n + 1), b->side);
         b->prof_mark(NESSI_KERNEL_GEMM, b->side);
@@ -297,10 +371,9 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
         const double n32 = mixed ? std::max(0, n - k - 1) : 0, n64 = n - n32;
         b->prof_end(NESSI_KERNEL_TV, S * S * ((double)nact * (8.0 * n32 * M + 16.0 * n64 * M + 32.0 * M +
                                                                  (mixed ? 8.0 * M : 0.0)) + 16.0 * n));
-        long rows = (long)(g.ntau + 1) * S * S;
-        dim3 grid2((unsigned)std::min<long>((rows + 255) / 256, 64), nact);
         b->prof_mark(NESSI_KERNEL_LES_OPERANDS);
-        k_les_operands<S><<<grid2, 256, 0, st>>>(gd, g.d_probs, n, 2);
+        dim3 grid2((unsigned)((g.ntau + 1 + LoCfg<S>::LOR - 1) / LoCfg<S>::LOR), (unsigned)((nact + LOT - 1) / LOT));
+        k_les_operands_t<S><<<grid2, 256, 0, st>>>(gd, g.d_probs, n, 2, nact);
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_LES_OPERANDS, 32.0 * S * S * (double)nact * (g.ntau + 1));
     }
@@ -316,11 +389,8 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
     }
     // lesser column
     {
-        size_t sm = les_smem<S>(k);
-        CK(cudaFuncSetAttribute(k_les<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         b->prof_mark(NESSI_KERNEL_LES);
-        k_les<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
-        CK(cudaGetLastError());
+        CKR((volterra_step<S, VIE>(b, g, gd, n, nact, false, st)));
         b->prof_end(NESSI_KERNEL_LES, 16.0 * S * S * ((double)nact * 2.0 * (n + 1) + tri_h(n + 1)));
     }
     return NESSI_OK;
@@ -485,6 +555,10 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
     nessi_batch *b = new nessi_batch();
     b->device = g_device;
     b->precision = precision;
+    if (const char *v = getenv("NESSI_VOLTERRA_PP")) {
+        const int pp = atoi(v);
+        if (pp == -1 || pp == 0 || pp == 1 || pp == 2 || pp == 4 || pp == 8) b->volterra_pp = pp;
+    }
     auto fail = [&](int r) { nessi_gpu_batch_destroy(b); return r; };
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
         set_err("stream creation failed");
@@ -502,6 +576,18 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
     if (cublasCreate(&b->cublas_side) != CUBLAS_STATUS_SUCCESS) { set_err("cublasCreate failed"); return fail(NESSI_ERR_CUDA); }
     cublasSetStream(b->cublas_side, b->side);
     cublasSetMathMode(b->cublas_side, CUBLAS_DEFAULT_MATH);
+    {
+        // fixed workspaces, so that cuBLAS allocates nothing while a graph is being recorded
+        const size_t wsz = 32u << 20;
+        if (cudaMalloc(&b->cublas_ws, wsz) != cudaSuccess || cudaMalloc(&b->cublas_ws_side, wsz) != cudaSuccess) {
+            set_err("cudaMalloc of the cuBLAS workspaces failed");
+            return fail(NESSI_ERR_OOM);
+        }
+        b->allocs.push_back(b->cublas_ws);
+        b->allocs.push_back(b->cublas_ws_side);
+        cublasSetWorkspace(b->cublas, b->cublas_ws, wsz);
+        cublasSetWorkspace(b->cublas_side, b->cublas_ws_side, wsz);
+    }
     b->probs.resize(count);
     // groups
     for (int i = 0; i < count; i++) {
@@ -593,6 +679,7 @@ int nessi_gpu_batch_destroy(nessi_batch *b) {
     if (!b) return NESSI_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
     for (void *q : b->allocs) cudaFree(q);
     for (auto &k : b->kp)
         for (cudaEvent_t e : k.ev) cudaEventDestroy(e);
@@ -1139,6 +1226,43 @@ int nessi_gpu_lattice_2b_timestep(nessi_batch *b, int n, int corrector_steps) {
     for (Group &g : b->groups)
         if (g.U && active_members(b, g, n) > 0) CKR(gloc_dispatch(b, g, n));
     b->prof_end(NESSI_KERNEL_LATTICE, 0.0);
+    return NESSI_OK;
+}
+
+int nessi_gpu_graph_record(nessi_batch *b, int kind, int n0, int n1, int corrector_steps) {
+    CKR(check_batch(b));
+    if (kind < 0 || kind > 2 || n1 < n0) { set_err("graph_record: bad arguments"); return NESSI_ERR_ARG; }
+    CK(cudaStreamSynchronize(b->stream));
+    CK(cudaStreamSynchronize(b->side));
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    const bool prof = b->prof;
+    b->prof = false;  // no timing events inside the graph
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = NESSI_OK;
+    for (int n = n0; n <= n1 && rc == NESSI_OK; n++) {
+        if (kind == 0) rc = nessi_gpu_dyson_timestep(b, n);
+        else if (kind == 1) rc = nessi_gpu_vie2_timestep(b, n);
+        else rc = nessi_gpu_lattice_2b_timestep(b, n, corrector_steps);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    b->prof = prof;
+    if (rc != NESSI_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) {
+        set_err("graph_record: capture failed: %s", cudaGetErrorString(e));
+        if (g) cudaGraphDestroy(g);
+        return NESSI_ERR_CUDA;
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) { b->graph = nullptr; set_err("graph_record: instantiate failed: %s", cudaGetErrorString(e2)); return NESSI_ERR_CUDA; }
+    return NESSI_OK;
+}
+
+int nessi_gpu_graph_launch(nessi_batch *b) {
+    CKR(check_batch(b));
+    if (!b->graph) { set_err("graph_launch: nothing recorded"); return NESSI_ERR_ARG; }
+    CK(cudaGraphLaunch(b->graph, b->stream));
     return NESSI_OK;
 }
 

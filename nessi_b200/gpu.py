@@ -85,6 +85,8 @@ EXPORTS = {
                                        [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     "nessi_gpu_convolution_timestep_host": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 5 +
                                             [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_graph_record": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 4),
+    "nessi_gpu_graph_launch": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
@@ -223,6 +225,16 @@ class Batch:
     def vie2_timestep(self, n):
         """cntr::vie2_timestep(n, ...) for every VIE2 problem."""
         _check(load_library().nessi_gpu_vie2_timestep(self._h, n))
+
+    # ---- CUDA graphs ------------------------------------------------------------------
+    GRAPH_DYSON, GRAPH_VIE2, GRAPH_LATTICE = 0, 1, 2
+
+    def graph_record(self, kind, n0, n1, corrector_steps=3):
+        """Record the launches of steps n0..n1 into a CUDA graph (nothing runs)."""
+        _check(load_library().nessi_gpu_graph_record(self._h, kind, n0, n1, corrector_steps))
+
+    def graph_launch(self):
+        _check(load_library().nessi_gpu_graph_launch(self._h))
 
     # ---- self-consistent lattice ----------------------------------------------------
     def set_U(self, group, U):

@@ -12,6 +12,11 @@ chain2 (2-band chain, size1 = 2, Nk k-points in [-pi, pi)):
     201 levels), shared by all k.
 chain4 (4-band chain, size1 = 4): diagonal -2cos(k - A) + eps_a, eps = (-1.5, -0.5, 0.5, 1.5),
     nearest-band hoppings 0.3, same Sigma (x) 1_4.
+uneven (independent problems of mixed orbital size and length): size1 drawn from {1,2,3,5,8} and
+    nt from U[500, 3000] with a seed; h = (X + X^H)/2, X complex N(0, 0.5^2); a rank-1 quench
+    u u^H (u complex N(0, 0.3^2)) switched on at t = 0; Sigma = 0.49 G_bath (x) 1_s shared by the
+    problems of one size (sigma_group = size1).  Every problem is a Dyson problem: VIE2 problems
+    would each carry a source term Q as large as G, which does not fit next to ~150 GB of G.
 lattice2b (square lattice, size1 = 1, nkx x nky k-points in [-pi, pi)^2):
     eps_k = -2(cos kx + cos ky), mu = 0 (half filling), free equilibrium (U = 0 on the Matsubara
     branch), U(t) = min(t, 2) switched on at t = 0; Sigma = Sigma_2B[G_loc, U] recomputed from the
@@ -31,7 +36,7 @@ class Workload:
     def __init__(self, name, descs, sigma, H, boot, k, info):
         self.name = name
         self.descs = descs          # list of batch descriptors
-        self.sigma = sigma          # herm_matrix shared by all problems (sigma_group 0)
+        self.sigma = sigma          # herm_matrix of sigma_group 0, or {sigma_group: herm_matrix}
         self.H = H                  # (nprob, nt+2, s, s)
         self.boot = boot            # list of herm_matrix(nt=k) with mat and steps 0..k per problem
         self.k = k
@@ -145,9 +150,53 @@ def config4(nkx=32, nky=32, nt=2000, ntau=800, kshift=0.0):
     return lattice2b(nkx, nky, nt, ntau, 20.0, 0.01, kshift=kshift)
 
 
+def uneven(nprob=96, sizes=(1, 2, 3, 5, 8), nt_range=(500, 3000), ntau=400, beta=10.0, h=0.01, k=5, V=0.7,
+           seed=20261203):
+    """Config 3: independent problems of uneven size and length in one batch (groups by size)."""
+    rng = np.random.default_rng(seed)
+    s_list = [int(rng.choice(sizes)) for _ in range(nprob)]
+    nt_list = [int(rng.integers(nt_range[0], nt_range[1] + 1)) for _ in range(nprob)]
+    H, boot, descs = [], [], []
+    for s, nt in zip(s_list, nt_list):
+        x = rng.normal(0, 0.5, (s, s)) + 1j * rng.normal(0, 0.5, (s, s))
+        h0 = (x + x.conj().T) / 2
+        u = rng.normal(0, 0.3, s) + 1j * rng.normal(0, 0.3, s)
+        Hp = np.zeros((nt + 2, s, s), np.complex128)
+        Hp[0] = h0
+        Hp[1:] = h0 + np.outer(u, u.conj())
+        H.append(Hp)
+        boot.append(bootstrap_free(h0, 0.0, beta, h, k, ntau))
+        descs.append(dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, sigma_group=s, beta=beta, h=h, mu=0.0))
+    Gb = eq.semicircle_bath(max(nt_list), ntau, beta, h)
+    sigma = {}
+    for s in sorted(set(s_list)):
+        ntg = max(nt for ss, nt in zip(s_list, nt_list) if ss == s)
+        Gs = herm_matrix(ntg, ntau, 1, -1)
+        Gs.ret[...] = Gb.ret[:Gs.ret.shape[0]]
+        Gs.les[...] = Gb.les[:Gs.les.shape[0]]
+        Gs.tv[...] = Gb.tv[:ntg + 1]
+        Gs.mat[...] = Gb.mat
+        sigma[s] = eq.kron_identity(Gs, s, V * V)
+    info = dict(model="uneven batch of independent Dyson problems", nprob=nprob, sizes=list(sizes),
+                nt_range=list(nt_range), ntau=ntau, beta=beta, h=h, solve_order=k, seed=seed,
+                size1_counts={str(s): s_list.count(s) for s in sorted(set(s_list))},
+                sigma="V^2 G_bath (x) 1_s, V=%g, shared per size1" % V)
+    W = Workload("uneven", descs, sigma, H, boot, k, info)
+    return W
+
+
+def config3(**kw):
+    """96 problems, size1 in {1,2,3,5,8}, nt in [500, 3000], ntau = 400, beta = 10, h = 0.01."""
+    return uneven(**kw)
+
+
 def upload(batch, W):
     """Copy Sigma, H and the bootstrap steps of a workload into a gpu.Batch."""
-    batch.set_sigma(0, W.sigma)
+    if isinstance(W.sigma, dict):
+        for grp, S in W.sigma.items():
+            batch.set_sigma(grp, S)
+    else:
+        batch.set_sigma(0, W.sigma)
     for p in range(W.nprob):
         batch.set_H(p, W.H[p])
         B = W.boot[p]

@@ -91,3 +91,24 @@ def test_single_problem_cntr_signature(oracle):
     e = component_errors(Gg, Gf, k + 1, k + 1)
     for comp, v in e.items():
         assert v < TOL, (comp, v)
+
+
+@pytest.fixture
+def volterra_pp(monkeypatch):
+    """Force the problems-per-CTA setting of the size1 <= 2 Volterra kernels for new batches."""
+    def set_pp(pp):
+        monkeypatch.setenv("NESSI_VOLTERRA_PP", str(pp))
+    return set_pp
+
+
+@pytest.mark.parametrize("s", [1, 2])
+@pytest.mark.parametrize("pp", [-1, 1, 2, 4, 8])
+def test_volterra_problems_per_cta(oracle, volterra_pp, s, pp):
+    """Every grouping of problems per CTA (and the one-problem kernels, -1) gives the oracle's
+    numbers on an uneven batch whose histories span several 32-row blocks; the batch size is not
+    a multiple of the grouping, so partly filled CTAs are exercised too."""
+    volterra_pp(pp)
+    errs = _run(oracle, s, [90, 75, 90, 40, 90, 66, 90, 90, 12], 10, seed=40 + s)
+    for e in errs:
+        for comp, v in e.items():
+            assert v < TOL, (comp, v)
