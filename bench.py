@@ -174,7 +174,57 @@ def build_workload(name, rank, world):
         return workloads.config4(kshift=shift)
     if name == "config4-small":  # 16x16 lattice, nt=400, ntau=200: quick checks of the lattice path
         return workloads.config4(nkx=16, nky=16, nt=400, ntau=200, kshift=shift)
+    if name == "config4-ncu":  # 32x32 lattice (the config-4 grid), nt=400, ntau=200: ~4 GB, for ncu
+        return workloads.config4(nkx=32, nky=32, nt=400, ntau=200, kshift=shift)
     raise SystemExit("unknown workload %s" % name)
+
+
+def _result_sample(b, W, nt):
+    """What the comparison looks at: G_loc of a lattice, else every component of up to 8
+    problems (all time steps)."""
+    from nessi_b200 import herm_matrix
+    out = []
+    if W.lattice:
+        d = W.descs[0]
+        L = herm_matrix(d["nt"], d["ntau"], d["size1"], d["sig"])
+        b.get_gloc(0, L)
+        out.append(L)
+    else:
+        for p in range(min(8, len(W.descs))):
+            d = W.descs[p]
+            G = herm_matrix(d["nt"], d["ntau"], d["size1"], d["sig"])
+            b.get_G(p, G)
+            out.append(G)
+    return out
+
+
+def compare_with_fp64(b, W, run_step, nt, k):
+    """Max relative error max|x - x64| / max|x64| per component of the mixed result against the
+    FP64 GPU path (itself parity-tested against the oracle at 1e-10) on the same inputs."""
+    from nessi_b200 import gpu, workloads
+    run_step()
+    b.synchronize()
+    mixed = _result_sample(b, W, nt)
+    b.close()
+    b64 = gpu.Batch(W.descs, precision=gpu.PREC_FP64)
+    workloads.upload(b64, W)
+    if W.lattice:
+        b64.lattice_2b_start(max_iter=30, tol=1e-12)
+        for n in range(k + 1, nt + 1):
+            b64.lattice_2b_timestep(n, W.ncorr)
+    else:
+        for n in range(k + 1, nt + 1):
+            b64.dyson_timestep(n)
+    b64.synchronize()
+    ref = _result_sample(b64, W, nt)
+    b64.close()
+    err = {}
+    for comp in ("ret", "les", "tv"):
+        num = max(float(np.max(np.abs(getattr(x, comp) - getattr(y, comp)))) for x, y in zip(mixed, ref))
+        den = max(float(np.max(np.abs(getattr(y, comp)))) for y in ref)
+        err[comp] = num / den if den else 0.0
+    err["compared"] = "G_loc, all time steps" if W.lattice else "all components of %d problems" % len(ref)
+    return err
 
 
 def dist_setup(args):
@@ -239,6 +289,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mixed-error", action="store_true",
+                    help="with --precision mixed: afterwards run the FP64 path on the same inputs and report the "
+                         "max relative error of the mixed result per component")
     ap.add_argument("--no-graph", action="store_true", help="launch every step eagerly instead of replaying "
                     "a CUDA graph of the propagation")
     args = ap.parse_args()
@@ -412,6 +465,12 @@ def main():
         v, thr, desc = cpu_sample(W, target_s=args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
 
+    groups = sorted(W.sigma.keys()) if isinstance(W.sigma, dict) else [0]
+    volterra = {str(gid): b.volterra_choice(gid) for gid in groups}
+    mixed_err = None
+    if args.mixed_error and args.precision == "mixed":
+        mixed_err = compare_with_fp64(b, W, run_step, nt, k)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -427,9 +486,13 @@ def main():
                                **W.info),
                 "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk,
-                "launch": "CUDA graph of the whole propagation, replayed each step" if use_graph else "eager"}
+                "launch": "CUDA graph of the whole propagation, replayed each step" if use_graph else "eager",
+                "volterra_kernels": {g: {"ret": v[0], "les": v[1]} for g, v in volterra.items()}}
+        if mixed_err is not None:
+            line["mixed_error_vs_fp64_gpu"] = mixed_err
         print(json.dumps(line), flush=True)
-    b.close()
+    if not (args.mixed_error and args.precision == "mixed"):
+        b.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

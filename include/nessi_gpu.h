@@ -211,6 +211,12 @@ int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nes
                                         int nt, int ntau, int size1, int sig_a, int sig_b, int solve_order,
                                         double beta, double h);
 
+/* Volterra kernels in use for a group: -1 = one problem per CTA, 2/4/8 = problems per CTA of the
+ * tensor-core kernels, 0 = not chosen yet (the autotuner decides at the first eager step with
+ * n >= min(128, nt); the environment variable NESSI_VOLTERRA_PP read at batch creation fixes
+ * the choice).  No reference counterpart. */
+int nessi_gpu_get_volterra_choice(nessi_batch *b, int group, int *pp_ret, int *pp_les);
+
 /* ---- CUDA graphs of the per-step launch sequence ---------------------------------------------
  * Record the launches of time steps n0..n1 (kind 0: dyson_timestep, 1: vie2_timestep,
  * 2: lattice_2b_timestep with corrector_steps) into a CUDA graph held by the batch, without

@@ -1229,6 +1229,15 @@ int nessi_gpu_lattice_2b_timestep(nessi_batch *b, int n, int corrector_steps) {
     return NESSI_OK;
 }
 
+int nessi_gpu_get_volterra_choice(nessi_batch *b, int group, int *pp_ret, int *pp_les) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    const int fixed = b->volterra_pp;
+    if (pp_ret) *pp_ret = fixed != 0 ? fixed : g->pp_ret;
+    if (pp_les) *pp_les = fixed != 0 ? fixed : g->pp_les;
+    return NESSI_OK;
+}
+
 int nessi_gpu_graph_record(nessi_batch *b, int kind, int n0, int n1, int corrector_steps) {
     CKR(check_batch(b));
     if (kind < 0 || kind > 2 || n1 < n0) { set_err("graph_record: bad arguments"); return NESSI_ERR_ARG; }

@@ -85,6 +85,8 @@ EXPORTS = {
                                        [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     "nessi_gpu_convolution_timestep_host": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 5 +
                                             [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_get_volterra_choice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                     ctypes.POINTER(ctypes.c_int)]),
     "nessi_gpu_graph_record": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 4),
     "nessi_gpu_graph_launch": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -232,6 +234,12 @@ class Batch:
     def graph_record(self, kind, n0, n1, corrector_steps=3):
         """Record the launches of steps n0..n1 into a CUDA graph (nothing runs)."""
         _check(load_library().nessi_gpu_graph_record(self._h, kind, n0, n1, corrector_steps))
+
+    def volterra_choice(self, group=0):
+        """(ret, les) Volterra kernels of a group: -1 one problem per CTA, 2/4/8 problems per CTA."""
+        r, l = ctypes.c_int(), ctypes.c_int()
+        _check(load_library().nessi_gpu_get_volterra_choice(self._h, group, ctypes.byref(r), ctypes.byref(l)))
+        return r.value, l.value
 
     def graph_launch(self):
         _check(load_library().nessi_gpu_graph_launch(self._h))
