@@ -5,15 +5,15 @@
 // blocks of 32 rows.  For a block, the sum over every row solved before it ("phase A") is
 //   ret:  acc(j) = sum_{m > jhi} w(n-j, n-m) G(n,m) Sigma^R(m,j)
 //   les:  acc(j) = sum_{m < jlo} w(j,m) Sigma^R(j,m) G^<(m,n)
-// Sigma (F / Fcc for VIE2) is shared by all problems of a group, so a CTA takes PP <= 8 problems
-// and computes phase A for all of them at once as a complex GEMM on the FP64 tensor cores
-// (mma.sync m8n8k4 .f64), its operands staged through shared memory with cp.async: each Sigma
-// tile is read once per CTA instead of once per problem.  Away from the diagonal (|m - j| > k) the
-// Gregory weight depends on m alone (c_m: omega at the n / 0 end, else 1), so it is a column
-// scale of the GEMM; the <= k terms next to the block are corrected to the exact weight
-// afterwards.  Warp q then solves the block's rows of problem q with each lane owning one row in
-// registers (as in the one-problem kernels), and the next block starts.  PP is chosen by the
-// autotuner on the host.
+// Sigma (F / Fcc for VIE2) is shared by all problems of a group, so a CTA takes PP problems and
+// streams each Sigma tile through shared memory ONCE for all of them (cp.async double buffer),
+// instead of every problem reading the whole triangle from L2.  Away from the diagonal
+// (|m - j| > k) the Gregory weight depends on m alone (c_m: omega at the n / 0 end, else 1), so
+// the tiles are weighted per column; the <= k terms next to the block are corrected to the exact
+// weight afterwards.  Each problem owns 8/PP warps that split the tile columns; their partial sums
+// are added in warp order.  The rows of the block are then solved by the problem's first warp
+// with each lane owning one row in registers (as in the one-problem kernels), and the next block
+// starts.  PP is chosen on the host from the number of active problems.
 #pragma once
 
 #define MP_JB 32  // rows per block (lane = row)
@@ -22,27 +22,13 @@ template <int S> struct MpCfg {
     static constexpr int s2 = S * S;
     static constexpr int TRI = MP_JB * (MP_JB - 1) / 2;    // packed strictly-lower block triangle
     static constexpr int WSW = 2 * NESSI_K1MAX * NESSI_K1MAX * s2 + 2 * NESSI_K1MAX * s2 + 2;  // start work/warp
-    static constexpr int KC = 32;                           // k per staged chunk (8 MMA k-steps)
-    static constexpr int LDA = KC + 4;                      // padded row of a staged A chunk
-    static constexpr int RMAX = MP_JB * S, NMAX = MP_JB * S;
-    static constexpr int LDB = NMAX + 2;                    // padded row of a staged B chunk
-    static constexpr int ASZ = RMAX * LDA, BSZ = KC * LDB;
-    static constexpr int stage = 0;                         // 2 x (A chunk, B chunk)
-    static constexpr int acc = stage + 2 * (ASZ + BSZ);     // 8 problems x 32 rows x s2: phase-A sums
-    static constexpr int red = acc + 8 * MP_JB * s2;        // 8 warps x 32 lanes x 2 tiles x 2 double2
-    static constexpr int sig = red + 8 * 32 * 4;            // TRI x s2
+    static constexpr int acc = 0;                           // 8 problems x 32 rows x s2: phase-A sums
+    static constexpr int red = acc + 8 * MP_JB * s2;        // 8 warps x 32 lanes x 2 double2: partial tiles
+    static constexpr int sig = red + 8 * 32 * 2;            // TRI x s2
     static constexpr int wb = sig + TRI * s2;               // TRI doubles
     static constexpr int total = wb + TRI / 2 + 1;
-    static_assert(acc >= 8 * WSW, "start workspaces must fit in the staging buffers");
+    static_assert(sig + TRI * s2 >= 8 * WSW, "start workspaces must fit below the weights");
 };
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // D += A B on the FP64 tensor cores, one 8x8x4 tile: lane holds A[lane/4][lane%4],
 // B[lane%4][lane/4] and D[lane/4][2(lane%4) + {0,1}] (mma.m8n8k4 .f64 fragment layout).
@@ -52,83 +38,57 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double
                  : "d"(a), "d"(b));
 }
 
-// Phase A as a complex GEMM C (R x N) = A (R x K) B (K x N), R, N <= 32 S, with the operands
-// staged in shared memory: chunks of KC k-values of A and B are copied with cp.async (double
-// buffered, every thread issuing copies, so many loads are in flight), and the warps take their
-// MMA fragments from the padded chunks (A rows padded to LDA = KC + 4, B rows to LDB = N + 2,
-// which keeps the fragment reads free of bank conflicts).  srcA(r, kk) / srcB(kk, c) give the
-// address of an operand element or nullptr for a zero; wA(kk) / wB(kk) scale column kk of A /
-// row kk of B.  The 8 warps share the 8x8 tiles, or the k-steps of a chunk when there are fewer
-// than 8 tiles (then summed in warp order).  put(r, c, value) stores an element of C.
-template <int S, class SA, class SB, class WA, class WB, class PUT>
-__device__ void zgemm_staged(const SA &srcA, const SB &srcB, const WA &wA, const WB &wB, const PUT &put, int R,
-                             int N, int K, double2 *stage, double2 *red, int tid) {
-    using C = MpCfg<S>;
-    const int warp = tid >> 5, lane = tid & 31;
-    const int MT = (R + 7) / 8, NT = (N + 7) / 8, tiles = MT * NT;
-    const int ksplit = tiles >= 8 ? 1 : 8 / tiles;
-    const int nmy = tiles >= 8 ? (tiles - warp + 7) / 8 : (warp / tiles < ksplit ? 1 : 0);  // tiles of this warp
-    double c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-    const int nch = (K + C::KC - 1) / C::KC;
-    auto load = [&](int ch, int buf) {
-        double2 *As = stage + buf * (C::ASZ + C::BSZ), *Bs = As + C::ASZ;
-        const int k0 = ch * C::KC;
-        for (int e = tid; e < R * C::KC; e += 256) {
-            const int r = e / C::KC, kk = e % C::KC;
-            const double2 *src = k0 + kk < K ? srcA(r, k0 + kk) : nullptr;
-            if (src) cp_async16(As + r * C::LDA + kk, src);
-            else As[r * C::LDA + kk] = cmk(0, 0);
-        }
-        for (int e = tid; e < C::KC * N; e += 256) {
-            const int kk = e / N, cc = e % N;
-            const double2 *src = k0 + kk < K ? srcB(k0 + kk, cc) : nullptr;
-            if (src) cp_async16(Bs + kk * C::LDB + cc, src);
-            else Bs[kk * C::LDB + cc] = cmk(0, 0);
-        }
-        cp_async_commit();
-    };
-    if (nch > 0) load(0, 0);
-    for (int ch = 0; ch < nch; ch++) {
-        if (ch + 1 < nch) { load(ch + 1, (ch + 1) & 1); cp_async_wait_all_but_one(); }
-        else cp_async_wait_all();
-        __syncthreads();
-        const double2 *As = stage + (ch & 1) * (C::ASZ + C::BSZ), *Bs = As + C::ASZ;
-        const int k0 = ch * C::KC;
+// Complex 8x8 tile (mt, nt) of C = A B over the k-steps ks0, ks0 + kstride, ... of K (4 per step):
+// c[0..1] real and c[2..3] imaginary parts of D[lane/4][2(lane%4) + {0,1}].  fa(r, kk) and fb(kk, cc)
+// return the operands (zero outside the matrices, in particular for kk >= K).  The fragments of
+// MMA_U k-steps are loaded first and multiplied afterwards, so that 2 MMA_U loads are in flight.
+#define MMA_U 8
+template <class FA, class FB>
+__device__ __forceinline__ void ztile884(const FA &fa, const FB &fb, int mt, int nt, int K, int ks0, int kstride,
+                                         int lane, double *c) {
+    const int ar = mt * 8 + (lane >> 2), bc = nt * 8 + (lane >> 2), kq = lane & 3;
+    for (int ks = ks0; ks * 4 < K; ks += MMA_U * kstride) {
+        double2 a[MMA_U], b[MMA_U];
 #pragma unroll
-        for (int i = 0; i < 2; i++) {
-            if (i >= nmy) break;
-            const int t = tiles >= 8 ? warp + 8 * i : warp % tiles;
-            const int ksl = tiles >= 8 ? 0 : warp / tiles;
-            const int ar = (t / NT) * 8 + (lane >> 2), bc = (t % NT) * 8 + (lane >> 2), kq = lane & 3;
-#pragma unroll
-            for (int ks = 0; ks < C::KC / 4; ks++) {
-                if (ks % ksplit != ksl) continue;
-                const int kk = ks * 4 + kq;
-                const double2 a = cscale(As[ar * C::LDA + kk], wA(k0 + kk));
-                const double2 b = cscale(Bs[kk * C::LDB + bc], wB(k0 + kk));
-                dmma884(c[i][0], c[i][1], a.x, b.x);
-                dmma884(c[i][0], c[i][1], -a.y, b.y);
-                dmma884(c[i][2], c[i][3], a.x, b.y);
-                dmma884(c[i][2], c[i][3], a.y, b.x);
-            }
+        for (int u = 0; u < MMA_U; u++) {
+            const int kk = (ks + u * kstride) * 4 + kq;
+            a[u] = fa(ar, kk);
+            b[u] = fb(kk, bc);
         }
-        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < MMA_U; u++) {
+            dmma884(c[0], c[1], a[u].x, b[u].x);
+            dmma884(c[0], c[1], -a[u].y, b[u].y);
+            dmma884(c[2], c[3], a[u].x, b[u].y);
+            dmma884(c[2], c[3], a[u].y, b[u].x);
+        }
     }
+}
+
+// Phase A of one block as a complex GEMM C (R x N) = A (R x K) B (K x N) on the tensor cores, the
+// 8 warps sharing the tiles (and the k-steps when there are fewer than 8 tiles, summed in warp
+// order).  put(r, c, value) stores an element of C.
+template <class FA, class FB, class PUT>
+__device__ void zgemm_cta(const FA &fa, const FB &fb, const PUT &put, int R, int N, int K, double2 *red, int warp,
+                          int lane) {
+    const int MT = (R + 7) / 8, NT = (N + 7) / 8, tiles = MT * NT;
     const int r0 = lane >> 2, c0 = 2 * (lane & 3);
     if (tiles >= 8) {
-#pragma unroll
-        for (int i = 0; i < 2; i++) {
-            if (i >= nmy) break;
-            const int t = warp + 8 * i;
+        for (int t = warp; t < tiles; t += 8) {
+            double c[4] = {0, 0, 0, 0};
+            ztile884(fa, fb, t / NT, t % NT, K, 0, 1, lane, c);
             const int r = (t / NT) * 8 + r0, cc = (t % NT) * 8 + c0;
-            put(r, cc, cmk(c[i][0], c[i][2]));
-            put(r, cc + 1, cmk(c[i][1], c[i][3]));
+            put(r, cc, cmk(c[0], c[2]));
+            put(r, cc + 1, cmk(c[1], c[3]));
         }
         __syncthreads();
         return;
     }
-    red[(warp * 32 + lane) * 2] = cmk(c[0][0], c[0][2]);
-    red[(warp * 32 + lane) * 2 + 1] = cmk(c[0][1], c[0][3]);
+    const int ksplit = 8 / tiles, t = warp % tiles, ks0 = warp / tiles;
+    double c[4] = {0, 0, 0, 0};
+    if (ks0 < ksplit) ztile884(fa, fb, t / NT, t % NT, K, ks0, ksplit, lane, c);
+    red[(warp * 32 + lane) * 2] = cmk(c[0], c[2]);
+    red[(warp * 32 + lane) * 2 + 1] = cmk(c[1], c[3]);
     __syncthreads();
     if (warp < tiles) {
         double2 v0 = cmk(0, 0), v1 = cmk(0, 0);
@@ -306,7 +266,7 @@ __global__ void __launch_bounds__(256) k_ret_mp(GroupDev g, const ProbDev *__res
             else grow[e] = (e / s2 == n && ab / S == ab % S) ? cmk(0.0, -1.0) : cmk(0, 0);
         }
         __syncwarp();
-        double2 *ws = smem + C::stage + warp * C::WSW;
+        double2 *ws = smem + warp * C::WSW;
         if (VIE) ret_start_block_vie<S, WarpExec>(g, p, n, ws, WarpExec{lane});
         else ret_start_block<S, WarpExec>(g, p, n, ws, WarpExec{lane});
     }
@@ -326,24 +286,21 @@ __global__ void __launch_bounds__(256) k_ret_mp(GroupDev g, const ProbDev *__res
             }
         }
         const int mb = jhi + 1;
-        auto srcA = [&](int r, int kk) -> const double2 * {
+        auto fa = [&](int r, int kk) -> double2 {
             const int q = r / S, a = r % S, m = mb + kk / S, b = kk % S;
-            return (q < np && m <= n) ? rows[q] + (long)m * s2 + a * S + b : nullptr;
+            if (q >= np || m > n) return cmk(0, 0);
+            return cscale(rows[q][(long)m * s2 + a * S + b], ret_cw(k, n, m));
         };
-        auto srcB = [&](int kk, int cc) -> const double2 * {
+        auto fb = [&](int kk, int cc) -> double2 {
             const int m = mb + kk / S, b = kk % S, jj = cc / S, d = cc % S;
-            return (m <= n && jj < nb) ? g.rret + (tri(m) + jlo + jj) * s2 + b * S + d : nullptr;
+            if (m > n || jj >= nb) return cmk(0, 0);
+            return g.rret[(tri(m) + jlo + jj) * s2 + b * S + d];
         };
-        auto wA = [&](int kk) -> double {
-            const int m = mb + kk / S;
-            return m <= n ? ret_cw(k, n, m) : 0.0;
-        };
-        auto wB = [](int) -> double { return 1.0; };
         auto put = [&](int r, int cc, double2 v) {
             const int q = r / S, a = r % S, jj = cc / S, d = cc % S;
             if (q < np && jj < MP_JB) acc_s[(q * MP_JB + jj) * s2 + a * S + d] = v;
         };
-        zgemm_staged<S>(srcA, srcB, wA, wB, put, np * S, MP_JB * S, (n - jhi) * S, smem + C::stage, red, tid);
+        zgemm_cta(fa, fb, put, np * S, MP_JB * S, (n - jhi) * S, red, warp, lane);
         if (owner) {
             const double2 *grow = rows[warp];
             const int j = jlo + lane;
@@ -400,7 +357,7 @@ __global__ void __launch_bounds__(256) k_les_mp(GroupDev g, const ProbDev *__res
     const double2 *gl = owner ? g.gles + (long)p.col * S : nullptr;  // gles(j)[a][d] at gl[(j*S+a)*ldc + d]
     if (owner) {
         double2 *xcol = cols[warp];
-        double2 *ws = smem + C::stage + warp * C::WSW;
+        double2 *ws = smem + warp * C::WSW;
         if (VIE) {
             les_start_block_vie<S, WarpExec>(g, p, n, gl, ldc, xcol, ws, WarpExec{lane});
         } else {
@@ -427,24 +384,21 @@ __global__ void __launch_bounds__(256) k_les_mp(GroupDev g, const ProbDev *__res
                 if (ab == 0) wb[q] = greg_w(k, jlo + r, jlo + r2);
             }
         }
-        auto srcA = [&](int r, int kk) -> const double2 * {
+        auto fa = [&](int r, int kk) -> double2 {
             const int jj = r / S, a = r % S, m = kk / S, b = kk % S;
-            return (jj < nb && m < jlo) ? g.sret + (tri(jlo + jj) + m) * s2 + a * S + b : nullptr;
+            if (jj >= nb || m >= jlo) return cmk(0, 0);
+            return g.sret[(tri(jlo + jj) + m) * s2 + a * S + b];
         };
-        auto srcB = [&](int kk, int cc) -> const double2 * {
+        auto fb = [&](int kk, int cc) -> double2 {
             const int m = kk / S, b = kk % S, q = cc / S, d = cc % S;
-            return (q < np && m < jlo) ? cols[q] + (long)m * s2 + b * S + d : nullptr;
-        };
-        auto wA = [](int) -> double { return 1.0; };
-        auto wB = [&](int kk) -> double {
-            const int m = kk / S;
-            return m < jlo ? les_cw(k, m) : 0.0;
+            if (q >= np || m >= jlo) return cmk(0, 0);
+            return cscale(cols[q][(long)m * s2 + b * S + d], les_cw(k, m));
         };
         auto put = [&](int r, int cc, double2 v) {
             const int jj = r / S, a = r % S, q = cc / S, d = cc % S;
             if (q < np && jj < MP_JB) acc_s[(q * MP_JB + jj) * s2 + a * S + d] = v;
         };
-        zgemm_staged<S>(srcA, srcB, wA, wB, put, MP_JB * S, np * S, jlo * S, smem + C::stage, red, tid);
+        zgemm_cta(fa, fb, put, MP_JB * S, np * S, jlo * S, red, warp, lane);
         if (owner) {
             double2 *xcol = cols[warp];
             const int j = jlo + lane;
