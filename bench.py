@@ -166,6 +166,8 @@ def build_workload(name, rank, world):
         return workloads.config1(nk=64, nt=200, ntau=100, kshift=shift)
     if name == "config1-ncu":  # config-1 chain at nt=ntau=300: 1.5 GB of G^tv history, > L2
         return workloads.config1(nk=256, nt=300, ntau=300, kshift=shift)
+    if name == "config2":  # one 32-k-point chunk of the 512-k 4-band chain (chunks are independent)
+        return workloads.config2(chunk=32, chunk_index=rank % 16)
     if name == "config3":  # 96 uneven problems; ranks draw their own problems (seed + rank)
         return workloads.config3(seed=20261203 + rank)
     if name == "config3-small":
@@ -251,7 +253,8 @@ def allmax(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -76,9 +76,9 @@ __global__ void k_extrapolate(GroupDev g, const ProbDev *__restrict__ probs, int
 }
 
 // ---------------------------------------------------------------------------------------
-// k_gloc: G_loc(tstp) = (1/P) sum_p G_p(tstp) over the P problems of a group.  Block (32, 8):
-// threadIdx.x = element of the slice, threadIdx.y = problem lane (problems y, y+8, ...), then
-// the 8 lane sums are added in lane order, so the result does not depend on scheduling.
+// k_gloc + k_gloc_final: G_loc(tstp) = (1/P) sum_p G_p(tstp) over the P problems of a group, as
+// partial sums over chunks of 64 problems (block (32, 8): threadIdx.x = element of the slice,
+// threadIdx.y = problem lane) added in a fixed order, so the result does not depend on scheduling.
 // Slice elements: [ret(t,0..t) | tv planes (e*M + tau) | les(0..t,t)], or mat for tstp = -1.
 // G_loc is stored in libcntr's layout (tv as ((t M + tau) s^2 + e)).
 // ---------------------------------------------------------------------------------------
@@ -86,17 +86,22 @@ struct LocDev {
     double2 *ret, *les, *tv, *mat;  // G_loc, libcntr layout, ntmax / ntau / s of the group
 };
 
+#define GLOC_CHUNK 64  // problems per partial sum
+
+// pass 1: part[c][e] = sum of element e over problems c*64 .. c*64+63 (lanes y = 0..7 take every
+// 8th problem of the chunk, then the 8 lane sums are added in lane order)
 template <int S>
 __global__ void __launch_bounds__(256) k_gloc(GroupDev g, const ProbDev *__restrict__ probs, int nprob, int tstp,
-                                              LocDev loc) {
+                                              double2 *part, long ldpart) {
     __shared__ double2 red[8][32];
     const int s2 = S * S, M = g.ntau + 1;
     const long nret = tstp >= 0 ? (long)(tstp + 1) * s2 : 0, ntv = (long)M * s2;
     const long total = tstp >= 0 ? 2 * nret + ntv : ntv;
     const long e = blockIdx.x * 32L + threadIdx.x;
+    const int q0 = blockIdx.y * GLOC_CHUNK, q1 = min(nprob, q0 + GLOC_CHUNK);
     double2 acc = cmk(0, 0);
     if (e < total) {
-        for (int q = threadIdx.y; q < nprob; q += 8) {
+        for (int q = q0 + threadIdx.y; q < q1; q += 8) {
             const ProbDev &p = probs[q];
             double2 v;
             if (tstp < 0) v = p.gmat[e];
@@ -111,6 +116,20 @@ __global__ void __launch_bounds__(256) k_gloc(GroupDev g, const ProbDev *__restr
     if (threadIdx.y == 0 && e < total) {
         double2 v = red[0][threadIdx.x];
         for (int y = 1; y < 8; y++) v = cadd(v, red[y][threadIdx.x]);
+        part[blockIdx.y * ldpart + e] = v;
+    }
+}
+
+// pass 2: G_loc element e = (1/P) sum_c part[c][e], chunks in order, stored in libcntr layout
+template <int S>
+__global__ void k_gloc_final(GroupDev g, int nprob, int tstp, const double2 *__restrict__ part, long ldpart,
+                             int nchunk, LocDev loc) {
+    const int s2 = S * S, M = g.ntau + 1;
+    const long nret = tstp >= 0 ? (long)(tstp + 1) * s2 : 0, ntv = (long)M * s2;
+    const long total = tstp >= 0 ? 2 * nret + ntv : ntv;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        double2 v = part[e];
+        for (int c = 1; c < nchunk; c++) v = cadd(v, part[c * ldpart + e]);
         v = cscale(v, 1.0 / nprob);
         if (tstp < 0) loc.mat[e] = v;
         else if (e < nret) loc.ret[tri(tstp) * s2 + e] = v;

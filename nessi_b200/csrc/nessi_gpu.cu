@@ -99,6 +99,8 @@ struct Group {
     bool gmat_valid = false;
     MatScratch *d_mat = nullptr;  // per-member scratch of dyson_mat (allocated on first use)
     LocDev loc{nullptr, nullptr, nullptr, nullptr};  // G_loc of the group (allocated on first use)
+    double2 *gloc_part = nullptr;    // partial sums of G_loc over chunks of problems
+    long gloc_ld = 0;
     bool vie = false;                // VIE2 group: s* hold F, fcc* hold Fcc (nessi_gpu_set_F)
     int pp_ret = 0, pp_les = 0;      // Volterra kernel chosen by the autotuner (0: not yet)
     double2 *fccret = nullptr, *fccles = nullptr;
@@ -456,8 +458,12 @@ template <int S> int gloc_group(nessi_batch *b, Group &g, int tstp) {
     if (nact == 0) { set_err("gloc: no problem of the group reaches time step %d", tstp); return NESSI_ERR_ARG; }
     const long M = g.ntau + 1, s2 = (long)S * S;
     const long total = tstp >= 0 ? (2L * (tstp + 1) + M) * s2 : M * s2;
-    k_gloc<S><<<(unsigned)((total + 31) / 32), dim3(32, 8), 0, b->stream>>>(group_dev(g), g.d_probs, nact, tstp,
-                                                                          g.loc);
+    const int nchunk = (nact + GLOC_CHUNK - 1) / GLOC_CHUNK;
+    k_gloc<S><<<dim3((unsigned)((total + 31) / 32), (unsigned)nchunk), dim3(32, 8), 0, b->stream>>>(
+        group_dev(g), g.d_probs, nact, tstp, g.gloc_part, g.gloc_ld);
+    CK(cudaGetLastError());
+    k_gloc_final<S><<<(unsigned)std::min<long>((total + 255) / 256, 1184), 256, 0, b->stream>>>(
+        group_dev(g), nact, tstp, g.gloc_part, g.gloc_ld, nchunk, g.loc);
     CK(cudaGetLastError());
     return NESSI_OK;
 }
@@ -1055,6 +1061,9 @@ static int ensure_loc(nessi_batch *b, Group &g) {
     CKR(b->alloc(&g.loc.les, tri_h(N) * s2));
     CKR(b->alloc(&g.loc.tv, N * M * s2));
     CKR(b->alloc(&g.loc.mat, M * s2));
+    g.gloc_ld = (2 * N + M) * s2;  // longest slice
+    const long nchunk = ((long)g.members.size() + GLOC_CHUNK - 1) / GLOC_CHUNK;
+    CKR(b->alloc(&g.gloc_part, nchunk * g.gloc_ld));
     return NESSI_OK;
 }
 

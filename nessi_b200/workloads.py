@@ -76,7 +76,7 @@ def bootstrap_free(H0, mu, beta, h, k, ntau, sig=-1):
     return G
 
 
-def chain(nk, nt, ntau, beta, h, size1, k=5, V=0.5, mu=0.0, kshift=0.0):
+def chain(nk, nt, ntau, beta, h, size1, k=5, V=0.5, mu=0.0, kshift=0.0, kslice=None):
     if size1 == 2:
         eps_band = np.array([0.0, 1.0])
         hop = np.array([[0, 0.5], [0.5, 0]], np.complex128)
@@ -88,20 +88,25 @@ def chain(nk, nt, ntau, beta, h, size1, k=5, V=0.5, mu=0.0, kshift=0.0):
     else:
         raise ValueError("chain workloads have size1 2 or 4")
     kvals = -np.pi + 2 * np.pi * np.arange(nk) / nk + kshift
+    if kslice is not None:  # one chunk of the k-grid (the grid is propagated chunk by chunk)
+        kvals = kvals[kslice]
     H = chain_H(kvals, nt, h, eps_band, hop)
     Gb = eq.semicircle_bath(nt, ntau, beta, h)
     sigma = eq.kron_identity(Gb, size1, V * V)
     boot = []
     cache = {}
-    for i in range(nk):
+    for i in range(len(kvals)):
         key = H[i, 0].tobytes()
         if key not in cache:
             cache[key] = bootstrap_free(H[i, 0], mu, beta, h, k, ntau)
         boot.append(cache[key])
     descs = [dict(nt=nt, ntau=ntau, size1=size1, sig=-1, solve_order=k, sigma_group=0, beta=beta, h=h, mu=mu)
-             for _ in range(nk)]
+             for _ in range(len(kvals))]
     info = dict(model="%d-band chain" % size1, size1=size1, nk=nk, nt=nt, ntau=ntau, beta=beta, h=h,
                 solve_order=k, sigma="V^2 G_bath (x) 1, V=%g, shared" % V)
+    if kslice is not None:
+        info["k_chunk"] = "k-points %d..%d of %d (one chunk; G of the whole grid is 2.5 TB)" % (
+            kslice.start, kslice.stop - 1, nk)
     return Workload("chain%d" % size1, descs, sigma, H, boot, k, info)
 
 
@@ -110,9 +115,11 @@ def config1(nk=256, nt=1000, ntau=600, kshift=0.0):
     return chain(nk, nt, ntau, 20.0, 0.01, 2, kshift=kshift)
 
 
-def config2(nk=512, nt=4000, ntau=800, kshift=0.0):
-    """4-band chain, Nk=512, nt=4000, ntau=800, beta=20, h=0.01 (k-chunked when it does not fit)."""
-    return chain(nk, nt, ntau, 20.0, 0.01, 4, kshift=kshift)
+def config2(nk=512, nt=4000, ntau=800, kshift=0.0, chunk=32, chunk_index=0):
+    """4-band chain, Nk=512, nt=4000, ntau=800, beta=20, h=0.01, propagated in chunks of `chunk`
+    k-points (one chunk: 32 x 4.1 GB of G)."""
+    sl = slice(chunk_index * chunk, min(nk, (chunk_index + 1) * chunk))
+    return chain(nk, nt, ntau, 20.0, 0.01, 4, kshift=kshift, kslice=sl)
 
 
 def lattice2b(nkx, nky, nt, ntau, beta, h, u_max=2.0, t_ramp=2.0, ncorr=3, k=5, kshift=0.0):
