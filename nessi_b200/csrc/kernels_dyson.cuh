@@ -7,7 +7,7 @@
 //   k_prep_group     history coefficients for tv, dense copies of Sigma^< and Sigma^tv
 //   k_ret            G^R(n, 0..n): k-block start + Volterra recursion in t'   (:80-222)
 //   k_tv             G^tv(n, 0..ntau): history stream + Matsubara integral + solve (:651-741)
-//   k_les_operands   right-hand operands of the Sigma-shared products
+//   k_les_operands_t right-hand operands of the Sigma-shared products
 //   2 x ZGEMM        tv*vt + les*adv convolutions for all problems at once (conv_impl :1075-1394)
 //   k_les            G^<(0..n, n): k-block start + Volterra recursion in t (:893-1056)
 #pragma once
@@ -562,38 +562,11 @@ __global__ void k_gmat_stack(GroupDev g, const ProbDev *__restrict__ probs) {
 }
 
 // ---------------------------------------------------------------------------------------
-// k_les_operands: right-hand operands of the Sigma-shared products (conv_impl :1075-1394)
+// k_les_operands_t: right-hand operands of the Sigma-shared products (conv_impl :1075-1394)
 //   badv[(m,c)][(col,d)] = h w(n,m) G^R(n,m)^dagger[c][d],                 m = 0..n
 //   btv [(m,c)][(col,d)] = w(ntau,m) (-i dtau)(-sig) G^tv(n,ntau-m)^dagger[c][d]
-// ---------------------------------------------------------------------------------------
-template <int S>
-__global__ void k_les_operands(GroupDev g, const ProbDev *__restrict__ probs, int n, int which) {
-    const ProbDev p = probs[blockIdx.y];
-    const int k = g.k, s2 = S * S, ntau = g.ntau;
-    const double h = g.h, dtau = g.beta / ntau;
-    const long ldc = g.ldc;
-    // which: 1 = badv rows only, 2 = btv rows only, 3 = both
-    const int r0 = (which & 1) ? 0 : n + 1, r1 = (which & 2) ? (n + 1) + (ntau + 1) : n + 1;
-    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < (long)(r1 - r0) * s2; e += (long)gridDim.x * blockDim.x) {
-        int r = r0 + (int)(e / s2), cd = (int)(e % s2), c = cd / S, d = cd % S;
-        if (r <= n) {
-            const int m = r;
-            double2 v = cconj(p.gret[(tri(n) + m) * s2 + d * S + c]);
-            g.badv[((long)m * S + c) * ldc + (long)p.col * S + d] = cscale(v, h * greg_w(k, n, m));
-        } else {
-            const int m = r - (n + 1);
-            double2 v = cconj(p.gtv[((long)n * s2 + d * S + c) * (ntau + 1) + (ntau - m)]);
-            // (-i dtau)(-sig) v * w
-            double2 f = cmk(0.0, dtau * (double)g.sig * greg_w(k, ntau, m));
-            g.btv[((long)m * S + c) * ldc + (long)p.col * S + d] = cmul(f, v);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------------------
-// k_les_operands_t: the same operands as k_les_operands, written row by row.  badv / btv are
-// row-major with the problems side by side in a row, so one problem's column is a strided
-// write; here a CTA takes a tile of LOT problems x LOR time indices, reads each problem's
+// badv / btv are row-major with the problems side by side in a row, so one problem's column is
+// a strided write; a CTA takes a tile of LOT problems x LOR time indices, reads each problem's
 // contiguous slice into shared memory and writes whole row segments (coalesced).
 //   which = 1: badv rows m = 0..n (from G^R(n, m)); which = 2: btv rows m = 0..ntau (from G^tv(n, .))
 // ---------------------------------------------------------------------------------------

@@ -5,15 +5,15 @@
 // blocks of 32 rows.  For a block, the sum over every row solved before it ("phase A") is
 //   ret:  acc(j) = sum_{m > jhi} w(n-j, n-m) G(n,m) Sigma^R(m,j)
 //   les:  acc(j) = sum_{m < jlo} w(j,m) Sigma^R(j,m) G^<(m,n)
-// Sigma (F / Fcc for VIE2) is shared by all problems of a group, so a CTA takes PP problems and
-// streams each Sigma tile through shared memory ONCE for all of them (cp.async double buffer),
-// instead of every problem reading the whole triangle from L2.  Away from the diagonal
-// (|m - j| > k) the Gregory weight depends on m alone (c_m: omega at the n / 0 end, else 1), so
-// the tiles are weighted per column; the <= k terms next to the block are corrected to the exact
-// weight afterwards.  Each problem owns 8/PP warps that split the tile columns; their partial sums
-// are added in warp order.  The rows of the block are then solved by the problem's first warp
-// with each lane owning one row in registers (as in the one-problem kernels), and the next block
-// starts.  PP is chosen on the host from the number of active problems.
+// Sigma (F / Fcc for VIE2) is shared by all problems of a group, so a CTA takes PP <= 8 problems
+// and computes phase A for all of them at once as one complex GEMM on the FP64 tensor cores
+// (mma.sync m8n8k4 .f64, four real MMAs per complex 8x8x4 tile): each Sigma element is read once
+// per CTA instead of once per problem.  The fragments are loaded from global memory (L2) eight
+// k-steps ahead of their MMAs.  Away from the diagonal (|m - j| > k) the Gregory weight depends
+// on m alone (c_m: omega at the n / 0 end, else 1), so it is a column scale of the GEMM; the <= k
+// terms next to the block are corrected to the exact weight afterwards.  Warp q then solves the
+// block's rows of problem q with each lane owning one row in registers (as in the one-problem
+// kernels), and the next block starts.  PP is chosen per group by the autotuner on the host.
 #pragma once
 
 #define MP_JB 32  // rows per block (lane = row)
