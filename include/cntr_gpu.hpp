@@ -78,6 +78,7 @@ template <class HM, class FN> class Batch {
     void set_Q(int p, HM &Q) {
         check(nessi_gpu_set_Q(b_, p, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0)));
     }
+    void vie2_mat() { check(nessi_gpu_vie2_mat(b_)); }
     void vie2_start() { check(nessi_gpu_vie2_start(b_)); }
     void vie2_timestep(int n) { check(nessi_gpu_vie2_timestep(b_, n)); }
     // self-consistent lattice with the local second-order self-energy of G_loc

@@ -97,8 +97,8 @@ int nessi_gpu_dyson_timestep(nessi_batch *b, int n);
  * A group becomes a VIE2 group when its kernel F is set: F (and its hermitian-conjugate partner
  * Fcc, which the retarded and lesser parts need where F is not hermitian) are shared by the
  * group, Q is per problem.  dyson_* calls act on Dyson groups only and vie2_* calls on VIE2
- * groups only, so one batch may hold both kinds.  G^mat of a VIE2 problem is the caller's
- * (set_G / set_timestep(-1)). */
+ * groups only, so one batch may hold both kinds.  G^mat of a VIE2 problem comes from
+ * nessi_gpu_vie2_mat or from the caller (set_G / set_timestep(-1)). */
 /* F and Fcc of a group (herm_matrix layout; Fcc's ret and les only). */
 int nessi_gpu_set_F(nessi_batch *b, int group, const void *ret, const void *les, const void *tv, const void *mat,
                     const void *cc_ret, const void *cc_les);
@@ -107,6 +107,10 @@ int nessi_gpu_set_F_timestep(nessi_batch *b, int group, int tstp, const void *sl
 /* The source term Q of problem p, whole or one time step. */
 int nessi_gpu_set_Q(nessi_batch *b, int p, const void *ret, const void *les, const void *tv, const void *mat);
 int nessi_gpu_set_Q_timestep(nessi_batch *b, int p, int tstp, const void *slice);
+/* cntr::vie2_mat(G, F, Fcc, Q, beta, SolveOrder) with the default fixpoint method
+ * (cntr_vie2_decl.hpp:63, cntr_vie2_impl.hpp:460-484, 1091-1160): G^mat of every VIE2 problem
+ * from the group's F^mat and the problem's Q^mat.  ntau must be even. */
+int nessi_gpu_vie2_mat(nessi_batch *b);
 /* cntr::vie2_start(G, F, Fcc, Q, SolveOrder, beta, h) (cntr_vie2_decl.hpp:67,
  * cntr_vie2_impl.hpp:1338-1420): time steps 0..k of every VIE2 problem from G^mat. */
 int nessi_gpu_vie2_start(nessi_batch *b);

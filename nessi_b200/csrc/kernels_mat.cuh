@@ -327,3 +327,37 @@ template <int S>
 __global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr) {
     dyson_mat_body<S>(g, probs[blockIdx.x], scr[blockIdx.x]);
 }
+
+// vie2_mat on the device (cntr::vie2_mat with the default fixpoint method, cntr_vie2_impl.hpp:
+// 460-484, 1091-1160): G^mat = vie2_mat_fourier(F, Q) (:305-455), then 6 corrections
+// G -= fourier(F, F*G + G - Q).  F^mat is the group's (g.smat), Q^mat of the problem is in w.G0.
+// One CTA per problem.
+template <int S>
+__global__ void __launch_bounds__(256) k_vie2_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr) {
+    constexpr int s2 = S * S;
+    __shared__ double2 qmasy[S * S];
+    extern __shared__ double2 tw[];  // 2 ntau twiddles e^{i pi q / ntau}
+    const ProbDev p = probs[blockIdx.x];
+    const MatScratch w = scr[blockIdx.x];
+    const int k = g.k, ntau = g.ntau, M = ntau + 1, sig = g.sig;
+    const double beta = g.beta, dtau = beta / ntau;
+    for (int q = threadIdx.x; q < 2 * ntau; q += blockDim.x) {
+        double sn, cs;
+        sincospi((double)q / (double)ntau, &sn, &cs);
+        tw[q] = cmk(cs, sn);
+    }
+    __syncthreads();
+    mat_dft_dev<S>(w.fdft, g.smat, ntau, sig == -1 ? 1 : 0, tw);
+    __syncthreads();
+    const int pcf = 5;
+    vie2_mat_fourier_dev<S>(p.gmat, g.smat, w.G0, w.fdft, w.qdft, w.Z, qmasy, ntau, sig, beta, pcf, tw);
+    for (int it = 0; it < 6; it++) {
+        conv_mat_dev<S>(w.Q, g.smat, p.gmat, k, ntau, sig, dtau);
+        __syncthreads();
+        for (int e = threadIdx.x; e < M * s2; e += blockDim.x) w.Q[e] = csub(cadd(w.Q[e], p.gmat[e]), w.G0[e]);
+        __syncthreads();
+        vie2_mat_fourier_dev<S>(w.dG, g.smat, w.Q, w.fdft, w.qdft, w.Z, qmasy, ntau, sig, beta, pcf, tw);
+        for (int e = threadIdx.x; e < M * s2; e += blockDim.x) p.gmat[e] = csub(p.gmat[e], w.dG[e]);
+        __syncthreads();
+    }
+}

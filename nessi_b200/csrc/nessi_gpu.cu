@@ -98,6 +98,7 @@ struct Group {
     int dense_valid = -1, ret_valid = -1, les_valid = -1;
     bool gmat_valid = false;
     MatScratch *d_mat = nullptr;  // per-member scratch of dyson_mat (allocated on first use)
+    std::vector<MatScratch> h_mat;   // host copy of the same pointers
     LocDev loc{nullptr, nullptr, nullptr, nullptr};  // G_loc of the group (allocated on first use)
     double2 *gloc_part = nullptr;    // partial sums of G_loc over chunks of problems
     long gloc_ld = 0;
@@ -412,27 +413,51 @@ template <int S> int start_group(nessi_batch *b, Group &g) {
     return NESSI_OK;
 }
 
+static int ensure_mat_scratch(nessi_batch *b, Group &g) {
+    if (g.d_mat) return NESSI_OK;
+    const long M = g.ntau + 1, s2 = (long)g.s * g.s;
+    std::vector<MatScratch> h(g.members.size());
+    for (auto &w : h) {
+        int r;
+        if ((r = b->alloc(&w.G0, M * s2)) || (r = b->alloc(&w.F, M * s2)) || (r = b->alloc(&w.Q, M * s2)) ||
+            (r = b->alloc(&w.dG, M * s2)) || (r = b->alloc(&w.fdft, M * s2)) || (r = b->alloc(&w.qdft, M * s2)) ||
+            (r = b->alloc(&w.Z, 2 * g.ntau * s2)))
+            return r;
+    }
+    void *q = nullptr;
+    CK(cudaMalloc(&q, h.size() * sizeof(MatScratch)));
+    b->allocs.push_back(q);
+    g.d_mat = (MatScratch *)q;
+    g.h_mat = h;
+    CK(cudaMemcpyAsync(g.d_mat, h.data(), h.size() * sizeof(MatScratch), cudaMemcpyHostToDevice, b->stream));
+    return NESSI_OK;
+}
+
 template <int S> int mat_group(nessi_batch *b, Group &g) {
     const GroupDev gd = group_dev(g);
-    const long M = g.ntau + 1, s2 = (long)S * S;
-    if (!g.d_mat) {
-        std::vector<MatScratch> h(g.members.size());
-        for (auto &w : h) {
-            int r;
-            if ((r = b->alloc(&w.G0, M * s2)) || (r = b->alloc(&w.F, M * s2)) || (r = b->alloc(&w.Q, M * s2)) ||
-                (r = b->alloc(&w.dG, M * s2)) || (r = b->alloc(&w.fdft, M * s2)) || (r = b->alloc(&w.qdft, M * s2)) ||
-                (r = b->alloc(&w.Z, 2 * g.ntau * s2)))
-                return r;
-        }
-        void *q = nullptr;
-        CK(cudaMalloc(&q, h.size() * sizeof(MatScratch)));
-        b->allocs.push_back(q);
-        g.d_mat = (MatScratch *)q;
-        CK(cudaMemcpyAsync(g.d_mat, h.data(), h.size() * sizeof(MatScratch), cudaMemcpyHostToDevice, b->stream));
-    }
+    CKR(ensure_mat_scratch(b, g));
     const size_t sm = 2 * (size_t)g.ntau * sizeof(double2);
     CK(cudaFuncSetAttribute(k_dyson_mat<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_dyson_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat);
+    CK(cudaGetLastError());
+    g.gmat_valid = false;
+    return NESSI_OK;
+}
+
+// vie2_mat of a VIE2 group: Q^mat of every member is copied into its scratch slot G0 first
+template <int S> int vie2_mat_group(nessi_batch *b, Group &g) {
+    const GroupDev gd = group_dev(g);
+    CKR(ensure_mat_scratch(b, g));
+    const long M = g.ntau + 1, s2 = (long)g.s * g.s;
+    for (size_t c = 0; c < g.members.size(); c++) {
+        const Prob &q = b->probs[g.members[c]];
+        if (!q.qmat) { set_err("vie2_mat: Q of problem %d not set", g.members[c]); return NESSI_ERR_ARG; }
+        CK(cudaMemcpyAsync(g.h_mat[c].G0, q.qmat, (size_t)M * s2 * sizeof(double2), cudaMemcpyDeviceToDevice,
+                           b->stream));
+    }
+    const size_t sm = 2 * (size_t)g.ntau * sizeof(double2);
+    CK(cudaFuncSetAttribute(k_vie2_mat<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_vie2_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat);
     CK(cudaGetLastError());
     g.gmat_valid = false;
     return NESSI_OK;
@@ -505,6 +530,7 @@ int extrap_dispatch(nessi_batch *b, Group &g, int n) { NESSI_SIZE_SWITCH(extrap_
 int gloc_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(gloc_group, b, g, tstp) }
 int sigma2b_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(sigma2b_group, b, g, tstp) }
 int mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(mat_group, b, g) }
+int vie2_mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(vie2_mat_group, b, g) }
 
 template <int S> int step_group_any(nessi_batch *b, Group &g, int n, int nact) {
     return g.vie ? step_group<S, true>(b, g, n, nact) : step_group<S, false>(b, g, n, nact);
@@ -962,6 +988,20 @@ static int start_kind(nessi_batch *b, bool vie, const char *name) {
 int nessi_gpu_dyson_start(nessi_batch *b) { return start_kind(b, false, "dyson_start"); }
 
 int nessi_gpu_vie2_start(nessi_batch *b) { return start_kind(b, true, "vie2_start"); }
+
+int nessi_gpu_vie2_mat(nessi_batch *b) {
+    CKR(check_batch(b));
+    bool any = false;
+    for (Group &g : b->groups) {
+        if (!g.vie) continue;
+        any = true;
+        if (g.ntau % 2) { set_err("vie2_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
+        CKR(vie2_mat_dispatch(b, g));
+    }
+    if (!any) { set_err("vie2_mat: the batch has no VIE2 group (nessi_gpu_set_F)"); return NESSI_ERR_ARG; }
+    CK(cudaStreamSynchronize(b->stream));
+    return NESSI_OK;
+}
 
 static int sync_probdev(nessi_batch *b, int p) {
     Prob &q = b->probs[p];

@@ -71,6 +71,7 @@ EXPORTS = {
     "nessi_gpu_set_Q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
     "nessi_gpu_set_Q_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "nessi_gpu_vie2_start": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_vie2_mat": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_vie2_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_set_U": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "nessi_gpu_extrapolate_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -219,6 +220,10 @@ class Batch:
     def set_Q_timestep(self, p, tstp, data):
         _check(load_library().nessi_gpu_set_Q_timestep(self._h, p, tstp, _ptr(np.ascontiguousarray(data,
                                                                                                     np.complex128))))
+
+    def vie2_mat(self):
+        """G^mat of every VIE2 problem (cntr::vie2_mat, fixpoint method)."""
+        _check(load_library().nessi_gpu_vie2_mat(self._h))
 
     def vie2_start(self):
         """Time steps 0..k of every VIE2 problem (cntr::vie2_start)."""

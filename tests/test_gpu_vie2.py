@@ -213,3 +213,32 @@ def test_vie2_problems_per_cta(oracle, monkeypatch, pp):
         b.get_G(p, Gg)
         _check(Gg, ref[p][0], k, nt, TOL)
     b.close()
+
+
+@pytest.mark.parametrize("s", [1, 2, 3])
+def test_vie2_mat_and_whole_pipeline(oracle, s):
+    """vie2_mat on the GPU (fixpoint method) against the oracle, then vie2_start and vie2_timestep
+    from that G^mat: the whole VIE2 propagation on the device."""
+    from nessi_b200 import gpu
+    rng = np.random.default_rng(500 + s)
+    nt, ntau, beta, h, k = 20, 16, 4.0, 0.05, 5
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Qs = [_source(oracle, rng, nt, ntau, s, beta, h) for _ in range(2)]
+    ref = [_oracle_vie2(oracle, F, Fcc, Q, beta, h, k) for Q in Qs]
+    b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, beta=beta, h=h)] * 2)
+    b.set_F(0, F, Fcc)
+    for p, Q in enumerate(Qs):
+        b.set_Q(p, Q)
+    b.vie2_mat()
+    for p in range(2):
+        m = np.zeros((ntau + 1, s, s), np.complex128)
+        b.get_timestep(p, -1, m)
+        assert rel_err(m, ref[p][1].mat) < TOL
+    b.vie2_start()
+    for n in range(k + 1, nt + 1):
+        b.vie2_timestep(n)
+    for p in range(2):
+        Gg = herm_matrix(nt, ntau, s, -1)
+        b.get_G(p, Gg)
+        _check(Gg, ref[p][0], k, nt, TOL)
+    b.close()
