@@ -220,13 +220,59 @@ def compare_with_fp64(b, W, run_step, nt, k):
     b64.synchronize()
     ref = _result_sample(b64, W, nt)
     b64.close()
-    err = {}
-    for comp in ("ret", "les", "tv"):
-        num = max(float(np.max(np.abs(getattr(x, comp) - getattr(y, comp)))) for x, y in zip(mixed, ref))
-        den = max(float(np.max(np.abs(getattr(y, comp)))) for y in ref)
-        err[comp] = num / den if den else 0.0
+    err = _max_rel(mixed, ref)
     err["compared"] = "G_loc, all time steps" if W.lattice else "all components of %d problems" % len(ref)
     return err
+
+
+def _max_rel(xs, ys):
+    err = {}
+    for comp in ("ret", "les", "tv"):
+        num = max(float(np.max(np.abs(getattr(x, comp) - getattr(y, comp)))) for x, y in zip(xs, ys))
+        den = max(float(np.max(np.abs(getattr(y, comp)))) for y in ys)
+        err[comp] = num / den if den else 0.0
+    return err
+
+
+def mixed_companion(b, W, nt, k, fp64_value, args, world, stream):
+    """The mixed-precision path on the same inputs, after the FP64 measurement: its throughput
+    (same step definition, warm-up and timing as the FP64 line) and the max relative error of its
+    result against the FP64 result per component.  The FP64 batch is released first."""
+    import torch
+    from nessi_b200 import gpu, workloads
+    ref = _result_sample(b, W, nt)
+    b.close()
+    bm = gpu.Batch(W.descs, precision=gpu.PREC_MIXED)
+    try:
+        workloads.upload(bm, W)
+        bm.set_stream(stream.cuda_stream)
+
+        def prop():
+            for n in range(k + 1, nt + 1):
+                bm.dyson_timestep(n)
+        for _ in range(max(1, args.warmup)):
+            prop()
+        bm.synchronize()
+        bm.graph_record(bm.GRAPH_DYSON, k + 1, nt)
+        bm.graph_launch()
+        bm.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            bm.graph_launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = allmax(e0.elapsed_time(e1), world)
+        value = world * W.kpt_steps() * args.steps / (ms / 1000.0)
+        err = _max_rel(_result_sample(bm, W, nt), ref)
+    finally:
+        bm.close()
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "ratio_to_fp64": value / fp64_value,
+            "max_rel_error_vs_fp64": err, "error_compared": "all components of %d problems, all time steps" % len(ref),
+            "dtype": "complex64 history / complex128 solves"}
 
 
 def dist_setup(args):
@@ -295,6 +341,8 @@ def main():
     ap.add_argument("--mixed-error", action="store_true",
                     help="with --precision mixed: afterwards run the FP64 path on the same inputs and report the "
                          "max relative error of the mixed result per component")
+    ap.add_argument("--no-mixed", action="store_true", help="do not add the mixed-precision companion "
+                    "measurement to the FP64 line")
     ap.add_argument("--no-graph", action="store_true", help="launch every step eagerly instead of replaying "
                     "a CUDA graph of the propagation")
     args = ap.parse_args()
@@ -473,6 +521,16 @@ def main():
     mixed_err = None
     if args.mixed_error and args.precision == "mixed":
         mixed_err = compare_with_fp64(b, W, run_step, nt, k)
+    # the metric compares mixed with FP64: the default (FP64) line of the chain workloads also
+    # carries the mixed path measured on the same inputs
+    mixed_line = None
+    closed = False
+    if args.precision == "fp64" and not W.lattice and not isinstance(W.sigma, dict) and not args.no_mixed:
+        try:
+            mixed_line = mixed_companion(b, W, nt, k, value, args, world, stream)
+        except Exception as exc:  # the FP64 line stands on its own
+            mixed_line = {"error": "%s: %s" % (type(exc).__name__, exc)}
+        closed = True
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -493,8 +551,10 @@ def main():
                 "volterra_kernels": {g: {"ret": v[0], "les": v[1]} for g, v in volterra.items()}}
         if mixed_err is not None:
             line["mixed_error_vs_fp64_gpu"] = mixed_err
+        if mixed_line is not None:
+            line["mixed"] = mixed_line
         print(json.dumps(line), flush=True)
-    if not (args.mixed_error and args.precision == "mixed"):
+    if not closed and not (args.mixed_error and args.precision == "mixed"):
         b.close()
     if world > 1:
         import torch.distributed as dist
