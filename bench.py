@@ -1,12 +1,19 @@
-"""Benchmark of the batched Dyson time stepping (libcntr dyson_timestep hot path) on B200.
+"""Benchmark of the batched Kadanoff-Baym time stepping (libcntr dyson_timestep hot path) on B200.
 
 One bench step = the whole time-stepping phase n = k+1..nt of every k-point of the workload
 (the metric counts k-point time steps; Matsubara and bootstrap are set-up, outside the timed
-region).  Inputs are resident in HBM for `value`; `e2e` repeats the step through the public
-API with host buffers (Sigma, H and bootstrap uploaded, the full G downloaded every step).
+region).  After the warm-up, one eager propagation gives the per-kernel device times (and the
+k_tv roofline); the propagation is then recorded as one CUDA graph and every timed step replays
+it (--no-graph: eager launches).  Inputs are resident in HBM for `value`; `e2e` repeats the step
+through the public API with host buffers (Sigma, H and bootstrap uploaded, the result downloaded
+every step).  The FP64 line of the chain workloads also carries `mixed`: the mixed-precision
+path on the same inputs, its throughput, its ratio to FP64 and its max relative error per
+component against the FP64 result (--no-mixed skips it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload config1] [--precision fp64|mixed]
+                    [--workload config1|config1-small|config1-ncu|config2|config3|config3-small|
+                                config4|config4-small|config4-ncu]
+                    [--precision fp64|mixed] [--mixed-error] [--no-cpu] [--no-e2e] [--no-graph]
 
 Under torchrun each rank advances its own k-grid (shifted by rank/N of a grid spacing): the
 k-points are independent, so ranks share no data ("scaling": "weak").  `--impl reference`
