@@ -16,7 +16,10 @@ component against the FP64 result (--no-mixed skips it).
                     [--precision fp64|mixed] [--mixed-error] [--no-cpu] [--no-e2e] [--no-graph]
 
 Under torchrun each rank advances its own k-grid (shifted by rank/N of a grid spacing): the
-k-points are independent, so ranks share no data ("scaling": "weak").  `--impl reference`
+k-points of the chain workloads are independent, so ranks share no data ("scaling": "weak").
+The lattice workloads (config4*) form ONE lattice from all ranks' grids: after every k-average
+the ranks sum the weighted G_loc time-step slice with an NCCL all-reduce (nessi_b200.lattice),
+and those steps launch eagerly.  `--impl reference`
 times the CPU restatement of libcntr's serial path (oracle/, OpenMP over k-points) on a
 bounded sample of the same workload.
 """
@@ -371,14 +374,30 @@ def main():
     k = W.k
     nt = max(d["nt"] for d in W.descs)
 
+    sharded = None
+    if W.lattice and world > 1:
+        # one lattice over the k-points of all ranks (each rank's grid is shifted, so together they
+        # form a finer one): after every k-average the ranks sum the weighted G_loc slice with one
+        # NCCL all-reduce; the steps launch eagerly (no graph around the collectives)
+        from nessi_b200.lattice import ShardedLattice
+        sharded = ShardedLattice(b, stream=stream)
+
+    def lattice_start():
+        if sharded is not None:
+            return sharded.start(max_iter=30, tol=1e-12)
+        return b.lattice_2b_start(max_iter=30, tol=1e-12)
+
     if W.lattice:
         # set-up (untimed): self-consistent bootstrap of steps 0..k
-        boot_iters, boot_err = b.lattice_2b_start(max_iter=30, tol=1e-12)
+        boot_iters, boot_err = lattice_start()
 
     def propagate():
         if W.lattice:
             for n in range(k + 1, nt + 1):
-                b.lattice_2b_timestep(n, W.ncorr)
+                if sharded is not None:
+                    sharded.timestep(n, W.ncorr)
+                else:
+                    b.lattice_2b_timestep(n, W.ncorr)
         else:
             for n in range(k + 1, nt + 1):
                 b.dyson_timestep(n)
@@ -386,7 +405,7 @@ def main():
     for _ in range(args.warmup):
         propagate()
     b.synchronize()
-    use_graph = not args.no_graph
+    use_graph = not args.no_graph and sharded is None
     if use_graph:
         # per-kernel device times from one eager propagation (untimed); then the propagation is
         # recorded once as a CUDA graph and every timed step replays it
@@ -490,7 +509,7 @@ def main():
         for _ in range(args.steps):
             workloads.upload(b, W)
             if W.lattice:
-                b.lattice_2b_start(max_iter=30, tol=1e-12)
+                lattice_start()
             run_step()
             if W.lattice:
                 b.get_gloc(0, gloc_host)
@@ -556,6 +575,12 @@ def main():
                 "gpu_launches": gpu_launches, "clocks": clk,
                 "launch": "CUDA graph of the whole propagation, replayed each step" if use_graph else "eager",
                 "volterra_kernels": {g: {"ret": v[0], "les": v[1]} for g, v in volterra.items()}}
+        if sharded is not None:
+            line["lattice_exchange"] = {
+                "collective": "NCCL all-reduce of the weighted G_loc time-step slice after every k-average",
+                "k_points_total": sharded.nk_total[0], "k_points_this_rank": len(W.descs),
+                "bytes_per_all_reduce_at_nt": sharded.exchange_bytes(nt),
+                "all_reduces_per_time_step": W.ncorr + 1}
         if mixed_err is not None:
             line["mixed_error_vs_fp64_gpu"] = mixed_err
         if mixed_line is not None:

@@ -180,6 +180,13 @@ int nessi_gpu_sigma_2b_timestep(nessi_batch *b, int group, int tstp);
 /* Download G_loc / Sigma of a group (libcntr layout; NULL skips a component). */
 int nessi_gpu_get_gloc(nessi_batch *b, int group, void *ret, void *les, void *tv, void *mat);
 int nessi_gpu_get_sigma(nessi_batch *b, int group, void *ret, void *les, void *tv, void *mat);
+/* Device addresses of the group's G_loc (libcntr layout: ret and les packed triangles,
+ * tv ((t (ntau+1) + tau) s^2 + e), mat), valid until the batch is destroyed.  For k-points
+ * sharded over processes: each process averages its own problems with nessi_gpu_gloc_timestep,
+ * and the processes sum the weighted time-step slices in place (an all-reduce over NCCL), which
+ * replaces the MPI_Allgatherv of the k-slices in gw_selfene_impl.cpp:18-28 /
+ * cntr_distributed_array_impl.hpp:370-399.  Launches nothing; NULL skips a component. */
+int nessi_gpu_gloc_device(nessi_batch *b, int group, void **ret, void **les, void **tv, void **mat);
 /* Bootstrap (hubbard_chain_2b.cpp:245-290 with G -> G_loc): iterate
  *   Sigma(0..k) = Sigma_2B[G_loc];  dyson_start of every problem;  G_loc(0..k)
  * until sum_t distance_norm2(t) between successive G_loc is below tol after more than 3

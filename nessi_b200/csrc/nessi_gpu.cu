@@ -1179,6 +1179,17 @@ int nessi_gpu_get_sigma(nessi_batch *b, int group, void *ret, void *les, void *t
     return NESSI_OK;
 }
 
+int nessi_gpu_gloc_device(nessi_batch *b, int group, void **ret, void **les, void **tv, void **mat) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    CKR(ensure_loc(b, *g));
+    if (ret) *ret = g->loc.ret;
+    if (les) *les = g->loc.les;
+    if (tv) *tv = g->loc.tv;
+    if (mat) *mat = g->loc.mat;
+    return NESSI_OK;
+}
+
 // distance_norm2 of time step t between two herm_matrix_timestep-like host buffers (ret row,
 // tv row, les column of t; cntr_utilities_impl.hpp:607-650)
 static double slice_distance(const double2 *a, const double2 *b, long n_elem, int s2) {

@@ -79,6 +79,7 @@ EXPORTS = {
     "nessi_gpu_sigma_2b_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "nessi_gpu_get_gloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
     "nessi_gpu_get_sigma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
+    "nessi_gpu_gloc_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.POINTER(ctypes.c_void_p)] * 4),
     "nessi_gpu_lattice_2b_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "nessi_gpu_lattice_2b_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
@@ -270,6 +271,23 @@ class Batch:
     def get_sigma(self, group, S):
         _check(load_library().nessi_gpu_get_sigma(self._h, group, _ptr(S.ret), _ptr(S.les), _ptr(S.tv), _ptr(S.mat)))
 
+    def group_shape(self, group):
+        """(ntmax, ntau, size1, solve_order, number of problems) of a sigma group."""
+        m = [d for d in self.descs if d.get("sigma_group", 0) == group]
+        if not m:
+            raise NessiGpuError(1, "no problem in sigma group %d" % group)
+        return max(d["nt"] for d in m), m[0]["ntau"], m[0].get("size1", 1), m[0].get("solve_order", 5), len(m)
+
+    def gloc_views(self, group):
+        """{component: torch float64 tensor} aliasing the group's G_loc in device memory (no copy;
+        libcntr layout, real and imaginary parts interleaved), valid while the batch lives."""
+        ntmax, ntau, s, _, _ = self.group_shape(group)
+        ptrs = [ctypes.c_void_p() for _ in range(4)]
+        _check(load_library().nessi_gpu_gloc_device(self._h, group, *[ctypes.byref(q) for q in ptrs]))
+        s2, N, M = s * s, ntmax + 1, ntau + 1
+        sizes = {"ret": N * (N + 1) // 2 * s2, "les": N * (N + 1) // 2 * s2, "tv": N * M * s2, "mat": M * s2}
+        return {c: _device_f64(q.value, 2 * sizes[c]) for c, q in zip(("ret", "les", "tv", "mat"), ptrs)}
+
     def lattice_2b_start(self, max_iter=20, tol=1e-12):
         """Bootstrap of the lattice; returns (iterations, last distance)."""
         it, err = ctypes.c_int(), ctypes.c_double()
@@ -295,6 +313,20 @@ class Batch:
                                                          ctypes.byref(by)))
             out[name] = (ms.value, nl.value, by.value)
         return out
+
+
+class _DeviceBuffer:
+    """Device memory of the library described by the CUDA array interface (read by torch)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2}
+
+
+def _device_f64(ptr, n):
+    import torch
+    if not ptr:
+        raise NessiGpuError(3, "null device pointer")
+    return torch.as_tensor(_DeviceBuffer(ptr, n), device="cuda")
 
 
 def dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, H_ptr, sigma_mat_ptr, gmat_ptr, stream=0):
