@@ -94,3 +94,42 @@ def test_extrapolation_is_exact_for_polynomials(oracle):
     assert np.allclose(G.tv[n + 1, :, 0, 0], [f(n + 1, m) for m in range(ntau + 1)], rtol=1e-10, atol=1e-9)
     assert np.allclose(G.ret_row(n + 1)[k + 1:, 0, 0], [f(n + 1, tp) for tp in range(k + 1, n + 2)],
                        rtol=1e-10, atol=1e-9)
+
+
+def test_dyson_mat_fixpoint_embedding(oracle):
+    """libcntr/test/matsubara.cpp:34-94: the Matsubara Dyson equation of the level eps1 = -1
+    embedded by lam = 0.2 into eps2 = 1 (beta = 20, ntau = 400, order 5), solved by the fixpoint
+    method, reproduces the (0,0) element of the free 2 x 2 propagator within 1e-7."""
+    O = oracle
+    eps1, eps2, lam, mu, beta, ntau, k = -1.0, 1.0, 0.2, 0.0, 20.0, 400, 5
+    G2 = herm_matrix(-1, ntau, 2, -1)
+    O.green_from_H(G2, mu, np.array([[eps1, 1j * lam], [-1j * lam, eps2]]), beta, 1.0)
+    exact = herm_matrix(-1, ntau, 1, -1)
+    exact.mat[:, 0, 0] = G2.mat[:, 0, 0]
+    Sig = herm_matrix(-1, ntau, 1, -1)
+    O.green_from_H(Sig, mu, np.array([[eps2]]), beta, 1.0)
+    Sig.smul(-1, lam * lam)
+    H = function(-1, 1)
+    H.set_value(-1, np.array([[eps1]]))
+    G = herm_matrix(-1, ntau, 1, -1)
+    O.dyson_mat(G, Sig, mu, H, beta, k, method=O.CNTR_MAT_FIXPOINT)
+    err = O.distance_norm2(-1, exact, G)
+    assert err < 1.0e-7, err               # matsubara.cpp:47 (tol_tight)
+
+
+@pytest.mark.parametrize("sig,shift", [(-1, 0.0), (1, 3.0)])
+def test_green_from_H_is_the_free_propagator(oracle, sig, shift):
+    """libcntr/test/equilibrium.cpp:240-290: green_from_H of the 2 x 2 H = sqrt(2) [[1, -i], [i, -1]]
+    (nt = 100, ntau = 500, beta = 5, h = 0.01) against the closed form V g(w) V^dagger of its
+    eigenlevels, summed distance over t = -1..nt-1 below 1e-6.  The bosonic variant shifts the
+    levels above the chemical potential (w + 3 > 0) so that the occupations stay finite."""
+    from test_oracle_bubble import FreeLevels
+    O = oracle
+    nt, ntau, beta, h = 100, 500, 5.0, 0.01
+    a = np.sqrt(2.0) * np.array([[1.0, -1j], [1j, -1.0]]) + shift * np.eye(2)
+    w, V = np.linalg.eigh(a)
+    exact = FreeLevels(w, sig, beta, V.conj().T).herm_matrix(nt, ntau, h)
+    G = herm_matrix(nt, ntau, 2, sig)
+    O.green_from_H(G, 0.0, a, beta, h)
+    err = sum(O.distance_norm2(t, G, exact) for t in range(-1, nt))
+    assert err < 1e-6, err                 # equilibrium.cpp:244 (eps)
