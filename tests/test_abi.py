@@ -33,3 +33,15 @@ def test_no_device_fails_loudly():
     from nessi_b200 import gpu
     with pytest.raises(gpu.NessiGpuError):
         gpu.init(0)
+
+
+def test_io_library_exports_all_declared_symbols():
+    from nessi_b200 import build, hm_file
+    build.build_io()
+    text = open(os.path.join(ROOT, "include", "nessi_io.h")).read()
+    syms = sorted(set(re.findall(r"\b(nessi_(?:hm|io)_\w+)\s*\(", text)))
+    assert len(syms) == 5
+    L = hm_file.load_library()
+    for s in syms:
+        assert hasattr(L, s), s
+        assert s in hm_file.EXPORTS, s
