@@ -22,11 +22,30 @@
 #include <vector>
 
 #include "nessi_gpu.h"
+#include "nessi_io.h"
 
 namespace cntr_gpu {
 
 inline void check(int rc) {
     if (rc != NESSI_OK) throw std::runtime_error(std::string("libnessi_gpu: ") + nessi_gpu_last_error());
+}
+
+inline void check_io(int rc) {
+    if (rc != 0) throw std::runtime_error(std::string("libnessi_io: ") + nessi_io_last_error());
+}
+
+// G.print_to_file(file, precision) and G.read_from_file(nt1, file) of libcntr
+// (cntr_herm_matrix_impl.hpp:1308-1560) through libnessi_io.so (link -lnessi_io); the files are
+// libcntr's text format.  Precision 17 makes the round trip exact.
+template <class HM> void print_to_file(HM &G, const char *file, int precision = 16) {
+    check_io(nessi_hm_print_to_file(file, G.nt(), G.ntau(), G.size1(), G.sig(), G.nt() >= 0 ? G.retptr(0, 0) : nullptr,
+                                    G.nt() >= 0 ? G.lesptr(0, 0) : nullptr, G.nt() >= 0 ? G.tvptr(0, 0) : nullptr,
+                                    G.matptr(0), precision));
+}
+template <class HM> void read_from_file(HM &G, int nt1, const char *file) {
+    check_io(nessi_hm_read_from_file_nt1(file, nt1, G.nt(), G.ntau(), G.size1(),
+                                         G.nt() >= 0 ? G.retptr(0, 0) : nullptr, G.nt() >= 0 ? G.lesptr(0, 0) : nullptr,
+                                         G.nt() >= 0 ? G.tvptr(0, 0) : nullptr, G.matptr(0)));
 }
 
 // number of complex<double> in one herm_matrix_timestep slice [ret | tv | les] (n >= 0)
@@ -109,10 +128,26 @@ template <class HM, class FN> class Batch {
         std::copy(s.begin() + (n1 + M) * es, s.end(), G.lesptr(0, n));
     }
     void download_all() {
-        for (size_t p = 0; p < G_.size(); p++) {
-            HM &G = *G_[p];
-            check(nessi_gpu_get_G(b_, (int)p, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0)));
-        }
+        for (size_t p = 0; p < G_.size(); p++) download(p);
+    }
+    // all components of problem p: device -> its herm_matrix, and back
+    void download(size_t p) {
+        HM &G = *G_[p];
+        check(nessi_gpu_get_G(b_, (int)p, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0)));
+    }
+    void upload(size_t p) {
+        HM &G = *G_[p];
+        check(nessi_gpu_set_G(b_, (int)p, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0)));
+    }
+    // checkpoint problem p in libcntr's text format; restart it from time steps 0..nt1 of such a
+    // file (the propagation continues with nt1 + 1)
+    void checkpoint(size_t p, const char *file, int precision = 17) {
+        download(p);
+        print_to_file(*G_[p], file, precision);
+    }
+    void restart(size_t p, int nt1, const char *file) {
+        read_from_file(*G_[p], nt1, file);
+        upload(p);
     }
     nessi_batch *handle() { return b_; }
 

@@ -7,6 +7,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 MOCK = r'''
 #include <complex>
+#include <string>
 #include <vector>
 #include "cntr_gpu.hpp"
 typedef std::complex<double> cplx;
@@ -31,6 +32,28 @@ struct FN {
     cplx *ptr(int t) { return d_.data() + (long)(t + 1) * s_ * s_; }
 };
 int main(int argc, char **argv) {
+    if (argc == 2 && std::string(argv[1]) == "io") {  // text checkpoint round trip, no GPU needed
+        HM A(7, 5, 2, 1), B(9, 5, 2, 1);
+        for (size_t i = 0; i < A.t_.size(); i++) A.t_[i] = cplx(0.1 * i, -1.0 / (i + 1));
+        for (size_t i = 0; i < A.r_.size(); i++) { A.r_[i] = cplx(i, 2.0 / 3); A.l_[i] = cplx(-1.0 / 7, i); }
+        for (size_t i = 0; i < A.m_.size(); i++) A.m_[i] = cplx(1e-300 * i, 3.0);
+        cntr_gpu::print_to_file(A, "ckpt.txt", 17);
+        cntr_gpu::read_from_file(B, 4, "ckpt.txt");
+        for (int t = 0; t <= 4; t++)
+            for (int j = 0; j <= 5; j++)
+                for (int e = 0; e < 4; e++)
+                    if (B.tvptr(t, j)[e] != A.tvptr(t, j)[e]) return 3;
+        for (int j = 0; j <= 4; j++)
+            for (int e = 0; e < 4; e++)
+                if (B.retptr(4, j)[e] != A.retptr(4, j)[e] || B.lesptr(j, 4)[e] != A.lesptr(j, 4)[e]) return 4;
+        if (B.tvptr(5, 0)[0] != cplx(0, 0)) return 5;  // steps after nt1 untouched
+        try {
+            cntr_gpu::read_from_file(B, 8, "ckpt.txt");  // nt1 beyond the file
+            return 6;
+        } catch (const std::runtime_error &) {
+        }
+        return 0;
+    }
     if (argc < 2) return 0;  // link check only
     HM G(12, 10, 2, -1), S(12, 10, 2, -1);
     FN H(12, 2);
@@ -54,6 +77,9 @@ def test_cntr_gpu_header_compiles_and_links(tmp_path):
     exe = tmp_path / "mock"
     libdir = os.path.join(ROOT, "nessi_b200")
     cmd = ["/usr/bin/g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
-           "-L", libdir, "-lnessi_gpu", "-Wl,-rpath," + libdir]
+           "-L", libdir, "-lnessi_gpu", "-lnessi_io", "-Wl,-rpath," + libdir]
     subprocess.check_call(cmd)
     assert exe.exists()
+    # the checkpoint functions of the front end run without a GPU
+    assert subprocess.call([str(exe), "io"], cwd=tmp_path) == 0
+    assert (tmp_path / "ckpt.txt").read_text().startswith("# 7 5 2  1\n")
