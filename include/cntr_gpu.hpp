@@ -227,17 +227,31 @@ void vie2_timestep(int n, HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, i
     std::copy(s.begin() + (n1 + M) * es, s.end(), G.lesptr(0, n));
 }
 
-// ---- convolution_timestep (cntr_convolution_decl.hpp:61) --------------------------------
+// ---- convolution_timestep / convolution (cntr_convolution_decl.hpp:59-68) ----------------
+template <class HM> inline nessi_hm_ptrs hm_ptrs(HM &X) {
+    nessi_hm_ptrs q;
+    q.ret = X.retptr(0, 0); q.les = X.lesptr(0, 0); q.tv = X.tvptr(0, 0); q.mat = X.matptr(0);
+    return q;
+}
 template <class HM>
 void convolution_timestep(int n, HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta, double h, int SolveOrder = 5) {
-    auto p = [](HM &X) {
-        nessi_hm_ptrs q;
-        q.ret = X.retptr(0, 0); q.les = X.lesptr(0, 0); q.tv = X.tvptr(0, 0); q.mat = X.matptr(0);
-        return q;
-    };
-    nessi_hm_ptrs c = p(C), a = p(A), acc = p(Acc), b = p(B), bcc = p(Bcc);
+    nessi_hm_ptrs c = hm_ptrs(C), a = hm_ptrs(A), acc = hm_ptrs(Acc), b = hm_ptrs(B), bcc = hm_ptrs(Bcc);
     check(nessi_gpu_convolution_timestep_host(n, &c, &a, &acc, &b, &bcc, C.nt(), C.ntau(), C.size1(), A.sig(), B.sig(),
                                               SolveOrder, beta, h));
+}
+// hermitian A and B (:64-65): Acc = A, Bcc = B
+template <class HM> void convolution_timestep(int n, HM &C, HM &A, HM &B, double beta, double h, int SolveOrder = 5) {
+    convolution_timestep(n, C, A, A, B, B, beta, h, SolveOrder);
+}
+// every time step, convolution_matsubara then n = 0..nt (:66-68, cntr_convolution_impl.hpp:1805-1812)
+template <class HM>
+void convolution(HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta, double h, int SolveOrder = 5) {
+    nessi_hm_ptrs c = hm_ptrs(C), a = hm_ptrs(A), acc = hm_ptrs(Acc), b = hm_ptrs(B), bcc = hm_ptrs(Bcc);
+    check(nessi_gpu_convolution_host(&c, &a, &acc, &b, &bcc, C.nt(), C.ntau(), C.size1(), A.sig(), B.sig(), SolveOrder,
+                                     beta, h));
+}
+template <class HM> void convolution(HM &C, HM &A, HM &B, double beta, double h, int SolveOrder = 5) {
+    convolution(C, A, A, B, B, beta, h, SolveOrder);
 }
 
 }  // namespace cntr_gpu

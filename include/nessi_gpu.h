@@ -222,6 +222,14 @@ int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nes
                                         int nt, int ntau, int size1, int sig_a, int sig_b, int solve_order,
                                         double beta, double h);
 
+/* cntr::convolution(C, A, Acc, B, Bcc, beta, h, SolveOrder) (cntr_convolution_decl.hpp:66-68,
+ * cntr_convolution_impl.hpp:1805-1812, 3170-3177 without ft): C = A * B at every time step,
+ * convolution_matsubara then n = 0..nt, on HOST herm_matrix data.  The operands are copied to the
+ * device once, all steps run there, and all of C comes back. */
+int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc,
+                               const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1,
+                               int sig_a, int sig_b, int solve_order, double beta, double h);
+
 /* Volterra kernels in use for a group: -1 = one problem per CTA, 2/4/8 = problems per CTA of the
  * tensor-core kernels, 0 = not chosen yet (the autotuner decides at the first eager step with
  * n >= min(128, nt); the environment variable NESSI_VOLTERRA_PP read at batch creation fixes

@@ -1506,12 +1506,14 @@ extern "C" int nessi_gpu_convolution_timestep(int n, int count, const nessi_hm_p
 
 // Host-data convenience for single calls with libcntr's signature: copies the five herm_matrix
 // objects to the device, runs the convolution for time step n and copies C's time step back.
-extern "C" int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
-                                                   const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B,
-                                                   const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a,
-                                                   int sig_b, int solve_order, double beta, double h) {
+// time steps n0..n1 of C = A * B on host herm_matrix data: upload the operands once, run the
+// steps on the device, bring back C's steps n0..n1 (all of C when the range is -1..nt)
+static int convolution_host_range(int n0, int n1, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                  const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt,
+                                  int ntau, int size1, int sig_a, int sig_b, int solve_order, double beta, double h,
+                                  const char *name) {
     if (!C || !A || !Acc || !B || !Bcc || nt < 0 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS) {
-        set_err("convolution_timestep_host: bad arguments");
+        set_err("%s: bad arguments", name);
         return NESSI_ERR_ARG;
     }
     CK(cudaSetDevice(g_device));
@@ -1536,24 +1538,43 @@ extern "C" int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C
             }
         }
     }
-    if (rc == NESSI_OK)
+    for (int n = n0; n <= n1 && rc == NESSI_OK; n++)
         rc = nessi_gpu_convolution_timestep(n, 1, &ds[0], &ds[1], &ds[2], &ds[3], &ds[4], nt, ntau, size1, sig_a, sig_b,
                                             solve_order, beta, h, nullptr);
     if (rc == NESSI_OK && cudaDeviceSynchronize() != cudaSuccess) { set_err("convolution failed"); rc = NESSI_ERR_CUDA; }
     if (rc == NESSI_OK) {
-        // C's time step n: ret row, tv row, les column (or mat)
-        auto back = [&](void *h, const void *d, long off, long cnt) {
-            return cudaMemcpy((char *)h + off * 16, (const char *)d + off * 16, (size_t)cnt * 16, cudaMemcpyDeviceToHost);
+        // C's time steps n0..n1: ret rows, tv rows, les columns (and mat for n0 = -1)
+        auto back = [&](void *hp, const void *d, long off, long cnt) {
+            if (!hp || !d) return cudaSuccess;
+            return cudaMemcpy((char *)hp + off * 16, (const char *)d + off * 16, (size_t)cnt * 16, cudaMemcpyDeviceToHost);
         };
         cudaError_t e = cudaSuccess;
-        if (n < 0) e = back(C->mat, ds[0].mat, 0, M * s2);
-        else {
-            e = back(C->ret, ds[0].ret, tri_h(n) * s2, (n + 1) * s2);
-            if (e == cudaSuccess) e = back(C->tv, ds[0].tv, (long)n * M * s2, M * s2);
-            if (e == cudaSuccess) e = back(C->les, ds[0].les, tri_h(n) * s2, (n + 1) * s2);
+        if (n0 < 0) e = back(C->mat, ds[0].mat, 0, M * s2);
+        const int t0 = n0 < 0 ? 0 : n0;
+        if (n1 >= t0 && e == cudaSuccess) {
+            // rows / columns t0..n1 are contiguous in the packed triangles and in tv
+            e = back(C->ret, ds[0].ret, tri_h(t0) * s2, (tri_h(n1 + 1) - tri_h(t0)) * s2);
+            if (e == cudaSuccess) e = back(C->tv, ds[0].tv, (long)t0 * M * s2, (long)(n1 - t0 + 1) * M * s2);
+            if (e == cudaSuccess) e = back(C->les, ds[0].les, tri_h(t0) * s2, (tri_h(n1 + 1) - tri_h(t0)) * s2);
         }
         if (e != cudaSuccess) { set_err("download failed"); rc = NESSI_ERR_CUDA; }
     }
     for (void *q : owned) cudaFree(q);
     return rc;
+}
+
+extern "C" int nessi_gpu_convolution_timestep_host(int n, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                                   const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B,
+                                                   const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a,
+                                                   int sig_b, int solve_order, double beta, double h) {
+    if (n < -1 || n > nt) { set_err("convolution_timestep_host: time step %d out of range", n); return NESSI_ERR_ARG; }
+    return convolution_host_range(n, n, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h,
+                                  "convolution_timestep_host");
+}
+
+extern "C" int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc,
+                                          const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1,
+                                          int sig_a, int sig_b, int solve_order, double beta, double h) {
+    return convolution_host_range(-1, nt, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h,
+                                  "convolution_host");
 }

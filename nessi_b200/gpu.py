@@ -87,6 +87,8 @@ EXPORTS = {
                                        [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     "nessi_gpu_convolution_timestep_host": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 5 +
                                             [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_convolution_host": (ctypes.c_int, [ctypes.POINTER(HmPtrs)] * 5 + [ctypes.c_int] * 6 +
+                                   [ctypes.c_double, ctypes.c_double]),
     "nessi_gpu_get_volterra_choice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                      ctypes.POINTER(ctypes.c_int)]),
     "nessi_gpu_graph_record": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 4),
@@ -366,6 +368,19 @@ def convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder=5):
         return ctypes.byref(HmPtrs(_ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
     _check(load_library().nessi_gpu_convolution_timestep_host(n, hp(C), hp(A), hp(Acc), hp(B), hp(Bcc), C.nt, C.ntau,
                                                               C.size1, A.sig, B.sig, SolveOrder, beta, h))
+
+
+def convolution(C, A, Acc, B, Bcc, beta, h, SolveOrder=5):
+    """cntr::convolution(C, A, Acc, B, Bcc, beta, h, SolveOrder) (cntr_convolution_decl.hpp:66-68):
+    C = A * B at every time step, -1..nt; the operands are copied to the device once.  For
+    hermitian operands pass A as Acc and B as Bcc (the reference's short form)."""
+    if not _inited:
+        init(0)
+
+    def hp(G):
+        return ctypes.byref(HmPtrs(_ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
+    _check(load_library().nessi_gpu_convolution_host(hp(C), hp(A), hp(Acc), hp(B), hp(Bcc), C.nt, C.ntau, C.size1,
+                                                     A.sig, B.sig, SolveOrder, beta, h))
 
 
 def dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder=5):

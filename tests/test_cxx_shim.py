@@ -64,6 +64,9 @@ int main(int argc, char **argv) {
     cntr_gpu::vie2_start(G, F, F, Q, 5.0, 0.05, 5);
     cntr_gpu::vie2_timestep(6, G, F, F, Q, 5.0, 0.05, 5);
     cntr_gpu::convolution_timestep(6, C, G, G, S, S, 5.0, 0.05, 5);
+    cntr_gpu::convolution_timestep(6, C, G, S, 5.0, 0.05, 5);
+    cntr_gpu::convolution(C, G, G, S, S, 5.0, 0.05, 5);
+    cntr_gpu::convolution(C, G, S, 5.0, 0.05);
     return 0;
 }
 '''
