@@ -53,6 +53,10 @@ typedef struct {
 
 /* Select the CUDA device used by later batches; replaces nothing (libcntr is CPU-only). */
 int nessi_gpu_init(int device);
+/* End of use: NESSI_ERR_ARG while batches are alive; otherwise waits for the devices used and
+ * forgets the per-device state (the next init or batch_create sets it up again).  The CUDA
+ * context is left alone, so a host program that also uses the device keeps it. */
+int nessi_gpu_finalize(void);
 const char *nessi_gpu_last_error(void);
 
 /* Allocate device storage for `count` problems.  precision is NESSI_PREC_*. */

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -24,6 +25,7 @@ namespace {
 
 thread_local std::string g_err;
 int g_device = 0;
+std::atomic<int> g_live_batches{0};  // created and not yet destroyed
 std::vector<int> g_tables_ready;  // devices whose c_tab was filled
 
 void set_err(const char *fmt, ...) {
@@ -585,6 +587,7 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
     CK(cudaSetDevice(g_device));
     CKR(ensure_tables(g_device));
     nessi_batch *b = new nessi_batch();
+    g_live_batches++;
     b->device = g_device;
     b->precision = precision;
     if (const char *v = getenv("NESSI_VOLTERRA_PP")) {
@@ -722,6 +725,20 @@ int nessi_gpu_batch_destroy(nessi_batch *b) {
     if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
+    g_live_batches--;
+    return NESSI_OK;
+}
+
+int nessi_gpu_finalize(void) {
+    if (g_live_batches.load() != 0) {
+        set_err("finalize: %d batches are still alive", g_live_batches.load());
+        return NESSI_ERR_ARG;
+    }
+    for (int dev : g_tables_ready) {
+        CK(cudaSetDevice(dev));
+        CK(cudaDeviceSynchronize());
+    }
+    g_tables_ready.clear();  // the next init or batch uploads the integration tables again
     return NESSI_OK;
 }
 

@@ -46,6 +46,7 @@ class HmPtrs(ctypes.Structure):
 EXPORTS = {
     "nessi_gpu_init": (ctypes.c_int, [ctypes.c_int]),
     "nessi_gpu_last_error": (ctypes.c_char_p, []),
+    "nessi_gpu_finalize": (ctypes.c_int, []),
     "nessi_gpu_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ProblemDesc),
                                               ctypes.c_int, ctypes.c_int]),
     "nessi_gpu_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -127,6 +128,13 @@ def init(device=0):
     L = load_library()
     _check(L.nessi_gpu_init(device))
     _inited = True
+
+
+def finalize():
+    """nessi_gpu_finalize: every batch must be closed first."""
+    global _inited
+    _check(load_library().nessi_gpu_finalize())
+    _inited = False
 
 
 def _ptr(a):

@@ -45,3 +45,8 @@ def test_io_library_exports_all_declared_symbols():
     for s in syms:
         assert hasattr(L, s), s
         assert s in hm_file.EXPORTS, s
+
+
+def test_finalize_without_batches_needs_no_device():
+    from nessi_b200 import gpu
+    gpu.finalize()   # nothing was set up: returns at once, on a machine without a GPU too
