@@ -187,44 +187,118 @@ void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder =
     b.download_timestep(0, -1);
 }
 
-// ---- VIE2 single-problem drop-ins (cntr_vie2_decl.hpp:67-72) --------------------------------
-template <class HM>
-void vie2_start(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5) {
+// Matsubara methods of libcntr (cntr_global_settings.hpp): the device solves by the default one
+constexpr int MAT_FIXPOINT = 2;
+inline void require_fixpoint(int method, bool force_hermitian = true) {
+    if (method != MAT_FIXPOINT || !force_hermitian)
+        throw std::invalid_argument("cntr_gpu: only the default Matsubara solve (CNTR_MAT_FIXPOINT, force_hermitian) "
+                                    "runs on the device");
+}
+
+// cntr::dyson(G, mu, H, Sigma, beta, h, SolveOrder, matsubara_method, force_hermitian)
+// (cntr_dyson_decl.hpp:95-98, cntr_dyson_impl.hpp:1725-1734): dyson_mat, dyson_start and every
+// time step k+1..nt on the device from one upload, then all of G comes back.  G.nt() >= 0.
+template <class HM, class FN>
+void dyson(HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveOrder = 5,
+           int matsubara_method = MAT_FIXPOINT, bool force_hermitian = true) {
+    require_fixpoint(matsubara_method, force_hermitian);
+    Batch<HM, FN> b;
+    b.add(G, H, mu, beta, h, SolveOrder);
+    b.build(Sigma);
+    b.dyson_mat();
+    b.dyson_start();
+    for (int n = SolveOrder + 1; n <= G.nt(); n++) b.dyson_timestep(n);
+    b.download_all();
+}
+
+// ---- VIE2 single-problem drop-ins (cntr_vie2_decl.hpp:63-90) --------------------------------
+// one-problem VIE2 batch of order k holding F, Fcc, Q and (optionally all of) G
+template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int k, bool whole_G) {
     nessi_problem_desc d;
     d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
-    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = h; d.mu = 0.0;
+    d.solve_order = k; d.sigma_group = 0; d.beta = beta; d.h = h; d.mu = 0.0;
     nessi_batch *b = nullptr;
     check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
-    int rc = nessi_gpu_set_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
+    int rc = whole_G ? nessi_gpu_set_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0))
+                     : nessi_gpu_set_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
     if (!rc) rc = nessi_gpu_set_F(b, 0, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0), Fcc.retptr(0, 0),
                                   Fcc.lesptr(0, 0));
     if (!rc) rc = nessi_gpu_set_Q(b, 0, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0));
-    if (!rc) rc = nessi_gpu_vie2_start(b);
-    if (!rc) rc = nessi_gpu_get_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), nullptr);
+    if (rc) {
+        nessi_gpu_batch_destroy(b);
+        check(rc);
+    }
+    return b;
+}
+
+// cntr::vie2_mat(G, F, Fcc, Q, beta, SolveOrder, method) (cntr_vie2_decl.hpp:63): G^mat
+template <class HM>
+void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT) {
+    require_fixpoint(method);
+    nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, 1.0, SolveOrder, false);
+    int rc = nessi_gpu_vie2_mat(b);
+    if (!rc) rc = nessi_gpu_get_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
     nessi_gpu_batch_destroy(b);
     check(rc);
 }
 
+// cntr::vie2(G, F, Fcc, Q, beta, h, SolveOrder, matsubara_method) (cntr_vie2_decl.hpp:85-86):
+// vie2_mat, vie2_start and every time step on the device from one upload.
 template <class HM>
-void vie2_timestep(int n, HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5) {
-    nessi_problem_desc d;
-    d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
-    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = h; d.mu = 0.0;
-    nessi_batch *b = nullptr;
-    check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
-    int rc = nessi_gpu_set_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0));
-    if (!rc) rc = nessi_gpu_set_F(b, 0, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0), Fcc.retptr(0, 0),
-                                  Fcc.lesptr(0, 0));
-    if (!rc) rc = nessi_gpu_set_Q(b, 0, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0));
-    if (!rc) rc = nessi_gpu_vie2_timestep(b, n);
-    std::vector<std::complex<double>> s(slice_len(G, n));
-    if (!rc) rc = nessi_gpu_get_timestep(b, 0, n, s.data());
+void vie2(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5, int matsubara_method = MAT_FIXPOINT) {
+    require_fixpoint(matsubara_method);
+    nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, h, SolveOrder, false);
+    int rc = nessi_gpu_vie2_mat(b);
+    if (!rc) rc = nessi_gpu_vie2_start(b);
+    for (int n = SolveOrder + 1; n <= G.nt() && !rc; n++) rc = nessi_gpu_vie2_timestep(b, n);
+    if (!rc) rc = nessi_gpu_get_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0));
     nessi_gpu_batch_destroy(b);
     check(rc);
+}
+
+// copy time step n (n >= 0) of problem 0 of a batch into G
+template <class HM> int fetch_timestep(nessi_batch *b, HM &G, int n) {
+    std::vector<std::complex<double>> s(slice_len(G, n));
+    int rc = nessi_gpu_get_timestep(b, 0, n, s.data());
+    if (rc) return rc;
     const long es = (long)G.size1() * G.size1(), n1 = n + 1, M = G.ntau() + 1;
     std::copy(s.begin(), s.begin() + n1 * es, G.retptr(n, 0));
     std::copy(s.begin() + n1 * es, s.begin() + (n1 + M) * es, G.tvptr(n, 0));
     std::copy(s.begin() + (n1 + M) * es, s.end(), G.lesptr(0, n));
+    return NESSI_OK;
+}
+
+// cntr::vie2_start(G, F, Fcc, Q, beta, h, SolveOrder) (cntr_vie2_decl.hpp:67): time steps 0..k
+template <class HM>
+void vie2_start(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5) {
+    nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, h, SolveOrder, false);
+    int rc = nessi_gpu_vie2_start(b);
+    for (int n = 0; n <= SolveOrder && !rc; n++) rc = fetch_timestep(b, G, n);
+    nessi_gpu_batch_destroy(b);
+    check(rc);
+}
+
+// cntr::vie2_timestep(n, G, F, Fcc, Q, beta, h, SolveOrder, matsubara_method)
+// (cntr_vie2_decl.hpp:72, cntr_vie2_impl.hpp:1597-1640): n = -1 gives vie2_mat and
+// 1 <= n <= SolveOrder a vie2_start of order n (time steps 0..n), as the reference dispatches;
+// n = 0, an order-0 start, is not available
+template <class HM>
+void vie2_timestep(int n, HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5,
+                   int matsubara_method = MAT_FIXPOINT) {
+    if (n == -1) {
+        vie2_mat(G, F, Fcc, Q, beta, SolveOrder, matsubara_method);
+        return;
+    }
+    if (n <= SolveOrder) {
+        if (n == 0) throw std::invalid_argument("cntr_gpu::vie2_timestep: an order-0 start (n = 0) is not available");
+        vie2_start(G, F, Fcc, Q, beta, h, n);
+        return;
+    }
+    nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, h, SolveOrder, true);
+    int rc = nessi_gpu_vie2_timestep(b, n);
+    if (!rc) rc = fetch_timestep(b, G, n);
+    nessi_gpu_batch_destroy(b);
+    check(rc);
 }
 
 // ---- convolution_timestep / convolution (cntr_convolution_decl.hpp:59-68) ----------------

@@ -63,6 +63,11 @@ int main(int argc, char **argv) {
     HM F(12, 10, 2, -1), Q(12, 10, 2, -1), C(12, 10, 2, -1);
     cntr_gpu::vie2_start(G, F, F, Q, 5.0, 0.05, 5);
     cntr_gpu::vie2_timestep(6, G, F, F, Q, 5.0, 0.05, 5);
+    cntr_gpu::vie2_timestep(-1, G, F, F, Q, 5.0, 0.05, 5);
+    cntr_gpu::vie2_timestep(3, G, F, F, Q, 5.0, 0.05);
+    cntr_gpu::vie2_mat(G, F, F, Q, 5.0, 5);
+    cntr_gpu::vie2(G, F, F, Q, 5.0, 0.05, 5);
+    cntr_gpu::dyson(G, 0.0, H, S, 5.0, 0.05, 5);
     cntr_gpu::convolution_timestep(6, C, G, G, S, S, 5.0, 0.05, 5);
     cntr_gpu::convolution_timestep(6, C, G, S, 5.0, 0.05, 5);
     cntr_gpu::convolution(C, G, G, S, S, 5.0, 0.05, 5);
