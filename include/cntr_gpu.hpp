@@ -211,6 +211,28 @@ void dyson(HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveO
     b.download_all();
 }
 
+// cntr::extrapolate_timestep(n, G, SolveOrder) (cntr_utilities_decl.hpp:23,
+// cntr_utilities_impl.hpp:22-130): time step n+1 of G predicted from n-k..n; n >= SolveOrder
+template <class HM> void extrapolate_timestep(int n, HM &G, int SolveOrder = 5) {
+    if (n + 1 > G.nt() || n < SolveOrder)  // where libcntr aborts (cntr_utilities_impl.hpp:35-39)
+        throw std::invalid_argument("cntr_gpu::extrapolate_timestep: n out of range");
+    nessi_problem_desc d;
+    d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = 1.0; d.h = 1.0; d.mu = 0.0;
+    nessi_batch *b = nullptr;
+    check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
+    int rc = nessi_gpu_set_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0));
+    if (!rc) rc = nessi_gpu_extrapolate_timestep(b, n);
+    std::vector<std::complex<double>> s(slice_len(G, n + 1));
+    if (!rc) rc = nessi_gpu_get_timestep(b, 0, n + 1, s.data());
+    nessi_gpu_batch_destroy(b);
+    check(rc);
+    const long es = (long)G.size1() * G.size1(), n1 = n + 2, M = G.ntau() + 1;
+    std::copy(s.begin(), s.begin() + n1 * es, G.retptr(n + 1, 0));
+    std::copy(s.begin() + n1 * es, s.begin() + (n1 + M) * es, G.tvptr(n + 1, 0));
+    std::copy(s.begin() + (n1 + M) * es, s.end(), G.lesptr(0, n + 1));
+}
+
 // ---- VIE2 single-problem drop-ins (cntr_vie2_decl.hpp:63-90) --------------------------------
 // one-problem VIE2 batch of order k holding F, Fcc, Q and (optionally all of) G
 template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int k, bool whole_G) {

@@ -68,6 +68,7 @@ int main(int argc, char **argv) {
     cntr_gpu::vie2_mat(G, F, F, Q, 5.0, 5);
     cntr_gpu::vie2(G, F, F, Q, 5.0, 0.05, 5);
     cntr_gpu::dyson(G, 0.0, H, S, 5.0, 0.05, 5);
+    cntr_gpu::extrapolate_timestep(7, G, 5);
     cntr_gpu::convolution_timestep(6, C, G, G, S, S, 5.0, 0.05, 5);
     cntr_gpu::convolution_timestep(6, C, G, S, 5.0, 0.05, 5);
     cntr_gpu::convolution(C, G, G, S, S, 5.0, 0.05, 5);
