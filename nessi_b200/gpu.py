@@ -404,3 +404,38 @@ def dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder=5):
     b.get_timestep(0, n, slc)
     G.set_timestep_data(n, slc)
     b.close()
+
+
+def dyson(G, mu, H, Sigma, beta, h, SolveOrder=5):
+    """cntr::dyson(G, mu, H, Sigma, beta, h, SolveOrder) (cntr_dyson_decl.hpp:95-98,
+    cntr_dyson_impl.hpp:1725-1734): dyson_mat (fixpoint), dyson_start and every time step on the
+    GPU from one upload; all of G is written."""
+    b = Batch([dict(nt=G.nt, ntau=G.ntau, size1=G.size1, sig=G.sig, solve_order=SolveOrder, beta=beta, h=h,
+                    mu=mu)])
+    try:
+        b.set_G(0, G)
+        b.set_H(0, H)
+        b.set_sigma(0, Sigma)
+        b.dyson_mat()
+        b.dyson_start()
+        for n in range(SolveOrder + 1, G.nt + 1):
+            b.dyson_timestep(n)
+        b.get_G(0, G)
+    finally:
+        b.close()
+
+
+def vie2(G, F, Fcc, Q, beta, h, SolveOrder=5):
+    """cntr::vie2(G, F, Fcc, Q, beta, h, SolveOrder) (cntr_vie2_decl.hpp:85-86): [1 + F] G = Q by
+    vie2_mat (fixpoint), vie2_start and every time step on the GPU from one upload."""
+    b = Batch([dict(nt=G.nt, ntau=G.ntau, size1=G.size1, sig=G.sig, solve_order=SolveOrder, beta=beta, h=h)])
+    try:
+        b.set_F(0, F, Fcc)
+        b.set_Q(0, Q)
+        b.vie2_mat()
+        b.vie2_start()
+        for n in range(SolveOrder + 1, G.nt + 1):
+            b.vie2_timestep(n)
+        b.get_G(0, G)
+    finally:
+        b.close()

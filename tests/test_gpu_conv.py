@@ -128,18 +128,3 @@ def test_convolution_host_dropin(oracle):
     for comp in ("ret", "les", "tv", "mat"):
         assert rel_err(getattr(C, comp), getattr(R, comp)) < TOL, comp
 
-
-def test_whole_convolution(oracle):
-    """gpu.convolution (cntr::convolution, every time step from one upload) against the oracle's
-    convolution_timestep at n = -1..nt, for a non-hermitian A with its partner Acc."""
-    from nessi_b200 import gpu
-    rng = np.random.default_rng(11)
-    nt, ntau, beta, h, k, s = 12, 10, 2.0, 0.05, 5, 2
-    A, Acc = _pair(oracle, rng, nt, ntau, s, -1, beta, h, k)
-    B = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.8)
-    C, R = herm_matrix(nt, ntau, s, -1), herm_matrix(nt, ntau, s, -1)
-    gpu.convolution(C, A, Acc, B, B, beta, h, k)
-    for n in range(-1, nt + 1):
-        oracle.convolution_timestep(n, R, A, Acc, B, B, beta, h, k)
-    for comp in ("ret", "les", "tv", "mat"):
-        assert rel_err(getattr(C, comp), getattr(R, comp)) < TOL, comp
