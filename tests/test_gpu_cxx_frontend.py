@@ -1,0 +1,122 @@
+"""include/cntr_gpu.hpp used as a libcntr program uses it, on the GPU: tests/cxx_frontend.cpp holds
+a herm_matrix / function pair with libcntr's accessors and layout and calls cntr_gpu::dyson,
+the single-call dyson_mat / dyson_start / dyson_timestep loop, vie2_timestep (n = -1, then
+n > k) with vie2_start, and cntr_gpu::convolution; the results are checked against the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from nessi_b200 import herm_matrix
+from builders import component_errors, make_H, make_sigma, rel_err, solve_oracle
+from test_gpu_conv import _pair
+from test_gpu_vie2 import _kernel_pair, _oracle_vie2, _source
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HERE = os.path.join(ROOT, "tests")
+TOL = 1e-10
+
+
+def build_frontend(tmp_path):
+    from nessi_b200 import build
+    build.build()
+    exe = tmp_path / "cxx_frontend"
+    libdir = os.path.join(ROOT, "nessi_b200")
+    subprocess.check_call(["/usr/bin/g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(HERE, "cxx_frontend.cpp"), "-o", str(exe), "-L", libdir, "-lnessi_gpu",
+                           "-lnessi_io", "-Wl,-rpath," + libdir])
+    return exe
+
+
+def write_case(d, dims, **hms):
+    d.mkdir(parents=True, exist_ok=True)
+    (d / "dims.txt").write_text(" ".join(str(x) for x in dims) + "\n")
+    for name, G in hms.items():
+        if isinstance(G, np.ndarray):
+            np.ascontiguousarray(G, np.complex128).tofile(str(d / (name + ".fn")))
+            continue
+        for c in ("ret", "les", "tv", "mat"):
+            np.ascontiguousarray(getattr(G, c)).tofile(str(d / ("%s.%s" % (name, c))))
+
+
+def read_out(d, nt, ntau, s, sig):
+    G = herm_matrix(nt, ntau, s, sig)
+    for c in ("ret", "les", "tv", "mat"):
+        a = getattr(G, c)
+        a[...] = np.fromfile(str(d / ("out." + c)), np.complex128).reshape(a.shape)
+    return G
+
+
+def run(exe, mode, d):
+    r = subprocess.run([str(exe), mode, str(d)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+
+
+def test_file_handling_without_device(tmp_path):
+    """The program's own file round trip (mode echo), which needs no GPU."""
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(1)
+    A = herm_matrix(6, 5, 2, -1)
+    for c in ("ret", "les", "tv", "mat"):
+        a = getattr(A, c)
+        a[...] = rng.normal(size=a.shape) + 1j * rng.normal(size=a.shape)
+    d = tmp_path / "echo"
+    write_case(d, (6, 5, 2, -1, 5, 1.0, 0.1, 0.0), A=A)
+    run(exe, "echo", d)
+    B = read_out(d, 6, 5, 2, -1)
+    for c in ("ret", "les", "tv", "mat"):
+        assert np.array_equal(getattr(A, c), getattr(B, c))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["dyson", "steps"])
+def test_dyson_through_the_cxx_frontend(oracle, tmp_path, mode):
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(41)
+    nt, ntau, s, beta, h, k, mu = 20, 16, 2, 3.0, 0.05, 5, 0.1
+    Sig = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h)
+    H = make_H(rng, nt, s, h)
+    ref, _ = solve_oracle(oracle, herm_matrix(nt, ntau, s, -1), H, Sig, mu, beta, h, k)
+    d = tmp_path / mode
+    write_case(d, (nt, ntau, s, -1, k, beta, h, mu), Sigma=Sig, H=getattr(H, "data", H))
+    run(exe, mode, d)
+    G = read_out(d, nt, ntau, s, -1)
+    assert rel_err(G.mat, ref.mat) < TOL
+    e = component_errors(G, ref, 0, nt)
+    assert max(e.values()) < TOL, e
+
+
+@pytest.mark.gpu
+def test_vie2_through_the_cxx_frontend(oracle, tmp_path):
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(43)
+    nt, ntau, s, beta, h, k = 20, 16, 2, 4.0, 0.05, 5
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Q = _source(oracle, rng, nt, ntau, s, beta, h)
+    ref, _ = _oracle_vie2(oracle, F, Fcc, Q, beta, h, k)
+    d = tmp_path / "vie2"
+    write_case(d, (nt, ntau, s, -1, k, beta, h, 0.0), F=F, Fcc=Fcc, Q=Q)
+    run(exe, "vie2", d)
+    G = read_out(d, nt, ntau, s, -1)
+    assert rel_err(G.mat, ref.mat) < TOL
+    e = component_errors(G, ref, 0, nt)
+    assert max(e.values()) < TOL, e
+
+
+@pytest.mark.gpu
+def test_convolution_through_the_cxx_frontend(oracle, tmp_path):
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(47)
+    nt, ntau, s, beta, h, k = 12, 10, 2, 2.0, 0.05, 5
+    A, Acc = _pair(oracle, rng, nt, ntau, s, -1, beta, h, k)
+    B = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.8)
+    R = herm_matrix(nt, ntau, s, -1)
+    for n in range(-1, nt + 1):
+        oracle.convolution_timestep(n, R, A, Acc, B, B, beta, h, k)
+    d = tmp_path / "conv"
+    write_case(d, (nt, ntau, s, -1, k, beta, h, 0.0), A=A, Acc=Acc, B=B)
+    run(exe, "conv", d)
+    C = read_out(d, nt, ntau, s, -1)
+    for c in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(C, c), getattr(R, c)) < TOL, c
