@@ -142,21 +142,22 @@ def _rank(rank, world, port, nkx, nky, out):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_match_the_single_process_lattice(oracle):
-    """3x3 k-points split 4 + 5 over two processes (unequal weights): G_loc after every exchange
-    is the full k-average, so every G_k and G_loc equal the one-process oracle lattice to
-    rounding (the two partial sums are added in a different order)."""
-    nkx, nky, world = 3, 3, 2
+@pytest.mark.parametrize("nkx,nky,world,blocks", [(3, 3, 2, [(0, 4), (4, 9)]),
+                                                  (5, 2, 3, [(0, 3), (3, 6), (6, 10)])])
+def test_gloo_ranks_match_the_single_process_lattice(oracle, nkx, nky, world, blocks):
+    """3x3 k-points split 4 + 5 over two processes and 5x2 split 3 + 3 + 4 over three (unequal
+    weights): G_loc after every exchange is the full k-average, so every G_k and G_loc equal the
+    one-process oracle lattice to rounding (the partial sums are added in another order)."""
     Gs, Gloc, it_o, err_o = _oracle_reference(oracle, nkx, nky)
-    port = 29611 + os.getpid() % 1000
+    port = 29611 + 7 * world + os.getpid() % 1000
     mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_rank, args=(world, port, nkx, nky, out), nprocs=world, join=True, start_method="spawn")
     res = [out[r] for r in range(world)]
-    assert [(r["first"], r["last"]) for r in res] == [(0, 4), (4, 9)]
+    assert [(r["first"], r["last"]) for r in res] == blocks
     steps = NT - K
     for r in res:
-        assert r["nk_total"] == 9
+        assert r["nk_total"] == nkx * nky
         assert r["it"] == it_o == 7
         assert abs(r["err"] - err_o) <= 1e-9 * err_o + 1e-14  # converged to rounding: ~1e-19
         # bootstrap: (k+1) slices before and after each of 7 iterations; steps: ncorr + 1 each
@@ -168,4 +169,5 @@ def test_two_gloo_ranks_match_the_single_process_lattice(oracle):
             for c in ("ret", "les", "tv"):
                 assert rel_err(G[c], getattr(R, c)) < 1e-13, c
     for c in ("ret", "les", "tv"):  # every process holds the same G_loc
-        assert np.array_equal(res[0]["Gloc"][c], res[1]["Gloc"][c])
+        for r in res[1:]:
+            assert np.array_equal(res[0]["Gloc"][c], r["Gloc"][c])
