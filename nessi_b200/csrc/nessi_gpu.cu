@@ -2,6 +2,7 @@
 // Host side of the C ABI declared in include/nessi_gpu.h.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -24,6 +25,15 @@
 namespace {
 
 thread_local std::string g_err;
+// NVTX range for the time a call spends on the host (launches included); no-op unless a
+// profiler is attached
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 int g_device = 0;
 std::atomic<int> g_live_batches{0};  // created and not yet destroyed
 std::vector<int> g_tables_ready;  // devices whose c_tab was filled
@@ -903,6 +913,7 @@ static int find_group_checked(nessi_batch *b, int group, Group **out) {
 }
 
 static int timestep_kind(nessi_batch *b, int n, bool vie, const char *name) {
+    NvtxRange nvtx_(vie ? "nessi::vie2_timestep" : "nessi::dyson_timestep");
     CKR(check_batch(b));
     bool any = false;
     for (Group &g : b->groups) {
@@ -969,6 +980,7 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
 }
 
 int nessi_gpu_dyson_mat(nessi_batch *b) {
+    NvtxRange nvtx_("nessi::dyson_mat");
     CKR(check_batch(b));
     for (Group &g : b->groups) {
         if (g.vie) continue;  // VIE2 groups take G^mat from the caller
@@ -980,6 +992,7 @@ int nessi_gpu_dyson_mat(nessi_batch *b) {
 }
 
 static int start_kind(nessi_batch *b, bool vie, const char *name) {
+    NvtxRange nvtx_(vie ? "nessi::vie2_start" : "nessi::dyson_start");
     CKR(check_batch(b));
     bool any = false;
     for (Group &g : b->groups) {
@@ -1007,6 +1020,7 @@ int nessi_gpu_dyson_start(nessi_batch *b) { return start_kind(b, false, "dyson_s
 int nessi_gpu_vie2_start(nessi_batch *b) { return start_kind(b, true, "vie2_start"); }
 
 int nessi_gpu_vie2_mat(nessi_batch *b) {
+    NvtxRange nvtx_("nessi::vie2_mat");
     CKR(check_batch(b));
     bool any = false;
     for (Group &g : b->groups) {
@@ -1137,6 +1151,7 @@ int nessi_gpu_set_U(nessi_batch *b, int group, const void *U) {
 }
 
 int nessi_gpu_extrapolate_timestep(nessi_batch *b, int n) {
+    NvtxRange nvtx_("nessi::extrapolate_timestep");
     CKR(check_batch(b));
     for (Group &g : b->groups)
         if (n < g.k) { set_err("extrapolate_timestep: n = %d below the solve order %d", n, g.k); return NESSI_ERR_ARG; }
@@ -1150,6 +1165,7 @@ int nessi_gpu_extrapolate_timestep(nessi_batch *b, int n) {
 }
 
 int nessi_gpu_gloc_timestep(nessi_batch *b, int group, int tstp) {
+    NvtxRange nvtx_("nessi::gloc_timestep");
     Group *g;
     CKR(find_group_checked(b, group, &g));
     if (tstp < -1 || tstp > g->ntmax) { set_err("gloc: time step %d out of range", tstp); return NESSI_ERR_ARG; }
@@ -1161,6 +1177,7 @@ int nessi_gpu_gloc_timestep(nessi_batch *b, int group, int tstp) {
 }
 
 int nessi_gpu_sigma_2b_timestep(nessi_batch *b, int group, int tstp) {
+    NvtxRange nvtx_("nessi::sigma_2b_timestep");
     Group *g;
     CKR(find_group_checked(b, group, &g));
     if (!g->U) { set_err("sigma_2b: nessi_gpu_set_U was not called for group %d", group); return NESSI_ERR_ARG; }
@@ -1223,6 +1240,7 @@ static double slice_distance(const double2 *a, const double2 *b, long n_elem, in
 }
 
 int nessi_gpu_lattice_2b_start(nessi_batch *b, int max_iter, double tol, int *iters, double *err_out) {
+    NvtxRange nvtx_("nessi::lattice_2b_start");
     CKR(check_batch(b));
     if (max_iter < 0) { set_err("lattice_2b_start: max_iter < 0"); return NESSI_ERR_ARG; }
     std::vector<Group *> lat;
@@ -1280,6 +1298,7 @@ int nessi_gpu_lattice_2b_start(nessi_batch *b, int max_iter, double tol, int *it
 }
 
 int nessi_gpu_lattice_2b_timestep(nessi_batch *b, int n, int corrector_steps) {
+    NvtxRange nvtx_("nessi::lattice_2b_timestep");
     CKR(check_batch(b));
     if (corrector_steps < 1) { set_err("lattice_2b_timestep: corrector_steps must be >= 1"); return NESSI_ERR_ARG; }
     bool any = false;
@@ -1316,6 +1335,7 @@ int nessi_gpu_get_volterra_choice(nessi_batch *b, int group, int *pp_ret, int *p
 }
 
 int nessi_gpu_graph_record(nessi_batch *b, int kind, int n0, int n1, int corrector_steps) {
+    NvtxRange nvtx_("nessi::graph_record");
     CKR(check_batch(b));
     if (kind < 0 || kind > 2 || n1 < n0) { set_err("graph_record: bad arguments"); return NESSI_ERR_ARG; }
     CK(cudaStreamSynchronize(b->stream));
@@ -1346,6 +1366,7 @@ int nessi_gpu_graph_record(nessi_batch *b, int kind, int n0, int n1, int correct
 }
 
 int nessi_gpu_graph_launch(nessi_batch *b) {
+    NvtxRange nvtx_("nessi::graph_launch");
     CKR(check_batch(b));
     if (!b->graph) { set_err("graph_launch: nothing recorded"); return NESSI_ERR_ARG; }
     CK(cudaGraphLaunch(b->graph, b->stream));
@@ -1392,6 +1413,7 @@ int noalloc_launch(const GroupDev &gd, const ProbDev &pd, const MatScratch &w, i
 
 extern "C" int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int solve_order, double beta, double mu,
                                            const void *H, const void *sigma_mat, void *gmat, void *stream) {
+    NvtxRange nvtx_("nessi::dyson_mat_noalloc");
     if (!H || !sigma_mat || !gmat) { set_err("dyson_mat_noalloc: null pointer"); return NESSI_ERR_ARG; }
     if (size1 < 1 || size1 > NESSI_MAXS || (sig != 1 && sig != -1) || solve_order < 1 || solve_order > CNTR_KMAX ||
         ntau < solve_order || ntau % 2 || !(beta > 0)) {
@@ -1469,6 +1491,7 @@ extern "C" int nessi_gpu_convolution_timestep(int n, int count, const nessi_hm_p
                                               const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B,
                                               const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a,
                                               int sig_b, int solve_order, double beta, double h, void *stream) {
+    NvtxRange nvtx_("nessi::convolution_timestep");
     if (count < 0 || !C || !A || !Acc || !B || !Bcc) { set_err("convolution_timestep: bad arguments"); return NESSI_ERR_ARG; }
     if (size1 < 1 || size1 > NESSI_MAXS || solve_order < 1 || solve_order > CNTR_KMAX || nt < solve_order ||
         ntau < solve_order || n < -1 || n > nt || (sig_a != 1 && sig_a != -1) || (sig_b != 1 && sig_b != -1) ||
