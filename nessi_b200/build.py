@@ -42,10 +42,12 @@ def build_io(force=False, verbose=False):
     if not force and os.path.exists(IO_LIB) and all(os.path.getmtime(f) <= os.path.getmtime(IO_LIB)
                                                     for f in IO_SOURCES):
         return IO_LIB
-    cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", IO_LIB, IO_SOURCES[0]]
+    tmp = IO_LIB + ".tmp"
+    cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", tmp, IO_SOURCES[0]]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd, cwd=CSRC)
+    os.replace(tmp, IO_LIB)  # a process that has the old library loaded keeps its copy
     return IO_LIB
 
 
@@ -53,10 +55,12 @@ def build(force=False, verbose=False):
     build_io(force=force, verbose=verbose)
     if not force and up_to_date():
         return LIB
-    cmd = [NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcublas"]
+    tmp = LIB + ".tmp"
+    cmd = [NVCC] + FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcublas"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd, cwd=CSRC)
+    os.replace(tmp, LIB)  # a process that has the old library loaded keeps its copy
     return LIB
 
 
