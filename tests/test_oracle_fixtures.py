@@ -133,3 +133,27 @@ def test_green_from_H_is_the_free_propagator(oracle, sig, shift):
     O.green_from_H(G, 0.0, a, beta, h)
     err = sum(O.distance_norm2(t, G, exact) for t in range(-1, nt))
     assert err < 1e-6, err                 # equilibrium.cpp:244 (eps)
+
+
+def test_convolution_bosonic_boundary_signs(oracle):
+    """libcntr/test/convolution.cpp:98-143: the free-boson identity A*B = (A - B)/(wa - wb) at
+    beta = 0.1, ntau = 500, t_max = 2 on refined grids h = 2/nt, nt = 10..640; the reference
+    checks the last time step of the finest grid at 1e-6 (its last assignment is the lesser
+    distance); here every component of that step is checked, and the error falls with h."""
+    O = oracle
+    wa, wb, k, beta, ntau, tmax = 1.123, 0.345, 5, 0.1, 500, 2.0
+    errs = []
+    for fac2 in (1, 4, 16, 64):
+        nt = 10 * fac2
+        h = tmax / nt
+        A, B, AB = (herm_matrix(nt, ntau, 1, 1) for _ in range(3))
+        O.green_from_H(A, 0.0, np.array([[wa]]), beta, h)
+        O.green_from_H(B, 0.0, np.array([[wb]]), beta, h)
+        C = A.copy()
+        C.incr_timestep(nt, B, -1.0)
+        C.smul(nt, 1.0 / (wa - wb))
+        for n in (-1, nt):  # convolution_timestep reads only A and B: the last step suffices
+            O.convolution_timestep(n, AB, A, A, B, B, beta, h, k)
+        errs.append(O.distance_norm2(nt, C, AB))
+    assert errs[-1] < 1e-6, errs            # convolution.cpp:142 (eps)
+    assert errs[-1] < errs[0]
