@@ -168,3 +168,20 @@ def test_restart_reproduces_the_propagation(oracle, tmp_path):
         O.dyson_timestep(n, R, mu, H, Sig, beta, h, k)
     for c in ("ret", "les", "tv", "mat"):
         assert np.array_equal(getattr(R, c), getattr(full, c)), c
+
+
+def test_reference_read_write_cases(oracle, tmp_path):
+    """libcntr/test/herm_matrix_member.cpp:472-506: a free 2 x 2 propagator (nt = 100, ntau = 50,
+    beta = 5, h = 0.01) printed at precision 12 and read back whole, and up to nt1 = 50; the
+    summed distance_norm2 stays below the reference's 1e-7."""
+    from nessi_b200.herm_matrix import distance_norm2
+    nt, ntau, s, beta, h = 100, 50, 2, 5.0, 0.01
+    h0 = np.array([[-0.4, 0.1j], [-0.1j, 0.6]])
+    G1 = herm_matrix(nt, ntau, s, -1)
+    oracle.green_from_H(G1, 0.0, h0, beta, h)
+    f = tmp_path / "herm_matrix_plain.dat"
+    hm_file.print_to_file(G1, f, 12)
+    G2 = hm_file.read_from_file(f, herm_matrix(nt, ntau, s, -1))
+    assert sum(distance_norm2(t, G1, G2) for t in range(-1, nt + 1)) < 1e-7
+    G3 = hm_file.read_from_file_nt1(herm_matrix(nt, ntau, s, -1), 50, f)
+    assert sum(distance_norm2(t, G1, G3) for t in range(-1, 51)) < 1e-7
