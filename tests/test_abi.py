@@ -50,3 +50,32 @@ def test_io_library_exports_all_declared_symbols():
 def test_finalize_without_batches_needs_no_device():
     from nessi_b200 import gpu
     gpu.finalize()   # nothing was set up: returns at once, on a machine without a GPU too
+
+
+@pytest.mark.parametrize("bad", [dict(nt=-1), dict(size1=9), dict(size1=0), dict(sig=0), dict(solve_order=6),
+                                 dict(solve_order=0), dict(ntau=3), dict(h=0.0), dict(beta=-1.0)])
+def test_bad_descriptor_is_rejected_before_the_device(bad):
+    """Host-side failure detection: descriptors libcntr would assert on come back as
+    NESSI_ERR_ARG with a message, before any device call (so also on a machine without a GPU)."""
+    import ctypes
+    from nessi_b200 import gpu
+    d = dict(nt=10, ntau=8, size1=2, sig=-1, solve_order=5, sigma_group=0, beta=2.0, h=0.05, mu=0.0)
+    d.update(bad)
+    arr = (gpu.ProblemDesc * 1)(gpu.ProblemDesc(d["nt"], d["ntau"], d["size1"], d["sig"], d["solve_order"],
+                                                d["sigma_group"], d["beta"], d["h"], d["mu"]))
+    h = ctypes.c_void_p()
+    L = gpu.load_library()
+    assert L.nessi_gpu_batch_create(ctypes.byref(h), arr, 1, gpu.PREC_FP64) == 1
+    assert b"bad descriptor" in L.nessi_gpu_last_error()
+    assert not h.value
+    assert L.nessi_gpu_batch_create(ctypes.byref(h), arr, 1, 7) == 1          # unknown precision
+    assert L.nessi_gpu_batch_create(ctypes.byref(h), arr, 0, gpu.PREC_FP64) == 1  # no problems
+
+
+def test_null_arguments_are_rejected_before_the_device():
+    from nessi_b200 import gpu
+    L = gpu.load_library()
+    assert L.nessi_gpu_dyson_mat_noalloc(10, 1, -1, 5, 2.0, 0.0, None, None, None, None) == 1
+    assert L.nessi_gpu_convolution_timestep_host(2, None, None, None, None, None, 10, 8, 1, -1, -1, 5, 2.0, 0.05) == 1
+    assert L.nessi_gpu_convolution_host(None, None, None, None, None, 10, 8, 1, -1, -1, 5, 2.0, 0.05) == 1
+    assert L.nessi_gpu_set_G(None, 0, None, None, None, None) == 1   # no batch
