@@ -171,3 +171,58 @@ def test_gloo_ranks_match_the_single_process_lattice(oracle, nkx, nky, world, bl
     for c in ("ret", "les", "tv"):  # every process holds the same G_loc
         for r in res[1:]:
             assert np.array_equal(res[0]["Gloc"][c], r["Gloc"][c])
+
+
+def _rank_with_failure(rank, world, port, out):
+    """Rank 1 raises in the middle of the time stepping (a host-side failure); rank 0 must see its
+    next exchange fail within the process group's timeout instead of waiting for ever."""
+    import time
+    import torch.distributed as dist
+    for p in (HERE, os.path.join(os.path.dirname(HERE), "oracle"), os.path.dirname(HERE)):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=10))
+    import oracle as O
+    first, last = shard_bounds(9, rank, world)
+    Gs, Hs, U = _lattice(O, 3, 3)
+    b = OracleLatticeBatch(O, Gs[first:last], Hs[first:last], U)
+    if rank == 1:
+        real = b.dyson_timestep
+
+        def failing(n):
+            if n == K + 3:
+                raise RuntimeError("injected failure on rank 1 at step %d" % n)
+            real(n)
+        b.dyson_timestep = failing
+    L = ShardedLattice(b)
+    L.start(max_iter=6, tol=0.0)
+    t0 = time.time()
+    try:
+        for n in range(K + 1, NT + 1):
+            L.timestep(n, NCORR)
+        out[rank] = ("finished", time.time() - t0)
+    except Exception as e:  # rank 1: the injected error; rank 0: the failed collective
+        out[rank] = (type(e).__name__ + ": " + str(e)[:200], time.time() - t0)
+        if rank == 1:
+            os._exit(3)   # leave without tearing down the group, as a crashed process would
+    os._exit(0)
+
+
+def test_a_failing_rank_does_not_hang_the_others():
+    world, port = 2, 29711 + os.getpid() % 1000
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    ctx = mp.start_processes(_rank_with_failure, args=(world, port, out), nprocs=world, join=False,
+                             start_method="spawn")
+    for p in ctx.processes:
+        p.join(timeout=120)
+    assert all(not p.is_alive() for p in ctx.processes), "a rank is still waiting"
+    for p in ctx.processes:
+        if p.is_alive():
+            p.kill()
+    assert "injected failure" in out[1][0]
+    msg, waited = out[0]
+    assert msg != "finished" and waited < 60, out[0]   # rank 0's collective failed, it did not hang
+    assert [p.exitcode for p in ctx.processes] == [0, 3]
