@@ -10,6 +10,11 @@
 // complex<double>, the routines of the hot path with the reference's loop order
 // and weight selection.  Each function names the reference lines it follows.
 //
+// Pinned against: the reference's integration tables (bit for bit), the closed-form
+// known answers of its test suite (embedding, convolution identities, bubbles, Matsubara
+// fixpoint, free propagators), and libcntr's own output: the golden densities of
+// libcntr/test/fkm_bethe_quench.h5, reproduced to 4.8e-13 (tests/test_oracle_fkm.py).
+//
 // Storage follows libcntr's herm_matrix exactly (cntr_herm_matrix_impl.hpp:457-477):
 //   ret(t,t'), t' <= t   at ((t(t+1))/2 + t') * s^2
 //   les(t,t'), t <= t'   at ((t'(t'+1))/2 + t) * s^2
