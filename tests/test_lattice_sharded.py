@@ -226,3 +226,20 @@ def test_a_failing_rank_does_not_hang_the_others():
     msg, waited = out[0]
     assert msg != "finished" and waited < 60, out[0]   # rank 0's collective failed, it did not hang
     assert [p.exitcode for p in ctx.processes] == [0, 3]
+
+
+def test_sharded_lattice_rejects_bad_arguments(oracle):
+    """The checks nessi_gpu_lattice_2b_start / _timestep make, and the exchange sizes."""
+    Gs, Hs, U = _lattice(oracle, 2, 2)
+    b = OracleLatticeBatch(oracle, Gs, Hs, U)
+    L = ShardedLattice(b)
+    with pytest.raises(ValueError):
+        L.start(max_iter=-1)
+    with pytest.raises(ValueError):
+        L.timestep(K, NCORR)          # n must exceed the solve order
+    with pytest.raises(ValueError):
+        L.timestep(K + 1, 0)          # at least one corrector
+    # one time step's all-reduce: ret row, tv row and les column of G_loc
+    assert L.exchange_bytes(NT) == 16 * (2 * (NT + 1) + NTAU + 1)
+    assert L.exchange_bytes(-1) == 16 * (NTAU + 1)
+    assert L.weight == {0: 1.0} and L.nk_total == {0: 4}
