@@ -167,6 +167,31 @@ def cpu_sample(W, target_s=15.0, max_threads=None):
 
 
 # ------------------------------------------------------------------------------------------
+def step_bytes(W, mixed):
+    """Algorithmic HBM bytes of one propagation (time steps k+1..nt of every problem), by the
+    per-problem-step formula of the history convolutions: with N = n+1, M = ntau+1,
+      b s^2 (N M) [G^tv history] + 16 s^2 (2N + M) [G slice] + 16 s^2 (N M + N(N+1) + M) [Sigma^tv
+      history, Sigma^R / Sigma^< triangles, G^mat], the Sigma part once per group and step,
+    b = 16 (FP64) or 8 (FP32 history); a lattice step repeats the Dyson step once per corrector."""
+    ncorr = getattr(W, "ncorr", None) or 1
+    groups = {}
+    for d in W.descs:
+        groups.setdefault(d.get("sigma_group", 0), []).append(d)
+    total = 0.0
+    for members in groups.values():
+        s2 = members[0]["size1"] ** 2
+        M = members[0]["ntau"] + 1
+        nts = np.array(sorted(d["nt"] for d in members))
+        n = np.arange(W.k + 1, int(nts.max()) + 1, dtype=np.float64)
+        N = n + 1
+        active = len(nts) - np.searchsorted(nts, n, side="left")  # members with nt >= n
+        b = 8.0 if mixed else 16.0
+        per_problem = b * s2 * N * M + 16.0 * s2 * (2 * N + M)
+        shared = 16.0 * s2 * (N * M + N * (N + 1) + M)
+        total += float(np.sum(active * per_problem + (active > 0) * shared))
+    return ncorr * total
+
+
 def build_workload(name, rank, world):
     from nessi_b200 import workloads
     shift = 0.0 if world == 1 else (2 * math.pi / 256) * rank / world
@@ -463,6 +488,17 @@ def main():
                                 "scaled to this launch's algorithmic bytes",
                 "algorithmic_bytes_per_launch": dbytes / dl if dl else None,
                 "avg_launch_ms": dms / dl if dl else None}
+    # the whole step against the same peak: all algorithmic bytes of the propagation over its
+    # time; low where the sequential Volterra recursions (k_ret, k_les) set the pace
+    try:
+        sb = step_bytes(W, args.precision == "mixed")
+        ach = sb * args.steps / (ms / 1000.0) / 1e9
+        step_roofline = {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind,
+                         "bytes_per_step": sb,
+                         "definition": "sum over problem-steps of the history-convolution bytes (G^tv, Sigma^tv "
+                                       "histories, Sigma triangles, G slices) / device time of the timed steps"}
+    except Exception as exc:  # the line stands without it
+        step_roofline = {"error": "%s: %s" % (type(exc).__name__, exc)}
     breakdown = {kname: {"ms": v[0] / prof_steps, "launches": v[1] // prof_steps,
                          "share": v[0] / max(1e-9, sum(x[0] for x in prof.values()))}
                  for kname, v in prof.items()}
@@ -571,7 +607,8 @@ def main():
                                           "dyson_start iterations (set-up, untimed)" % boot_iters) if W.lattice else
                                "free propagator of H_k(-1) for mat and steps 0..k (set-up, untimed)",
                                **W.info),
-                "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "step_roofline": step_roofline, "kernels": breakdown, "cpu_baseline": cpu,
+                "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk,
                 "launch": "CUDA graph of the whole propagation, replayed each step" if use_graph else "eager",
                 "volterra_kernels": {g: {"ret": v[0], "les": v[1]} for g, v in volterra.items()}}
