@@ -439,3 +439,52 @@ def vie2(G, F, Fcc, Q, beta, h, SolveOrder=5):
         b.get_G(0, G)
     finally:
         b.close()
+
+
+def _value_at_minus1(X, s):
+    """The (s, s) value of a cntr::function at t = -1, or a plain matrix."""
+    a = X.get_value(-1) if isinstance(X, function) else np.asarray(X, np.complex128)
+    return np.ascontiguousarray(a, np.complex128).reshape(s, s)
+
+
+def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None):
+    """cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder) with the default fixpoint method and
+    force_hermitian (cntr_dyson_decl.hpp:77-79): writes G^mat.  With ``SigmaMF`` (a
+    cntr::function or the (s, s) matrix of its value at -1) it is the mean-field overload
+    dyson_mat(G, mu, H, SigmaMF, Sigma, beta, SolveOrder) (:81-83; cntr_dyson_impl.hpp:472-492,
+    1270-1298): with G0 the free propagator of H(-1), [1 + F] G = G0 is solved by the fixpoint
+    with F = -(G0 * Sigma + G0 SigmaMF(-1)); the convolution and the fixpoint run on the GPU."""
+    from .equilibrium import green_from_H
+    k, s, ntau, sig = SolveOrder, G.size1, G.ntau, G.sig
+    h0 = _value_at_minus1(H, s)
+    Sk = herm_matrix(k, ntau, s, sig)  # only the Matsubara branch takes part
+    Sk.mat[...] = Sigma.mat
+    desc = dict(nt=k, ntau=ntau, size1=s, sig=sig, solve_order=k, beta=beta, h=1.0, mu=mu)
+    out = herm_matrix(k, ntau, s, sig)
+    if SigmaMF is None:
+        b = Batch([desc])
+        try:
+            b.set_H(0, np.broadcast_to(h0, (k + 2, s, s)).copy())
+            b.set_sigma(0, Sk)
+            b.dyson_mat()
+            b.get_G(0, out)
+        finally:
+            b.close()
+        G.mat[...] = out.mat
+        return
+    mf = _value_at_minus1(SigmaMF, s)
+    G0 = herm_matrix(k, ntau, s, sig)
+    green_from_H(G0, mu, h0, beta, 1.0)
+    C = herm_matrix(k, ntau, s, sig)
+    convolution_timestep(-1, C, G0, G0, Sk, Sk, beta, 1.0, k)  # convolution_matsubara(G0, Sigma)
+    F = herm_matrix(k, ntau, s, sig)
+    F.mat[...] = -(C.mat + G0.mat @ mf)
+    b = Batch([desc])
+    try:
+        b.set_F(0, F, F)
+        b.set_Q(0, G0)
+        b.vie2_mat()
+        b.get_G(0, out)
+    finally:
+        b.close()
+    G.mat[...] = 0.5 * (out.mat + out.mat.conj().transpose(0, 2, 1))  # force_matsubara_hermitian

@@ -56,3 +56,56 @@ def test_whole_vie2(oracle):
     assert rel_err(G.mat, ref.mat) < TOL
     e = component_errors(G, ref, 0, nt)
     assert max(e.values()) < TOL, e
+
+
+def _mat_problem(oracle, seed, s, ntau, beta):
+    from builders import rand_herm
+    from nessi_b200 import function
+    rng = np.random.default_rng(seed)
+    Sig = herm_matrix(-1, ntau, s, -1)
+    oracle.green_from_H(Sig, 0.0, rand_herm(rng, s, 0.7), beta, 1.0)
+    Sig.smul(-1, 0.3)
+    h0, mf = rand_herm(rng, s, 0.8), rand_herm(rng, s, 0.3)
+    H = function(-1, s)
+    H.set_value(-1, h0)
+    return Sig, H, h0, mf
+
+
+@pytest.mark.parametrize("s", [1, 2])
+def test_dyson_mat_drop_in(oracle, s):
+    """gpu.dyson_mat (cntr::dyson_mat, fixpoint) on a Matsubara-only herm_matrix (nt = -1)."""
+    from nessi_b200 import gpu
+    ntau, beta, k, mu = 200, 5.0, 5, 0.1
+    Sig, H, _, _ = _mat_problem(oracle, 60 + s, s, ntau, beta)
+    ref = herm_matrix(-1, ntau, s, -1)
+    oracle.dyson_mat(ref, Sig, mu, H, beta, k)
+    G = herm_matrix(-1, ntau, s, -1)
+    gpu.dyson_mat(G, mu, H, Sig, beta, k)
+    assert rel_err(G.mat, ref.mat) < TOL
+
+
+@pytest.mark.parametrize("s", [1, 2])
+def test_dyson_mat_mean_field_overload(oracle, s):
+    """dyson_mat(G, mu, H, SigmaMF, Sigma, ...) (cntr_dyson_impl.hpp:472-492): against the same
+    steps done by the oracle (G0 = green_from_H, F = -(G0 * Sigma + G0 SigmaMF), vie2_mat
+    fixpoint, force_matsubara_hermitian), and against dyson_mat with H(-1) + SigmaMF."""
+    from nessi_b200 import function, gpu
+    ntau, beta, k, mu = 200, 5.0, 5, 0.1
+    Sig, H, h0, mf = _mat_problem(oracle, 70 + s, s, ntau, beta)
+    G0 = herm_matrix(-1, ntau, s, -1)
+    oracle.green_from_H(G0, mu, h0, beta, 1.0)
+    C = herm_matrix(-1, ntau, s, -1)
+    oracle.convolution_matsubara(C, G0, Sig, beta, k)
+    F = herm_matrix(-1, ntau, s, -1)
+    F.mat[...] = -(C.mat + G0.mat @ mf)
+    ref = herm_matrix(-1, ntau, s, -1)
+    oracle.vie2_mat(ref, F, F, G0, beta, k)
+    oracle.force_matsubara_hermitian(ref)
+    G = herm_matrix(-1, ntau, s, -1)
+    gpu.dyson_mat(G, mu, H, Sig, beta, k, SigmaMF=mf)
+    assert rel_err(G.mat, ref.mat) < TOL
+    Hmf = function(-1, s)
+    Hmf.set_value(-1, h0 + mf)
+    alt = herm_matrix(-1, ntau, s, -1)
+    oracle.dyson_mat(alt, Sig, mu, Hmf, beta, k)
+    assert rel_err(G.mat, alt.mat) < 1e-9    # the two formulations agree to the fixpoint's convergence
