@@ -159,6 +159,14 @@ template <class HM, class FN> class Batch {
     std::vector<FN *> H_;
 };
 
+// Matsubara methods of libcntr (cntr_global_settings.hpp): the device solves by the default one
+constexpr int MAT_FIXPOINT = 2;
+inline void require_fixpoint(int method, bool force_hermitian = true) {
+    if (method != MAT_FIXPOINT || !force_hermitian)
+        throw std::invalid_argument("cntr_gpu: only the default Matsubara solve (CNTR_MAT_FIXPOINT, force_hermitian) "
+                                    "runs on the device");
+}
+
 // ---- single-problem drop-ins (cntr_dyson_decl.hpp:78-92) -------------------------------
 template <class HM, class FN>
 void dyson_timestep(int n, HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveOrder = 5) {
@@ -178,21 +186,27 @@ void dyson_start(HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int 
     for (int n = 0; n <= SolveOrder; n++) b.download_timestep(0, n);
 }
 
+// cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder, method, force_hermitian)
+// (cntr_dyson_decl.hpp:77-79): only H(-1) and Sigma^mat take part, so G may hold the Matsubara
+// branch alone (nt = -1); the device problem carries k time steps that stay unused
 template <class HM, class FN>
-void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder = 5) {
-    Batch<HM, FN> b;
-    b.add(G, H, mu, beta, 1.0, SolveOrder);
-    b.build(Sigma);
-    b.dyson_mat();
-    b.download_timestep(0, -1);
-}
-
-// Matsubara methods of libcntr (cntr_global_settings.hpp): the device solves by the default one
-constexpr int MAT_FIXPOINT = 2;
-inline void require_fixpoint(int method, bool force_hermitian = true) {
-    if (method != MAT_FIXPOINT || !force_hermitian)
-        throw std::invalid_argument("cntr_gpu: only the default Matsubara solve (CNTR_MAT_FIXPOINT, force_hermitian) "
-                                    "runs on the device");
+void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT,
+               bool force_hermitian = true) {
+    require_fixpoint(method, force_hermitian);
+    nessi_problem_desc d;
+    d.nt = SolveOrder; d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = 1.0; d.mu = mu;
+    const long es = (long)G.size1() * G.size1();
+    std::vector<std::complex<double>> h0((long)(SolveOrder + 2) * es);
+    for (int t = 0; t < SolveOrder + 2; t++) std::copy(H.ptr(-1), H.ptr(-1) + es, h0.begin() + t * es);
+    nessi_batch *b = nullptr;
+    check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
+    int rc = nessi_gpu_set_H(b, 0, h0.data());
+    if (!rc) rc = nessi_gpu_set_sigma(b, 0, nullptr, nullptr, nullptr, Sigma.matptr(0));
+    if (!rc) rc = nessi_gpu_dyson_mat(b);
+    if (!rc) rc = nessi_gpu_get_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
+    nessi_gpu_batch_destroy(b);
+    check(rc);
 }
 
 // cntr::dyson(G, mu, H, Sigma, beta, h, SolveOrder, matsubara_method, force_hermitian)

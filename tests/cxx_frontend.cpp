@@ -2,7 +2,7 @@
 // herm_matrix / function pair with libcntr's accessors and layout, filled from raw files
 // (complex128, libcntr layout), one cntr_gpu call, the result written back.
 //
-//   cxx_frontend <mode> <dir>      mode: echo | dyson | steps | vie2 | conv
+//   cxx_frontend <mode> <dir>      mode: echo | mat | dyson | steps | vie2 | conv
 //
 // Files in <dir>: dims.txt ("nt ntau size1 sig k beta h mu"), and <name>.{ret,les,tv,mat}
 // for the herm_matrix operands (H.fn for the function).  The result is G (or C).
@@ -69,7 +69,7 @@ static void save_hm(const HM &G, const std::string &base) {
 
 int main(int argc, char **argv) {
     if (argc != 3) {
-        std::fprintf(stderr, "usage: %s echo|dyson|steps|vie2|conv <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s echo|mat|dyson|steps|vie2|conv <dir>\n", argv[0]);
         return 2;
     }
     const std::string mode = argv[1], dir = std::string(argv[2]) + "/";
@@ -86,6 +86,13 @@ int main(int argc, char **argv) {
         HM G(nt, ntau, s, sig);
         if (mode == "echo") {  // the file handling alone (no device)
             load_hm(G, dir + "A");
+            save_hm(G, dir + "out");
+        } else if (mode == "mat") {  // cntr::dyson_mat, also for a Matsubara-only G (nt = -1)
+            HM Sigma(nt, ntau, s, sig);
+            FN H(nt, s);
+            load_hm(Sigma, dir + "Sigma");
+            load(H.d_, dir + "H.fn");
+            cntr_gpu::dyson_mat(G, mu, H, Sigma, beta, k);
             save_hm(G, dir + "out");
         } else if (mode == "dyson" || mode == "steps") {
             HM Sigma(nt, ntau, s, sig);

@@ -54,20 +54,44 @@ def run(exe, mode, d):
     assert r.returncode == 0, r.stderr
 
 
-def test_file_handling_without_device(tmp_path):
+@pytest.mark.parametrize("nt", [6, -1])
+def test_file_handling_without_device(tmp_path, nt):
     """The program's own file round trip (mode echo), which needs no GPU."""
     exe = build_frontend(tmp_path)
     rng = np.random.default_rng(1)
-    A = herm_matrix(6, 5, 2, -1)
+    A = herm_matrix(nt, 5, 2, -1)
     for c in ("ret", "les", "tv", "mat"):
         a = getattr(A, c)
         a[...] = rng.normal(size=a.shape) + 1j * rng.normal(size=a.shape)
     d = tmp_path / "echo"
-    write_case(d, (6, 5, 2, -1, 5, 1.0, 0.1, 0.0), A=A)
+    write_case(d, (nt, 5, 2, -1, 5, 1.0, 0.1, 0.0), A=A)
     run(exe, "echo", d)
-    B = read_out(d, 6, 5, 2, -1)
+    B = read_out(d, nt, 5, 2, -1)
     for c in ("ret", "les", "tv", "mat"):
         assert np.array_equal(getattr(A, c), getattr(B, c))
+
+
+@pytest.mark.gpu
+def test_dyson_mat_of_a_matsubara_only_matrix(oracle, tmp_path):
+    """cntr_gpu::dyson_mat on herm_matrix(-1, ntau, 2, -1), as libcntr programs call it for the
+    equilibrium alone."""
+    from nessi_b200 import function
+    from builders import rand_herm
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(53)
+    ntau, s, beta, k, mu = 100, 2, 5.0, 5, 0.1
+    Sig = herm_matrix(-1, ntau, s, -1)
+    oracle.green_from_H(Sig, 0.0, rand_herm(rng, s, 0.7), beta, 1.0)
+    Sig.smul(-1, 0.3)
+    H = function(-1, s)
+    H.set_value(-1, rand_herm(rng, s, 0.8))
+    ref = herm_matrix(-1, ntau, s, -1)
+    oracle.dyson_mat(ref, Sig, mu, H, beta, k)
+    d = tmp_path / "mat"
+    write_case(d, (-1, ntau, s, -1, k, beta, 1.0, mu), Sigma=Sig, H=H.data)
+    run(exe, "mat", d)
+    G = read_out(d, -1, ntau, s, -1)
+    assert rel_err(G.mat, ref.mat) < TOL
 
 
 @pytest.mark.gpu
