@@ -268,11 +268,19 @@ template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double
 }
 
 // cntr::vie2_mat(G, F, Fcc, Q, beta, SolveOrder, method) (cntr_vie2_decl.hpp:63): G^mat
+// (only the Matsubara branches take part, so the matrices may hold it alone, nt = -1)
 template <class HM>
 void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT) {
     require_fixpoint(method);
-    nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, 1.0, SolveOrder, false);
-    int rc = nessi_gpu_vie2_mat(b);
+    (void)Fcc;  // F^mat alone enters the Matsubara equation
+    nessi_problem_desc d;
+    d.nt = SolveOrder; d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+    d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = 1.0; d.mu = 0.0;
+    nessi_batch *b = nullptr;
+    check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
+    int rc = nessi_gpu_set_F(b, 0, nullptr, nullptr, nullptr, F.matptr(0), nullptr, nullptr);
+    if (!rc) rc = nessi_gpu_set_Q(b, 0, nullptr, nullptr, nullptr, Q.matptr(0));
+    if (!rc) rc = nessi_gpu_vie2_mat(b);
     if (!rc) rc = nessi_gpu_get_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
     nessi_gpu_batch_destroy(b);
     check(rc);
