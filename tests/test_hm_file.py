@@ -185,3 +185,34 @@ def test_reference_read_write_cases(oracle, tmp_path):
     assert sum(distance_norm2(t, G1, G2) for t in range(-1, nt + 1)) < 1e-7
     G3 = hm_file.read_from_file_nt1(herm_matrix(nt, ntau, s, -1), 50, f)
     assert sum(distance_norm2(t, G1, G3) for t in range(-1, 51)) < 1e-7
+
+
+def test_format_against_the_reference_reader(tmp_path):
+    """tests/golden/hm_text_small.{txt,json} (tests/golden/make_text_format_golden.py): the writer
+    reproduces the committed text byte for byte, and the reader returns exactly what the
+    reference's own Python reader (libcntr/python3/ReadCNTR.py read_gf) parsed from it."""
+    import json
+    import os
+    import sys
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, golden)
+    from make_text_format_golden import hm_text_values
+    G = hm_text_values()
+    f = tmp_path / "g.txt"
+    hm_file.print_to_file(G, f, precision=17)
+    txt = os.path.join(golden, "hm_text_small.txt")
+    assert f.read_bytes() == open(txt, "rb").read()
+    ref = json.load(open(os.path.join(golden, "hm_text_small.json")))
+
+    def arr(c):
+        return (np.array(ref[c]["re"]) + 1j * np.array(ref[c]["im"])).reshape(ref[c]["shape"])
+    R = hm_file.read_from_file(txt)
+    assert (R.nt, R.ntau, R.size1, R.sig) == (ref["nt"], ref["ntau"], ref["dim"], ref["sig"])
+    assert np.array_equal(R.mat, arr("mat")) and np.array_equal(R.tv, arr("tv"))
+    ret, les = arr("ret"), arr("les")
+    for i in range(R.nt + 1):
+        for j in range(i + 1):
+            assert np.array_equal(R.get_ret(i, j), ret[i, j])
+            assert np.array_equal(R.get_les(j, i), les[j, i])
+    for c in ("ret", "les", "tv", "mat"):  # and both equal the values written
+        assert np.array_equal(getattr(R, c), getattr(G, c))
