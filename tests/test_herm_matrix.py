@@ -83,3 +83,36 @@ def test_bad_dimensions_raise():
     for args in ((-2, 4, 1, -1), (3, -1, 1, -1), (3, 4, 0, -1), (3, 4, 1, 0)):
         with pytest.raises(ValueError):
             herm_matrix(*args)
+
+
+def test_distance_norm2_definition(oracle):
+    """libcntr/test/utilities.cpp:380-450: distance_norm2(tstp) is the sum over the time step's
+    elements (ret row, tv row, les column; mat for -1) of the Frobenius norm of the difference;
+    the host function, the oracle and an explicit loop agree for two free 2 x 2 propagators."""
+    nt, ntau, beta, h = 10, 20, 5.0, 0.05
+    h1 = np.array([[-1.0, -0.7j], [0.7j, 0.8]])
+    h2 = np.array([[-2.0, -1.4j], [1.4j, 1.6]])
+    G1, G2 = herm_matrix(nt, ntau, 2, -1), herm_matrix(nt, ntau, 2, -1)
+    oracle.green_from_H(G1, 0.0, h1, beta, h)
+    oracle.green_from_H(G2, 0.0, h2, beta, h)
+    for t in range(-1, nt + 1):
+        if t < 0:
+            ref = sum(np.linalg.norm(G1.mat[m] - G2.mat[m]) for m in range(ntau + 1))
+        else:
+            ref = (sum(np.linalg.norm(G1.get_ret(t, j) - G2.get_ret(t, j)) for j in range(t + 1)) +
+                   sum(np.linalg.norm(G1.get_tv(t, m) - G2.get_tv(t, m)) for m in range(ntau + 1)) +
+                   sum(np.linalg.norm(G1.get_les(j, t) - G2.get_les(j, t)) for j in range(t + 1)))
+        assert abs(distance_norm2(t, G1, G2) - ref) <= 1e-12 * ref
+        assert abs(oracle.distance_norm2(t, G1, G2) - ref) <= 1e-12 * ref
+
+
+def test_force_matsubara_hermitian(oracle):
+    """utilities.cpp:452-486: G^M + i G2^M made hermitian again at every tau."""
+    ntau, beta = 20, 5.0
+    G1, G2 = herm_matrix(-1, ntau, 2, -1), herm_matrix(-1, ntau, 2, -1)
+    oracle.green_from_H(G1, 0.0, np.array([[-1.0, -0.7j], [0.7j, 0.8]]), beta, 0.05)
+    oracle.green_from_H(G2, 0.0, np.array([[0.8, 0.7], [0.7, -1.0]]), beta, 0.05)
+    G1.incr_timestep(-1, G2, 1j)
+    assert max(np.linalg.norm(m - m.conj().T) for m in G1.mat) > 1e-3
+    oracle.force_matsubara_hermitian(G1)
+    assert sum(np.linalg.norm(m - m.conj().T) for m in G1.mat) < 1e-14
