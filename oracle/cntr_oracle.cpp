@@ -1684,6 +1684,57 @@ void orc_bubble2_scalar(int tstp, orc_hm *Ch, orc_hm *Ah, orc_hm *Acch, orc_hm *
     for (int m = 0; m <= ntau; m++) *C.tvptr(tstp, m) = kI * *A.tvptr(tstp, m) * *B.tvptr(tstp, m);
 }
 
+// Element-index bubbles (cntr_bubble_impl.hpp:17-130, 138-330):
+//   Bubble1: C_{c1c2}(t,t') = i A_{a1a2}(t,t') B_{b2b1}(t',t)
+//   Bubble2: C_{c1c2}(t,t') = i A_{a1a2}(t,t') B_{b1b2}(t,t')
+// at time step tstp (tstp = -1: Matsubara, C(tau) = -sig_B A(tau) B(beta - tau) and
+// -A(tau) B(tau)); the continuations to t' > t come from the partners Acc, Bcc.
+void orc_bubble1(int tstp, orc_hm *Ch, int c1, int c2, orc_hm *Ah, orc_hm *Acch, int a1, int a2, orc_hm *Bh,
+                 orc_hm *Bcch, int b1, int b2) {
+    HM C(Ch), A(Ah), Acc(Acch), B(Bh), Bcc(Bcch);
+    const int ntau = C.ntau(), c12 = c1 * C.s + c2, a12 = a1 * A.s + a2, a21 = a2 * A.s + a1;
+    const int b12 = b1 * B.s + b2, b21 = b2 * B.s + b1;
+    if (tstp == -1) {
+        const double sg = -1.0 * B.sig();
+        for (int m = 0; m <= ntau; m++) C.matptr(m)[c12] = sg * A.matptr(m)[a12] * B.matptr(ntau - m)[b21];
+        return;
+    }
+    const cplx msigb = -1.0 * B.sig();
+    for (int m = 0; m <= tstp; m++) {
+        const cplx bles21_tt1 = -std::conj(Bcc.lesptr(m, tstp)[b12]);     // B^<_{21}(t, m)
+        const cplx bgtr21_tt1 = B.retptr(tstp, m)[b21] + bles21_tt1;        // B^>_{21}(t, m)
+        const cplx bles21_t1t = B.lesptr(m, tstp)[b21];                     // B^<_{21}(m, t)
+        const cplx bgtr21_t1t = -std::conj(Bcc.retptr(tstp, m)[b12]) + bles21_t1t;
+        const cplx ales12_tt1 = -std::conj(Acc.lesptr(m, tstp)[a21]);       // A^<_{12}(t, m)
+        const cplx agtr12_tt1 = A.retptr(tstp, m)[a12] + ales12_tt1;
+        C.retptr(tstp, m)[c12] = kI * agtr12_tt1 * bles21_t1t - kI * ales12_tt1 * bgtr21_t1t;
+        C.lesptr(m, tstp)[c12] = kI * A.lesptr(m, tstp)[a12] * bgtr21_tt1;
+    }
+    for (int m = 0; m <= ntau; m++) {
+        const cplx bvt21 = msigb * std::conj(Bcc.tvptr(tstp, ntau - m)[b12]);  // B^vt_{21}(m, t)
+        C.tvptr(tstp, m)[c12] = kI * A.tvptr(tstp, m)[a12] * bvt21;
+    }
+}
+
+void orc_bubble2(int tstp, orc_hm *Ch, int c1, int c2, orc_hm *Ah, orc_hm *Acch, int a1, int a2, orc_hm *Bh,
+                 orc_hm *Bcch, int b1, int b2) {
+    HM C(Ch), A(Ah), Acc(Acch), B(Bh), Bcc(Bcch);
+    const int ntau = C.ntau(), c12 = c1 * C.s + c2, a12 = a1 * A.s + a2, a21 = a2 * A.s + a1;
+    const int b12 = b1 * B.s + b2, b21 = b2 * B.s + b1;
+    if (tstp == -1) {
+        for (int m = 0; m <= ntau; m++) C.matptr(m)[c12] = -A.matptr(m)[a12] * B.matptr(m)[b12];
+        return;
+    }
+    for (int m = 0; m <= tstp; m++) {
+        const cplx bgtr12_tt1 = B.retptr(tstp, m)[b12] - std::conj(Bcc.lesptr(m, tstp)[b21]);
+        const cplx agtr12_tt1 = A.retptr(tstp, m)[a12] - std::conj(Acc.lesptr(m, tstp)[a21]);
+        const cplx cles_tt1 = kI * std::conj(Acc.lesptr(m, tstp)[a21]) * std::conj(Bcc.lesptr(m, tstp)[b21]);
+        C.retptr(tstp, m)[c12] = kI * agtr12_tt1 * bgtr12_tt1 - cles_tt1;
+        C.lesptr(m, tstp)[c12] = kI * A.lesptr(m, tstp)[a12] * B.lesptr(m, tstp)[b12];
+    }
+    for (int m = 0; m <= ntau; m++) C.tvptr(tstp, m)[c12] = kI * A.tvptr(tstp, m)[a12] * B.tvptr(tstp, m)[b12];
+}
+
 void orc_dyson_timestep_batch(int n0, int n1, int nprob, orc_hm *G, double mu, const cplx *H, long h_stride,
                               orc_hm *Sigma, int k, double beta, double h, int nthreads) {
     integ_init_all();  // integration::I is not thread-safe on first use (integration.hpp:506-514)

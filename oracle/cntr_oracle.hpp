@@ -77,6 +77,11 @@ void orc_force_matsubara_hermitian(orc_hm *G);
 // and C = i A(t,t') B(t,t') for scalar (1x1) functions.
 void orc_bubble1_scalar(int tstp, orc_hm *C, orc_hm *A, orc_hm *Acc, orc_hm *B, orc_hm *Bcc);
 void orc_bubble2_scalar(int tstp, orc_hm *C, orc_hm *A, orc_hm *Acc, orc_hm *B, orc_hm *Bcc);
+// element-index forms (cntr_bubble_impl.hpp:17-330): C_{c1c2} from A_{a1a2} and B_{b2b1} / B_{b1b2}
+void orc_bubble1(int tstp, orc_hm *C, int c1, int c2, orc_hm *A, orc_hm *Acc, int a1, int a2, orc_hm *B,
+                 orc_hm *Bcc, int b1, int b2);
+void orc_bubble2(int tstp, orc_hm *C, int c1, int c2, orc_hm *A, orc_hm *Acc, int a1, int a2, orc_hm *B,
+                 orc_hm *Bcc, int b1, int b2);
 
 // Self-consistent lattice with a local second-order self-energy (examples/programs/
 // hubbard_chain_selfen_impl.cpp:63-75, hubbard_chain_2b.cpp:245-324, with G -> G_loc, the

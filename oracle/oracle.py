@@ -63,6 +63,8 @@ def lib():
             "orc_force_matsubara_hermitian": (None, [P]),
             "orc_bubble1_scalar": (None, [i, P, P, P, P, P]),
             "orc_bubble2_scalar": (None, [i, P, P, P, P, P]),
+            "orc_bubble1": (None, [i, P, i, i, P, P, i, i, P, P, i, i]),
+            "orc_bubble2": (None, [i, P, i, i, P, P, i, i, P, P, i, i]),
             "orc_dyson_timestep_batch": (None, [i, i, i, P, d, vp, ctypes.c_long, P, i, d, d, i]),
             "orc_sigma_2b_timestep": (None, [i, P, P, vp]),
             "orc_gloc_timestep": (None, [i, i, P, P]),
@@ -212,6 +214,20 @@ def bubble2(tstp, C, A, Acc, B, Bcc):
     c, a, acc, b, bcc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
     lib().orc_bubble2_scalar(tstp, ctypes.byref(c), ctypes.byref(a), ctypes.byref(acc), ctypes.byref(b),
                              ctypes.byref(bcc))
+
+
+def bubble1_el(tstp, C, c, A, Acc, a, B, Bcc, b):
+    """C_{c1c2}(t,t') = i A_{a1a2}(t,t') B_{b2b1}(t',t) at tstp; c, a, b are index pairs."""
+    hc, ha, hac, hb, hbc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    lib().orc_bubble1(tstp, ctypes.byref(hc), c[0], c[1], ctypes.byref(ha), ctypes.byref(hac), a[0], a[1],
+                      ctypes.byref(hb), ctypes.byref(hbc), b[0], b[1])
+
+
+def bubble2_el(tstp, C, c, A, Acc, a, B, Bcc, b):
+    """C_{c1c2}(t,t') = i A_{a1a2}(t,t') B_{b1b2}(t,t') at tstp; c, a, b are index pairs."""
+    hc, ha, hac, hb, hbc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    lib().orc_bubble2(tstp, ctypes.byref(hc), c[0], c[1], ctypes.byref(ha), ctypes.byref(hac), a[0], a[1],
+                      ctypes.byref(hb), ctypes.byref(hbc), b[0], b[1])
 
 
 def dyson_timestep_batch(n0, n1, Gs, mu, Hs, Sigma, beta, h, k=5, nthreads=0):

@@ -141,3 +141,50 @@ def test_sigma_2b_of_rotated_free_levels(oracle):
         oracle.sigma_2b_timestep(t, S, G, u_matrices(U))
         err += distance_norm2(t, S, ref)
     assert err < 1e-8, err
+
+
+def _bubble_ref_el(kind, A, B, nt, ntau, h):
+    """Closed form of the element bubbles with c = a = b = (i, j) for every (i, j):
+    Bubble1 C_ij = i A_ij(t,t') B_ji(t',t), Bubble2 C_ij = i A_ij(t,t') B_ij(t,t')."""
+    s = len(A.w)
+    C = herm_matrix(nt, ntau, s, A.sg * B.sg)
+    beta = A.beta
+    Tr = lambda X: np.swapaxes(X, -1, -2)
+    taus = np.arange(ntau + 1) * (beta / ntau)
+    T, TAU = np.meshgrid(np.arange(nt + 1) * h, taus, indexing="ij")
+    a, b = tri_times(nt, h)
+    if kind == 1:
+        C.mat[...] = -A.mat(taus) * B.sg * Tr(B.mat(beta - taus))
+        C.tv[...] = II * A.tv(T, TAU) * Tr(B.vt(TAU, T))
+        C.ret[...] = II * A.gtr(a, b) * Tr(B.les(b, a)) - II * A.les(a, b) * Tr(B.gtr(b, a))
+        C.les[...] = II * A.les(b, a) * Tr(B.gtr(a, b))
+    else:
+        C.mat[...] = -A.mat(taus) * B.mat(taus)
+        C.tv[...] = II * A.tv(T, TAU) * B.tv(T, TAU)
+        C.ret[...] = II * A.gtr(a, b) * B.gtr(a, b) - II * A.les(a, b) * B.les(a, b)
+        C.les[...] = II * A.les(b, a) * B.les(b, a)
+    return C
+
+
+@pytest.mark.parametrize("kind", [1, 2])
+@pytest.mark.parametrize("sa,sb", [(-1, -1), (-1, 1), (1, -1), (1, 1)])
+def test_element_bubbles_of_rotated_free_levels(oracle, kind, sa, sb):
+    """libcntr/test/bubble.cpp:818-1161: 2 x 2 free propagators with levels (1.123, 0.567) and
+    (0.345, 0.876) rotated by 1 and 2 radians, nt = ntau = 50, beta = 0.5, h = 0.02; every
+    element bubble C_ij from A_ij and B_ji (Bubble1) or B_ij (Bubble2), all four Fermi/Bose
+    pairings, summed distance_norm2 < 1e-8."""
+    nt, ntau, beta, h = 50, 50, 0.5, 0.02
+    rot = lambda x: np.array([[np.cos(x), -np.sin(x)], [np.sin(x), np.cos(x)]])
+    A = FreeLevels([1.123, 0.567], sa, beta, rot(1.0))
+    B = FreeLevels([0.345, 0.876], sb, beta, rot(2.0))
+    GA, GB = A.herm_matrix(nt, ntau, h), B.herm_matrix(nt, ntau, h)
+    R = _bubble_ref_el(kind, A, B, nt, ntau, h)
+    C = herm_matrix(nt, ntau, 2, sa * sb)
+    f = oracle.bubble1_el if kind == 1 else oracle.bubble2_el
+    err = 0.0
+    for t in range(-1, nt + 1):
+        for i in range(2):
+            for j in range(2):
+                f(t, C, (i, j), GA, GA, (i, j), GB, GB, (i, j))
+        err += distance_norm2(t, C, R)
+    assert err < 1e-8, err
