@@ -230,6 +230,53 @@ def bubble2_el(tstp, C, c, A, Acc, a, B, Bcc, b):
                       ctypes.byref(hb), ctypes.byref(hbc), b[0], b[1])
 
 
+def add_kpoints(nk, k1, s1, k2, s2):
+    """Index of s1 k1 + s2 k2 on the 1-d grid k_i = (i - nk/2) 2 pi / nk (gw_latt_impl.cpp:46-51)."""
+    g = nk // 2
+    return (s1 * (k1 - g) + s2 * (k2 - g) + g) % nk
+
+
+def _zero_timestep(G, tstp):
+    if tstp == -1:
+        G.mat[...] = 0
+    else:
+        G.ret_row(tstp)[...] = 0
+        G.tv[tstp] = 0
+        G.les_col(tstp)[...] = 0
+
+
+def gw_polarization_timestep(tstp, P, q, Gs, weights):
+    """get_Polarization_Bubble (examples/programs/gw_selfene_impl.cpp:133-153):
+    P_q(tstp) = -sum_k w_k Bubble1(G_{k-q}, G_k), element by element (a1 a2 = b1 b2 = c1 c2)."""
+    from nessi_b200 import herm_matrix
+    s = P.size1
+    _zero_timestep(P, tstp)
+    tmp = herm_matrix(P.nt, P.ntau, s, P.sig)
+    for kk in range(len(Gs)):
+        kq = add_kpoints(len(Gs), kk, 1, q, -1)
+        _zero_timestep(tmp, tstp)
+        for i1 in range(s):
+            for i2 in range(s):
+                bubble1_el(tstp, tmp, (i1, i2), Gs[kq], Gs[kq], (i1, i2), Gs[kk], Gs[kk], (i1, i2))
+        P.incr_timestep(tstp, tmp, -weights[kk])
+
+
+def gw_sigma_timestep(tstp, S, kk, Gs, Ws, weights):
+    """sigma_GW (examples/programs/gw_selfene_impl.cpp:114-131):
+    Sigma_k(tstp) = sum_q w_q Bubble2(G_{k-q}, W_q), element by element."""
+    from nessi_b200 import herm_matrix
+    s = S.size1
+    _zero_timestep(S, tstp)
+    tmp = herm_matrix(S.nt, S.ntau, s, S.sig)
+    for q in range(len(Ws)):
+        kq = add_kpoints(len(Gs), kk, 1, q, -1)
+        _zero_timestep(tmp, tstp)
+        for i1 in range(s):
+            for i2 in range(s):
+                bubble2_el(tstp, tmp, (i1, i2), Gs[kq], Gs[kq], (i1, i2), Ws[q], Ws[q], (i1, i2))
+        S.incr_timestep(tstp, tmp, weights[q])
+
+
 def dyson_timestep_batch(n0, n1, Gs, mu, Hs, Sigma, beta, h, k=5, nthreads=0):
     """Time steps n0..n1 for every problem in ``Gs`` (shared Sigma), OpenMP over problems.
     ``Hs`` is an array (nprob, nt+2, s, s)."""
