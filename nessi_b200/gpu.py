@@ -488,3 +488,61 @@ def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None):
     finally:
         b.close()
     G.mat[...] = 0.5 * (out.mat + out.mat.conj().transpose(0, 2, 1))  # force_matsubara_hermitian
+
+
+def vie2_timestep_sin(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, SolveOrder=5):
+    """cntr::vie2_timestep_sin(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, SolveOrder)
+    (cntr_vie2_decl.hpp:58, cntr_vie2_impl.hpp:1779-1838): [1 + F] G = Q where F, Q and G carry
+    instantaneous parts Fsin, Qsin, Gsin (cntr::function).  The time-local algebra runs on the
+    host as in the reference: for t = -1..n2 (n2 = max(n, k) in the start region),
+    Finv = (1 + Fsin)^-1, Gsin = Finv Qsin, F -> Finv F, Fcc -> Fcc Finv, Q -> Finv Q - (Finv F) Gsin;
+    the Volterra solve runs on the GPU: vie2_mat for n = -1, a start of order n for 1 <= n <= k
+    (time steps 0..n), vie2_timestep for n > k.  n = 0 (an order-0 start) is not available."""
+    k = SolveOrder
+    if n == 0:
+        raise NessiGpuError(1, "vie2_timestep_sin: n = 0 needs an order-0 start, which is not available")
+    if n < -1 or n > G.nt:
+        raise NessiGpuError(1, "vie2_timestep_sin: time step %d out of range" % n)
+    s, nt, ntau, sig = G.size1, G.nt, G.ntau, G.sig
+    n2 = k if 0 <= n <= k else n
+    fs = Fsin.data if isinstance(Fsin, function) else np.asarray(Fsin)
+    qs = Qsin.data if isinstance(Qsin, function) else np.asarray(Qsin)
+    gs = Gsin.data if isinstance(Gsin, function) else Gsin
+    finv = np.zeros((nt + 2, s, s), np.complex128)
+    finv[:n2 + 2] = np.linalg.inv(np.eye(s) + fs[:n2 + 2])
+    gs[:n2 + 2] = finv[:n2 + 2] @ qs[:n2 + 2]
+    tF, tFcc, tQ = F.copy(), Fcc.copy(), Q.copy()
+    for t in range(-1, n2 + 1):
+        tF.left_multiply(t, finv)
+        tFcc.right_multiply(t, finv)
+        tQ.left_multiply(t, finv)
+    tF1 = tF.copy()
+    for t in range(-1, n2 + 1):
+        tF1.right_multiply(t, gs)
+        tQ.incr_timestep(t, tF1, -1.0)
+    order = n if 1 <= n <= k else k
+    b = Batch([dict(nt=nt, ntau=ntau, size1=s, sig=sig, solve_order=order, beta=beta, h=h)])
+    try:
+        b.set_G(0, G)
+        b.set_F(0, tF, tFcc)
+        b.set_Q(0, tQ)
+        if n == -1:
+            b.vie2_mat()
+            steps = [-1]
+        elif n <= k:
+            b.vie2_start()
+            steps = list(range(0, n + 1))
+        else:
+            b.vie2_timestep(n)
+            steps = [n]
+        for t in steps:
+            out = np.zeros((_slice_len(t, ntau), s, s), np.complex128)
+            b.get_timestep(0, t, out)
+            G.set_timestep_data(t, out)
+    finally:
+        b.close()
+
+
+def _slice_len(t, ntau):
+    """Elements of time step t's slice: ret row, tv row and les column, or mat for t = -1."""
+    return ntau + 1 if t < 0 else 2 * (t + 1) + ntau + 1

@@ -118,6 +118,29 @@ class herm_matrix:
             self.tv[tstp] += alpha * other.tv[tstp]
             self.les_col(tstp)[...] += alpha * other.les_col(tstp)
 
+    def left_multiply(self, tstp, f, weight=1.0):
+        """C(t,t') -> weight f(t) C(t,t') at time step tstp (cntr_herm_matrix_impl.hpp:2955-2995):
+        f(-1) on mat, f(tstp) on ret(tstp, .) and tv(tstp, .), f(m) on les(m, tstp).  ``f`` is a
+        cntr::function or its (nt+2, s, s) data, t = -1 first."""
+        F = f.data if isinstance(f, function) else np.asarray(f)
+        if tstp == -1:
+            self.mat[...] = weight * np.einsum("ab,mbc->mac", F[0], self.mat)
+            return
+        self.ret_row(tstp)[...] = weight * np.einsum("ab,mbc->mac", F[tstp + 1], self.ret_row(tstp))
+        self.tv[tstp] = weight * np.einsum("ab,mbc->mac", F[tstp + 1], self.tv[tstp])
+        self.les_col(tstp)[...] = weight * np.einsum("mab,mbc->mac", F[1:tstp + 2], self.les_col(tstp))
+
+    def right_multiply(self, tstp, f, weight=1.0):
+        """C(t,t') -> weight C(t,t') f(t') at time step tstp (cntr_herm_matrix_impl.hpp:3206-3246):
+        f(-1) on mat and tv(tstp, .), f(m) on ret(tstp, m), f(tstp) on les(m, tstp)."""
+        F = f.data if isinstance(f, function) else np.asarray(f)
+        if tstp == -1:
+            self.mat[...] = weight * np.einsum("mab,bc->mac", self.mat, F[0])
+            return
+        self.ret_row(tstp)[...] = weight * np.einsum("mab,mbc->mac", self.ret_row(tstp), F[1:tstp + 2])
+        self.tv[tstp] = weight * np.einsum("mab,bc->mac", self.tv[tstp], F[0])
+        self.les_col(tstp)[...] = weight * np.einsum("mab,bc->mac", self.les_col(tstp), F[tstp + 1])
+
     def set_matrixelement(self, tstp, i1, i2, other, j1=0, j2=0):
         """self(i1,i2) <- other(j1,j2) at one time step (cntr_herm_matrix_impl.hpp set_matrixelement)."""
         if tstp == -1:

@@ -1611,6 +1611,88 @@ void orc_vie2_timestep(int n, orc_hm *Gh, orc_hm *Fh, orc_hm *Fcch, orc_hm *Qh, 
     ORC_DISPATCH(vie2_timestep_les_t, n, G, F, Fcc, Q, In, beta, h);
 }
 
+// vie2_timestep_sin (cntr_vie2_impl.hpp:1779-1838): [1 + F] G = Q where F and Q carry
+// instantaneous parts Fsin, Qsin (cntr::function data, (nt+2) blocks, t = -1 first).  For
+// t = -1..n2: Finv(t) = (1 + Fsin(t))^-1 and Gsin(t) = Finv Qsin; the regular equation is
+// [1 + Finv F] G = Finv Q - (Finv F) Gsin with Fcc -> Fcc Finv, solved by vie2_timestep
+// (whose dispatch gives vie2_mat for n = -1 and a start of order n for n <= k).
+void orc_vie2_timestep_sin(int n, orc_hm *Gh, cplx *Gsin, orc_hm *Fh, orc_hm *Fcch, const cplx *Fsin, orc_hm *Qh,
+                           const cplx *Qsin, int k, double beta, double h) {
+    const int s = Fh->size, es = s * s, nt = Fh->nt, ntau = Fh->ntau;
+    const int n2 = (n <= k && n >= 0) ? k : n;
+    std::vector<cplx> finv((long)(n2 + 2) * es), id(es, cplx(0)), onef(es);
+    for (int i = 0; i < s; i++) id[i * s + i] = 1.0;
+    auto mul = [&](cplx *z, const cplx *a, const cplx *b) {  // z = a b (s x s), z may not alias
+        for (int i = 0; i < s; i++)
+            for (int j = 0; j < s; j++) {
+                cplx x = 0;
+                for (int l = 0; l < s; l++) x += a[i * s + l] * b[l * s + j];
+                z[i * s + j] = x;
+            }
+    };
+    for (int t = -1; t <= n2; t++) {
+        const cplx *fs = Fsin + (long)(t + 1) * es;
+        for (int i = 0; i < es; i++) onef[i] = fs[i] + id[i];
+        cplx *fi = finv.data() + (long)(t + 1) * es;
+        orc_cplx_solve(s, s, onef.data(), id.data(), fi);
+        mul(Gsin + (long)(t + 1) * es, fi, Qsin + (long)(t + 1) * es);
+    }
+    // working copies of F, Fcc, Q
+    const long nret = nt >= 0 ? (long)(nt + 1) * (nt + 2) / 2 * es : 0, ntv = (long)(nt + 1) * (ntau + 1) * es,
+               nmat = (long)(ntau + 1) * es;
+    auto clone = [&](orc_hm *X, std::vector<cplx> &buf) {
+        buf.assign(2 * nret + ntv + nmat, cplx(0));
+        if (nret) std::copy(X->ret, X->ret + nret, buf.begin());
+        if (nret) std::copy(X->les, X->les + nret, buf.begin() + nret);
+        if (ntv) std::copy(X->tv, X->tv + ntv, buf.begin() + 2 * nret);
+        std::copy(X->mat, X->mat + nmat, buf.begin() + 2 * nret + ntv);
+        orc_hm v = {nt, ntau, s, X->sig, buf.data(), buf.data() + nret, buf.data() + 2 * nret,
+                    buf.data() + 2 * nret + ntv};
+        return v;
+    };
+    std::vector<cplx> bF, bFcc, bQ, bF1, tmp(es);
+    orc_hm tF = clone(Fh, bF), tFcc = clone(Fcch, bFcc), tQ = clone(Qh, bQ);
+    // herm_matrix::left_multiply / right_multiply at one time step (cntr_herm_matrix_impl.hpp:
+    // 2955-2995, 3206-3246): f(-1) on mat, f(t) / f(m) on the slice as the time arguments say
+    auto lmul = [&](orc_hm *X, int t, const cplx *f) {
+        HM x(X);
+        auto fp = [&](int tt) { return f + (long)(tt + 1) * es; };
+        auto app = [&](cplx *e, const cplx *fa) { mul(tmp.data(), fa, e); std::copy(tmp.begin(), tmp.end(), e); };
+        if (t == -1) { for (int m = 0; m <= ntau; m++) app(x.matptr(m), fp(-1)); return; }
+        for (int m = 0; m <= t; m++) app(x.retptr(t, m), fp(t));
+        for (int m = 0; m <= ntau; m++) app(x.tvptr(t, m), fp(t));
+        for (int m = 0; m <= t; m++) app(x.lesptr(m, t), fp(m));
+    };
+    auto rmul = [&](orc_hm *X, int t, const cplx *f) {
+        HM x(X);
+        auto fp = [&](int tt) { return f + (long)(tt + 1) * es; };
+        auto app = [&](cplx *e, const cplx *fa) { mul(tmp.data(), e, fa); std::copy(tmp.begin(), tmp.end(), e); };
+        if (t == -1) { for (int m = 0; m <= ntau; m++) app(x.matptr(m), fp(-1)); return; }
+        for (int m = 0; m <= t; m++) app(x.retptr(t, m), fp(m));
+        for (int m = 0; m <= ntau; m++) app(x.tvptr(t, m), fp(-1));
+        for (int m = 0; m <= t; m++) app(x.lesptr(m, t), fp(t));
+    };
+    for (int t = -1; t <= n2; t++) {
+        lmul(&tF, t, finv.data());
+        rmul(&tFcc, t, finv.data());
+        lmul(&tQ, t, finv.data());
+    }
+    orc_hm tF1 = clone(&tF, bF1);
+    for (int t = -1; t <= n2; t++) rmul(&tF1, t, Gsin);
+    // tQ(t) -= tF1(t) on the time steps -1..n2 (herm_matrix::incr_timestep)
+    for (int t = -1; t <= n2; t++) {
+        HM q(&tQ), f1(&tF1);
+        if (t == -1) {
+            for (long i = 0; i < nmat; i++) q.matptr(0)[i] -= f1.matptr(0)[i];
+            continue;
+        }
+        for (long i = 0; i < (long)(t + 1) * es; i++) q.retptr(t, 0)[i] -= f1.retptr(t, 0)[i];
+        for (long i = 0; i < (long)(ntau + 1) * es; i++) q.tvptr(t, 0)[i] -= f1.tvptr(t, 0)[i];
+        for (long i = 0; i < (long)(t + 1) * es; i++) q.lesptr(0, t)[i] -= f1.lesptr(0, t)[i];
+    }
+    orc_vie2_timestep(n, Gh, &tF, &tFcc, &tQ, k, beta, h, 2);
+}
+
 void orc_extrapolate_timestep(int n, orc_hm *Gh, int k) {
     HM G(Gh);
     int s1 = G.s;

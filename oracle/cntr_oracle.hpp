@@ -67,6 +67,9 @@ void orc_vie2_mat(orc_hm *G, orc_hm *F, orc_hm *Fcc, orc_hm *Q, double beta, int
 void orc_vie2_start(orc_hm *G, orc_hm *F, orc_hm *Fcc, orc_hm *Q, int k, double beta, double h);
 void orc_vie2_timestep(int n, orc_hm *G, orc_hm *F, orc_hm *Fcc, orc_hm *Q, int k, double beta,
                        double h, int method);
+// vie2_timestep_sin (cntr_vie2_impl.hpp:1779-1838): Fsin, Qsin, Gsin are (nt+2) s x s blocks.
+void orc_vie2_timestep_sin(int n, orc_hm *G, ocplx *Gsin, orc_hm *F, orc_hm *Fcc, const ocplx *Fsin, orc_hm *Q,
+                           const ocplx *Qsin, int k, double beta, double h);
 
 // Utilities (cntr_utilities_impl.hpp:22-170, 607-650, 2077-2110).
 void orc_extrapolate_timestep(int n, orc_hm *G, int k);

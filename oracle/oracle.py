@@ -63,6 +63,7 @@ def lib():
             "orc_force_matsubara_hermitian": (None, [P]),
             "orc_bubble1_scalar": (None, [i, P, P, P, P, P]),
             "orc_bubble2_scalar": (None, [i, P, P, P, P, P]),
+            "orc_vie2_timestep_sin": (None, [i, P, vp, P, P, vp, P, vp, i, d, d]),
             "orc_bubble1": (None, [i, P, i, i, P, P, i, i, P, P, i, i]),
             "orc_bubble2": (None, [i, P, i, i, P, P, i, i, P, P, i, i]),
             "orc_dyson_timestep_batch": (None, [i, i, i, P, d, vp, ctypes.c_long, P, i, d, d, i]),
@@ -187,6 +188,17 @@ def vie2_timestep(n, G, F, Fcc, Q, beta, h, k=5, method=CNTR_MAT_FIXPOINT):
     g, f, fc, q = hm(G), hm(F), hm(Fcc), hm(Q)
     lib().orc_vie2_timestep(n, ctypes.byref(g), ctypes.byref(f), ctypes.byref(fc), ctypes.byref(q), k, beta, h,
                             method)
+
+
+def vie2_timestep_sin(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, k=5):
+    """cntr::vie2_timestep_sin (cntr_vie2_impl.hpp:1779-1838); Gsin, Fsin, Qsin are cntr::function
+    objects (or their (nt+2, s, s) data); Gsin is written for t = -1..max(n, k)."""
+    g, f, fc, q = hm(G), hm(F), hm(Fcc), hm(Q)
+    arr = lambda X: X.data if hasattr(X, "data") and not isinstance(X, np.ndarray) else X
+    gs, fs, qs = arr(Gsin), np.ascontiguousarray(arr(Fsin), np.complex128), np.ascontiguousarray(arr(Qsin), np.complex128)
+    assert gs.dtype == np.complex128 and gs.flags["C_CONTIGUOUS"]
+    lib().orc_vie2_timestep_sin(n, ctypes.byref(g), gs.ctypes.data, ctypes.byref(f), ctypes.byref(fc),
+                                fs.ctypes.data, ctypes.byref(q), qs.ctypes.data, k, beta, h)
 
 
 def extrapolate_timestep(n, G, k=5):

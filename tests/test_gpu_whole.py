@@ -109,3 +109,27 @@ def test_dyson_mat_mean_field_overload(oracle, s):
     alt = herm_matrix(-1, ntau, s, -1)
     oracle.dyson_mat(alt, Sig, mu, Hmf, beta, k)
     assert rel_err(G.mat, alt.mat) < 1e-9    # the two formulations agree to the fixpoint's convergence
+
+
+def test_vie2_timestep_sin(oracle):
+    """gpu.vie2_timestep_sin through a propagation (n = -1, the start at n = k, then every step)
+    against the oracle's restatement of cntr_vie2_impl.hpp:1779-1838, regular part and Gsin."""
+    from nessi_b200 import function, gpu
+    rng = np.random.default_rng(81)
+    nt, ntau, beta, h, k, s = 14, 12, 3.0, 0.05, 5, 2
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Q = _source(oracle, rng, nt, ntau, s, beta, h)
+    Fsin, Qsin = function(nt, s), function(nt, s)
+    for t in range(-1, nt + 1):
+        Fsin.set_value(t, 0.3 * (rng.normal(size=(s, s)) + 1j * rng.normal(size=(s, s))))
+        Qsin.set_value(t, rng.normal(size=(s, s)) + 1j * rng.normal(size=(s, s)))
+    runs = []
+    for f in (gpu.vie2_timestep_sin, oracle.vie2_timestep_sin):
+        G, Gsin = herm_matrix(nt, ntau, s, -1), function(nt, s)
+        for n in [-1, k] + list(range(k + 1, nt + 1)):
+            f(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, k)
+        runs.append((G, Gsin))
+    (G, Gs), (R, Rs) = runs
+    assert rel_err(Gs.data, Rs.data) < 1e-13
+    for c in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(G, c), getattr(R, c)) < TOL, c
