@@ -345,6 +345,114 @@ void vie2_timestep(int n, HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, i
     check(rc);
 }
 
+// ---- vie2_timestep_sin (cntr_vie2_decl.hpp:58, cntr_vie2_impl.hpp:1779-1838) ------------------
+namespace detail {
+typedef std::complex<double> cplx;
+// z = a b for s x s row-major blocks (z must not alias a or b)
+inline void mat_mul(int s, cplx *z, const cplx *a, const cplx *b) {
+    for (int i = 0; i < s; i++)
+        for (int j = 0; j < s; j++) {
+            cplx x = 0;
+            for (int l = 0; l < s; l++) x += a[i * s + l] * b[l * s + j];
+            z[i * s + j] = x;
+        }
+}
+// inv = a^-1 by Gauss-Jordan elimination with partial pivoting; false if a is singular
+inline bool mat_inverse(int s, const cplx *a, cplx *inv) {
+    std::vector<cplx> m(a, a + s * s);
+    for (int i = 0; i < s * s; i++) inv[i] = (i / s == i % s) ? 1.0 : 0.0;
+    for (int c = 0; c < s; c++) {
+        int p = c;
+        for (int r = c + 1; r < s; r++)
+            if (std::abs(m[r * s + c]) > std::abs(m[p * s + c])) p = r;
+        if (std::abs(m[p * s + c]) == 0.0) return false;
+        for (int j = 0; j < s; j++) {
+            std::swap(m[c * s + j], m[p * s + j]);
+            std::swap(inv[c * s + j], inv[p * s + j]);
+        }
+        const cplx d = 1.0 / m[c * s + c];
+        for (int j = 0; j < s; j++) { m[c * s + j] *= d; inv[c * s + j] *= d; }
+        for (int r = 0; r < s; r++) {
+            if (r == c) continue;
+            const cplx f = m[r * s + c];
+            for (int j = 0; j < s; j++) { m[r * s + j] -= f * m[c * s + j]; inv[r * s + j] -= f * inv[c * s + j]; }
+        }
+    }
+    return true;
+}
+// herm_matrix::left_multiply / right_multiply at time step t with f given as blocks f(-1), f(0), ...
+// (cntr_herm_matrix_impl.hpp:2955-2995, 3206-3246)
+template <class HM> void left_multiply(HM &X, int t, const cplx *f) {
+    const int s = X.size1(), es = s * s;
+    std::vector<cplx> z(es);
+    auto fp = [&](int tt) { return f + (long)(tt + 1) * es; };
+    auto app = [&](cplx *e, const cplx *fa) { mat_mul(s, z.data(), fa, e); std::copy(z.begin(), z.end(), e); };
+    if (t == -1) {
+        for (int m = 0; m <= X.ntau(); m++) app(X.matptr(m), fp(-1));
+        return;
+    }
+    for (int m = 0; m <= t; m++) app(X.retptr(t, m), fp(t));
+    for (int m = 0; m <= X.ntau(); m++) app(X.tvptr(t, m), fp(t));
+    for (int m = 0; m <= t; m++) app(X.lesptr(m, t), fp(m));
+}
+template <class HM> void right_multiply(HM &X, int t, const cplx *f) {
+    const int s = X.size1(), es = s * s;
+    std::vector<cplx> z(es);
+    auto fp = [&](int tt) { return f + (long)(tt + 1) * es; };
+    auto app = [&](cplx *e, const cplx *fa) { mat_mul(s, z.data(), e, fa); std::copy(z.begin(), z.end(), e); };
+    if (t == -1) {
+        for (int m = 0; m <= X.ntau(); m++) app(X.matptr(m), fp(-1));
+        return;
+    }
+    for (int m = 0; m <= t; m++) app(X.retptr(t, m), fp(m));
+    for (int m = 0; m <= X.ntau(); m++) app(X.tvptr(t, m), fp(-1));
+    for (int m = 0; m <= t; m++) app(X.lesptr(m, t), fp(t));
+}
+// X(t) -= Y(t) on time step t
+template <class HM> void decr_timestep(HM &X, HM &Y, int t) {
+    const long es = (long)X.size1() * X.size1();
+    auto sub = [&](cplx *x, const cplx *y, long n) { for (long i = 0; i < n; i++) x[i] -= y[i]; };
+    if (t == -1) { sub(X.matptr(0), Y.matptr(0), (X.ntau() + 1) * es); return; }
+    sub(X.retptr(t, 0), Y.retptr(t, 0), (t + 1) * es);
+    sub(X.tvptr(t, 0), Y.tvptr(t, 0), (X.ntau() + 1) * es);
+    sub(X.lesptr(0, t), Y.lesptr(0, t), (t + 1) * es);
+}
+}  // namespace detail
+
+// [1 + F] G = Q where F, Q and G carry instantaneous parts Fsin, Qsin, Gsin: the time-local
+// algebra on the host as in the reference (Finv = (1 + Fsin)^-1, Gsin = Finv Qsin, F -> Finv F,
+// Fcc -> Fcc Finv, Q -> Finv Q - (Finv F) Gsin on t = -1..max(n, k)), then vie2_timestep's
+// dispatch on the device.  HM must be copyable (libcntr's herm_matrix is).
+template <class HM, class FN>
+void vie2_timestep_sin(int n, HM &G, FN &Gsin, HM &F, HM &Fcc, FN &Fsin, HM &Q, FN &Qsin, double beta, double h,
+                       int SolveOrder = 5) {
+    if (n == 0) throw std::invalid_argument("cntr_gpu::vie2_timestep_sin: an order-0 start (n = 0) is not available");
+    const int s = G.size1(), es = s * s;
+    const int n2 = (n >= 0 && n <= SolveOrder) ? SolveOrder : n;
+    std::vector<detail::cplx> finv((long)(n2 + 2) * es), gsin((long)(n2 + 2) * es), a(es);
+    for (int t = -1; t <= n2; t++) {
+        const detail::cplx *fs = Fsin.ptr(t);
+        for (int i = 0; i < es; i++) a[i] = fs[i] + ((i / s == i % s) ? 1.0 : 0.0);
+        detail::cplx *fi = finv.data() + (long)(t + 1) * es, *gs = gsin.data() + (long)(t + 1) * es;
+        if (!detail::mat_inverse(s, a.data(), fi))
+            throw std::runtime_error("cntr_gpu::vie2_timestep_sin: 1 + Fsin is singular");
+        detail::mat_mul(s, gs, fi, Qsin.ptr(t));
+        std::copy(gs, gs + es, Gsin.ptr(t));
+    }
+    HM tF(F), tFcc(Fcc), tQ(Q);
+    for (int t = -1; t <= n2; t++) {
+        detail::left_multiply(tF, t, finv.data());
+        detail::right_multiply(tFcc, t, finv.data());
+        detail::left_multiply(tQ, t, finv.data());
+    }
+    HM tF1(tF);
+    for (int t = -1; t <= n2; t++) {
+        detail::right_multiply(tF1, t, gsin.data());
+        detail::decr_timestep(tQ, tF1, t);
+    }
+    vie2_timestep(n, G, tF, tFcc, tQ, beta, h, SolveOrder);
+}
+
 // ---- convolution_timestep / convolution (cntr_convolution_decl.hpp:59-68) ----------------
 template <class HM> inline nessi_hm_ptrs hm_ptrs(HM &X) {
     nessi_hm_ptrs q;

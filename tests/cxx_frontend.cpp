@@ -2,7 +2,7 @@
 // herm_matrix / function pair with libcntr's accessors and layout, filled from raw files
 // (complex128, libcntr layout), one cntr_gpu call, the result written back.
 //
-//   cxx_frontend <mode> <dir>      mode: echo | mat | dyson | steps | vie2 | conv
+//   cxx_frontend <mode> <dir>      mode: echo | algebra | mat | dyson | steps | vie2 | sin | conv
 //
 // Files in <dir>: dims.txt ("nt ntau size1 sig k beta h mu"), and <name>.{ret,les,tv,mat}
 // for the herm_matrix operands (H.fn for the function).  The result is G (or C).
@@ -69,7 +69,7 @@ static void save_hm(const HM &G, const std::string &base) {
 
 int main(int argc, char **argv) {
     if (argc != 3) {
-        std::fprintf(stderr, "usage: %s echo|mat|dyson|steps|vie2|conv <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s echo|algebra|mat|dyson|steps|vie2|sin|conv <dir>\n", argv[0]);
         return 2;
     }
     const std::string mode = argv[1], dir = std::string(argv[2]) + "/";
@@ -87,6 +87,23 @@ int main(int argc, char **argv) {
         if (mode == "echo") {  // the file handling alone (no device)
             load_hm(G, dir + "A");
             save_hm(G, dir + "out");
+        } else if (mode == "algebra") {  // the host algebra of vie2_timestep_sin (no device)
+            HM L(nt, ntau, s, sig), R(nt, ntau, s, sig);
+            FN f(nt, s), inv(nt, s);
+            load_hm(L, dir + "A");
+            load_hm(R, dir + "A");
+            load(f.d_, dir + "f.fn");
+            for (int t = -1; t <= nt; t++) {
+                cntr_gpu::detail::left_multiply(L, t, f.ptr(-1));
+                cntr_gpu::detail::right_multiply(R, t, f.ptr(-1));
+                std::vector<cplx> a(f.ptr(t), f.ptr(t) + s * s);
+                for (int i = 0; i < s; i++) a[i * s + i] += 1.0;
+                if (!cntr_gpu::detail::mat_inverse(s, a.data(), inv.ptr(t))) throw std::runtime_error("singular");
+            }
+            cntr_gpu::detail::decr_timestep(L, R, 2);
+            save_hm(L, dir + "out");
+            save_hm(R, dir + "outR");
+            save(inv.d_, dir + "inv.fn");
         } else if (mode == "mat") {  // cntr::dyson_mat, also for a Matsubara-only G (nt = -1)
             HM Sigma(nt, ntau, s, sig);
             FN H(nt, s);
@@ -116,6 +133,18 @@ int main(int argc, char **argv) {
             cntr_gpu::vie2_start(G, F, Fcc, Q, beta, h, k);
             for (int n = k + 1; n <= nt; n++) cntr_gpu::vie2_timestep(n, G, F, Fcc, Q, beta, h, k);
             save_hm(G, dir + "out");
+        } else if (mode == "sin") {  // vie2_timestep_sin through a propagation
+            HM F(nt, ntau, s, sig), Fcc(nt, ntau, s, sig), Q(nt, ntau, s, sig);
+            FN Fsin(nt, s), Qsin(nt, s), Gsin(nt, s);
+            load_hm(F, dir + "F");
+            load_hm(Fcc, dir + "Fcc");
+            load_hm(Q, dir + "Q");
+            load(Fsin.d_, dir + "Fsin.fn");
+            load(Qsin.d_, dir + "Qsin.fn");
+            cntr_gpu::vie2_timestep_sin(-1, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, k);
+            for (int n = k; n <= nt; n++) cntr_gpu::vie2_timestep_sin(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, k);
+            save_hm(G, dir + "out");
+            save(Gsin.d_, dir + "out.fn");
         } else if (mode == "conv") {
             HM A(nt, ntau, s, sig), Acc(nt, ntau, s, sig), B(nt, ntau, s, sig);
             load_hm(A, dir + "A");

@@ -71,6 +71,64 @@ def test_file_handling_without_device(tmp_path, nt):
         assert np.array_equal(getattr(A, c), getattr(B, c))
 
 
+def test_vie2_sin_host_algebra_without_device(tmp_path):
+    """The host half of cntr_gpu::vie2_timestep_sin (mode algebra, no GPU): left and right
+    multiplication by a function at every time step, the inverses of 1 + f(t), and the slice
+    subtraction, against the Python herm_matrix and numpy."""
+    from nessi_b200 import function
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(5)
+    nt, ntau, s = 6, 4, 3
+    A = herm_matrix(nt, ntau, s, -1)
+    for c in ("ret", "les", "tv", "mat"):
+        a = getattr(A, c)
+        a[...] = rng.normal(size=a.shape) + 1j * rng.normal(size=a.shape)
+    f = function(nt, s)
+    f.data[...] = 0.4 * (rng.normal(size=f.data.shape) + 1j * rng.normal(size=f.data.shape))
+    d = tmp_path / "algebra"
+    write_case(d, (nt, ntau, s, -1, 5, 1.0, 0.1, 0.0), A=A, f=f.data)
+    run(exe, "algebra", d)
+    L, R = A.copy(), A.copy()
+    for t in range(-1, nt + 1):
+        L.left_multiply(t, f)
+        R.right_multiply(t, f)
+    L.incr_timestep(2, R, -1.0)
+    got_R = herm_matrix(nt, ntau, s, -1)
+    for c in ("ret", "les", "tv", "mat"):
+        a = getattr(got_R, c)
+        a[...] = np.fromfile(str(d / ("outR." + c)), np.complex128).reshape(a.shape)
+    got_L = read_out(d, nt, ntau, s, -1)
+    for c in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(got_L, c), getattr(L, c)) < 1e-14, c
+        assert rel_err(getattr(got_R, c), getattr(R, c)) < 1e-14, c
+    inv = np.fromfile(str(d / "inv.fn"), np.complex128).reshape(f.data.shape)
+    assert rel_err(inv, np.linalg.inv(np.eye(s) + f.data)) < 1e-13
+
+
+@pytest.mark.gpu
+def test_vie2_timestep_sin_through_the_cxx_frontend(oracle, tmp_path):
+    from nessi_b200 import function
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(59)
+    nt, ntau, s, beta, h, k = 14, 12, 2, 3.0, 0.05, 5
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Q = _source(oracle, rng, nt, ntau, s, beta, h)
+    Fsin, Qsin = function(nt, s), function(nt, s)
+    Fsin.data[...] = 0.3 * (rng.normal(size=Fsin.data.shape) + 1j * rng.normal(size=Fsin.data.shape))
+    Qsin.data[...] = rng.normal(size=Qsin.data.shape) + 1j * rng.normal(size=Qsin.data.shape)
+    R, Rsin = herm_matrix(nt, ntau, s, -1), function(nt, s)
+    for n in [-1] + list(range(k, nt + 1)):
+        oracle.vie2_timestep_sin(n, R, Rsin, F, Fcc, Fsin, Q, Qsin, beta, h, k)
+    d = tmp_path / "sin"
+    write_case(d, (nt, ntau, s, -1, k, beta, h, 0.0), F=F, Fcc=Fcc, Q=Q, Fsin=Fsin.data, Qsin=Qsin.data)
+    run(exe, "sin", d)
+    G = read_out(d, nt, ntau, s, -1)
+    Gsin = np.fromfile(str(d / "out.fn"), np.complex128).reshape(Rsin.data.shape)
+    assert rel_err(Gsin, Rsin.data) < 1e-13
+    for c in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(G, c), getattr(R, c)) < TOL, c
+
+
 @pytest.mark.gpu
 def test_dyson_mat_of_a_matsubara_only_matrix(oracle, tmp_path):
     """cntr_gpu::dyson_mat on herm_matrix(-1, ntau, 2, -1), as libcntr programs call it for the
