@@ -1,4 +1,4 @@
-// A libcntr-style program on include/cntr_gpu.hpp, for tests/test_gpu_cxx_frontend.py: a
+// A libcntr-style program on include/cntr_gpu.hpp, for tests/test_gpu_whole_cxx.py: a
 // herm_matrix / function pair with libcntr's accessors and layout, filled from raw files
 // (complex128, libcntr layout), one cntr_gpu call, the result written back.
 //
