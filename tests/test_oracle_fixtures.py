@@ -157,3 +157,46 @@ def test_convolution_bosonic_boundary_signs(oracle):
         errs.append(O.distance_norm2(nt, C, AB))
     assert errs[-1] < 1e-6, errs            # convolution.cpp:142 (eps)
     assert errs[-1] < errs[0]
+
+
+def test_downfolding_of_a_three_level_system(oracle):
+    """libcntr/test/downfold.cpp:367-427 (time-independent): the (0,0) element of the free 3 x 3
+    propagator of a = [[1, -1, -1], [-1, 2, -1], [-1, -1, 3]] (the e^{+-i pi} couplings), from the
+    embedded 1 x 1 problem: G0 the zero-level propagator, eta = a_{0R} G_RR a_{R0} with G_RR the
+    free propagator of the 2 x 2 rest, F = -(G0 * eta) - G0 a_00, Fcc = -(eta * G0) - a_00 G0,
+    [1 + F] G = G0 by vie2 (nt = 20, ntau = 300, beta = 1, h = 0.01, order 5); the reference
+    accepts a summed distance below 1e-6."""
+    O = oracle
+    nt, ntau, beta, h, k = 20, 300, 1.0, 0.01, 5
+    a = np.array([[1.0, np.exp(1j * np.pi), np.exp(1j * np.pi)],
+                  [np.exp(-1j * np.pi), 2.0, np.exp(1j * np.pi)],
+                  [np.exp(-1j * np.pi), np.exp(-1j * np.pi), 3.0]])
+    A = herm_matrix(nt, ntau, 3, -1)
+    O.green_from_H(A, 0.0, a, beta, h)
+    R = herm_matrix(nt, ntau, 2, -1)
+    O.green_from_H(R, 0.0, a[1:, 1:], beta, h)
+    G0 = herm_matrix(nt, ntau, 1, -1)
+    O.green_from_H(G0, 0.0, np.zeros((1, 1)), beta, h)
+    eta = herm_matrix(nt, ntau, 1, -1)
+    v, w = a[0:1, 1:], a[1:, 0:1]   # a_{0R}, a_{R0}: time-independent couplings
+    for c in ("ret", "les", "tv", "mat"):
+        getattr(eta, c)[...] = np.einsum("ab,nbc,cd->nad", v, getattr(R, c).reshape(-1, 2, 2), w).reshape(
+            getattr(eta, c).shape)
+    F, Fcc = herm_matrix(nt, ntau, 1, -1), herm_matrix(nt, ntau, 1, -1)
+    for n in range(-1, nt + 1):
+        O.convolution_timestep(n, F, G0, G0, eta, eta, beta, h, k)
+        O.convolution_timestep(n, Fcc, eta, eta, G0, G0, beta, h, k)
+    e00 = a[0, 0].real
+    for c in ("ret", "les", "tv", "mat"):
+        getattr(F, c)[...] = -getattr(F, c) - e00 * getattr(G0, c)
+        getattr(Fcc, c)[...] = -getattr(Fcc, c) - e00 * getattr(G0, c)
+    G = herm_matrix(nt, ntau, 1, -1)
+    O.vie2_mat(G, F, Fcc, G0, beta, k)
+    O.vie2_start(G, F, Fcc, G0, beta, h, k)
+    for n in range(k + 1, nt + 1):
+        O.vie2_timestep(n, G, F, Fcc, G0, beta, h, k)
+    A00 = herm_matrix(nt, ntau, 1, -1)
+    for t in range(-1, nt + 1):
+        A00.set_matrixelement(t, 0, 0, A, 0, 0)
+    err = sum(O.distance_norm2(t, G, A00) for t in range(-1, nt))
+    assert err < 1e-6, err                 # downfold.cpp:371 (eps)
