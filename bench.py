@@ -1,27 +1,28 @@
 """Benchmark of the batched Kadanoff-Baym time stepping (libcntr dyson_timestep hot path) on B200.
 
-One bench step = the whole time-stepping phase n = k+1..nt of every k-point of the workload
-(the metric counts k-point time steps; Matsubara and bootstrap are set-up, outside the timed
-region).  After the warm-up, one eager propagation gives the per-kernel device times (and the
-k_tv roofline); the propagation is then recorded as one CUDA graph and every timed step replays
-it (--no-graph: eager launches).  Inputs are resident in HBM for `value`; `e2e` repeats the step
-through the public API with host buffers (Sigma, H and bootstrap uploaded, the result downloaded
-every step).  The FP64 line of the chain workloads also carries `mixed`: the mixed-precision
-path on the same inputs, its throughput, its ratio to FP64 and its max relative error per
-component against the FP64 result (--no-mixed skips it).
+Default workload: config 4, the self-consistent 32 x 32 square lattice (size1 = 1, nt = 2000,
+ntau = 800, 3 predictor-corrector iterations per step), the configuration the metric's
+mixed-versus-FP64 target is stated on.  One bench step = the whole time-stepping phase n = k+1..nt
+of every k-point (the metric counts k-point time steps; Matsubara and bootstrap are set-up,
+outside the timed region).  After the warm-up, one eager propagation gives the per-kernel device
+times (and the roofline of the dominant kernel); the propagation is then recorded as one CUDA
+graph and every timed step replays it (--no-graph: eager launches).  Inputs are resident in HBM
+for `value`; `e2e` repeats the step through the public API with host buffers (Sigma, H and
+bootstrap uploaded, the result downloaded every step).  The FP64 line also carries `mixed`: the
+mixed-precision path on the same inputs, its throughput, its ratio to FP64 and its max relative
+error per component against the FP64 result (--no-mixed skips it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload config1|config1-small|config1-ncu|config2|config3|config3-small|
-                                config4|config4-small|config4-ncu]
+                    [--workload config4|config4-small|config4-ncu|config1|config1-small|config1-ncu|
+                                config2|config3|config3-small]
                     [--precision fp64|mixed] [--mixed-error] [--no-cpu] [--no-e2e] [--no-graph]
 
 Under torchrun each rank advances its own k-grid (shifted by rank/N of a grid spacing): the
 k-points of the chain workloads are independent, so ranks share no data ("scaling": "weak").
 The lattice workloads (config4*) form ONE lattice from all ranks' grids: after every k-average
 the ranks sum the weighted G_loc time-step slice with an NCCL all-reduce (nessi_b200.lattice),
-and those steps launch eagerly.  `--impl reference`
-times the CPU restatement of libcntr's serial path (oracle/, OpenMP over k-points) on a
-bounded sample of the same workload.
+and those steps launch eagerly.  `--impl reference` times the CPU restatement of libcntr's
+serial path (oracle/, OpenMP over k-points) on a bounded sample of the same workload.
 """
 import argparse
 import json
@@ -46,6 +47,27 @@ def load_peaks():
         d = json.load(open(p))
         return d.get("hbm_gbs", 6650.0), "measured"
     return 6650.0, "fallback"
+
+
+def fp64_peak_tflops(n=8192, reps=8):
+    """FP64 tensor-core throughput measured in this run: a cuBLAS DGEMM (torch.matmul on float64
+    tensors) of n x n x n, timed with CUDA events after a warm-up.  Only the roofline denominator
+    of the FP64 contractions; nothing on the product path uses cuBLAS."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        c = a @ b
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (ms / 1000.0) / 1e12
 
 
 # ------------------------------------------------------------------------------------------
@@ -271,8 +293,10 @@ def _max_rel(xs, ys):
 
 def mixed_companion(b, W, nt, k, fp64_value, args, world, stream):
     """The mixed-precision path on the same inputs, after the FP64 measurement: its throughput
-    (same step definition, warm-up and timing as the FP64 line) and the max relative error of its
-    result against the FP64 result per component.  The FP64 batch is released first."""
+    (same step definition and timing as the FP64 line: a CUDA graph of the propagation replayed
+    `--steps` times after an eager warm-up propagation) and the max relative error of its result
+    against the FP64 result per component (G_loc of a lattice, else every component of up to 8
+    problems).  The FP64 batch is released first."""
     import torch
     from nessi_b200 import gpu, workloads
     ref = _result_sample(b, W, nt)
@@ -281,14 +305,23 @@ def mixed_companion(b, W, nt, k, fp64_value, args, world, stream):
     try:
         workloads.upload(bm, W)
         bm.set_stream(stream.cuda_stream)
+        if W.lattice:
+            bm.lattice_2b_start(max_iter=30, tol=1e-12)
 
         def prop():
             for n in range(k + 1, nt + 1):
-                bm.dyson_timestep(n)
-        for _ in range(max(1, args.warmup)):
-            prop()
+                if W.lattice:
+                    bm.lattice_2b_timestep(n, W.ncorr)
+                else:
+                    bm.dyson_timestep(n)
+        prop()  # eager: the Volterra autotuner decides here
         bm.synchronize()
-        bm.graph_record(bm.GRAPH_DYSON, k + 1, nt)
+        bm.set_profiling(True)
+        prop()
+        bm.synchronize()
+        prof = bm.read_profile()
+        bm.set_profiling(False)
+        bm.graph_record(bm.GRAPH_LATTICE if W.lattice else bm.GRAPH_DYSON, k + 1, nt, W.ncorr or 3)
         bm.graph_launch()
         bm.synchronize()
         barrier(world)
@@ -303,11 +336,56 @@ def mixed_companion(b, W, nt, k, fp64_value, args, world, stream):
         ms = allmax(e0.elapsed_time(e1), world)
         value = world * W.kpt_steps() * args.steps / (ms / 1000.0)
         err = _max_rel(_result_sample(bm, W, nt), ref)
+        groups = sorted(W.sigma.keys()) if isinstance(W.sigma, dict) else [0]
+        volterra = {str(gid): bm.volterra_choice(gid) for gid in groups}
     finally:
         bm.close()
+    compared = "G_loc, all time steps" if W.lattice else "all components of %d problems, all time steps" % len(ref)
     return {"value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "ratio_to_fp64": value / fp64_value,
-            "max_rel_error_vs_fp64": err, "error_compared": "all components of %d problems, all time steps" % len(ref),
-            "dtype": "complex64 history / complex128 solves"}
+            "max_rel_error_vs_fp64": err, "error_compared": compared,
+            "kernels": {kname: {"ms": v[0], "launches": v[1]} for kname, v in prof.items()},
+            "volterra_kernels": {g: {"ret": v[0], "les": v[1]} for g, v in volterra.items()},
+            "dtype": "complex64 G^tv history / complex128 sums, solves and contractions"}
+
+
+# kernel classes of the profile whose algorithmic count is flops (nessi_gpu_read_profile)
+FLOP_KERNELS = ("ret", "les", "gemm")
+
+
+def kernel_roofline(prof, prof_steps, peak_hbm, hbm_kind, peak_fp64, traffic_ratio):
+    """Breakdown per kernel class and the roofline of the dominant one (largest device time):
+    HBM bytes against the measured copy peak for the streaming kernels, FP64 flops against the
+    FP64 tensor-core peak measured in this run for the contractions (k_zgemm, the Volterra
+    recursions)."""
+    total = max(1e-9, sum(v[0] for v in prof.values()))
+    breakdown = {}
+    for name, (ms, launches, work) in prof.items():
+        e = {"ms": ms / prof_steps, "launches": launches // prof_steps, "share": ms / total}
+        if ms > 0 and work > 0:
+            if name in FLOP_KERNELS:
+                e["tflops"] = work / (ms / 1000.0) / 1e12
+            else:
+                e["gbs"] = work / (ms / 1000.0) / 1e9
+        breakdown[name] = e
+    dom = max(prof, key=lambda x: prof[x][0])
+    ms, launches, work = prof[dom]
+    avg = ms / launches if launches else None
+    if dom in FLOP_KERNELS:
+        achieved = (work / launches) / (avg / 1000.0) / 1e12 if launches else 0.0
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                "frac": achieved / peak_fp64, "peak_source": "measured in-run (cuBLAS DGEMM 8192^3, FP64 tensor cores)",
+                "traffic": None, "algorithmic_flops_per_launch": work / launches if launches else None,
+                "avg_launch_ms": avg}
+    else:
+        achieved = (work / launches) / (avg / 1000.0) / 1e9 if launches else 0.0
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
+                "frac": achieved / peak_hbm, "peak_source": hbm_kind,
+                "traffic": (traffic_ratio * work / launches) if (traffic_ratio and launches and dom == "tv") else None,
+                "algorithmic_bytes_per_launch": work / launches if launches else None, "avg_launch_ms": avg}
+        if roof["traffic"] is not None:
+            roof["traffic_note"] = ("DRAM bytes per algorithmic byte from one ncu capture of k_tv, scaled to this "
+                                    "launch's algorithmic bytes")
+    return breakdown, roof
 
 
 def dist_setup(args):
@@ -341,24 +419,32 @@ def allmax(x, world):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle (CPU restatement of libcntr's serial dyson_timestep and of
+    the lattice driver) with OpenMP over k-points on the host cores.  Each step is a bounded
+    sample of the workload (windows of time steps at several n); `value` is the throughput of the
+    whole propagation integrated from the sample's fit, `ms_per_step` the sample's wall time."""
     if rank != 0:
         return
     W = build_workload(args.workload, 0, 1)
-    vals = []
+    vals, walls = [], []
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         v, thr, desc = cpu_sample(W, target_s=args.cpu_seconds)
         if i >= args.warmup:
             vals.append(v)
+            walls.append(time.perf_counter() - t0)
     value = float(np.median(vals))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * W.kpt_steps() / value, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.mean(walls)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
             "impl": "reference",
             "config": dict(workload=args.workload, **W.info),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "ms_per_step_note": "wall time of one bounded sample (a step); the whole propagation would take "
+                                "%.0f s at the fitted rate" % (W.kpt_steps() / value),
             "note": "libcntr needs Eigen3, absent here: the timed CPU path is the oracle's C++ restatement "
-                    "of libcntr's serial dyson_timestep with OpenMP over k-points"}
+                    "of libcntr's serial dyson_timestep (and lattice driver) with OpenMP over k-points"}
     print(json.dumps(line), flush=True)
 
 
@@ -368,7 +454,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1")
+    ap.add_argument("--workload", default="config4")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -465,31 +551,19 @@ def main():
     prof_steps = 1 if use_graph else args.steps
     units = world * W.kpt_steps() * args.steps
     value = units / (ms / 1000.0)
-    kernels_per_step = 7  # prep_problem, prep_group, ret, mat_operator, tv, les_operands, les
-    if W.lattice:  # extrapolate + ncorr x (gloc, sigma_2b, Dyson step) + final gloc
-        kernels_per_step = 1 + W.ncorr * (2 + kernels_per_step) + 1
-    gpu_launches = kernels_per_step * (nt - k) * args.steps
 
-    # roofline of k_tv, the G^tv history stream: the largest single kernel in the serialised ncu
-    # launch list (profiles/launches_config1-ncu.md) and the HBM-bound core of the step
+    # per-kernel device times and the roofline of the dominant kernel class
     peak, peak_kind = load_peaks()
-    dom = "tv"
-    dms, dl, dbytes = prof[dom]
-    achieved = (dbytes / dl) / ((dms / dl) / 1000.0) / 1e9 if dl else 0.0
-    traffic = None
+    peak_fp64 = fp64_peak_tflops()
+    traffic_ratio = None
     tpath = os.path.join(ROOT, "profiles", "k_tv_config1-ncu.md")
-    if os.path.exists(tpath) and dl:
+    if os.path.exists(tpath):
         for line in open(tpath):
             if line.startswith("traffic_ratio:"):
-                traffic = float(line.split(":")[1]) * dbytes / dl
-    roofline = {"kernel": "k_tv", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                "traffic_note": "DRAM bytes per algorithmic byte from one ncu capture at nt=ntau=300, "
-                                "scaled to this launch's algorithmic bytes",
-                "algorithmic_bytes_per_launch": dbytes / dl if dl else None,
-                "avg_launch_ms": dms / dl if dl else None}
-    # the whole step against the same peak: all algorithmic bytes of the propagation over its
-    # time; low where the sequential Volterra recursions (k_ret, k_les) set the pace
+                traffic_ratio = float(line.split(":")[1])
+    breakdown, roofline = kernel_roofline(prof, prof_steps, peak, peak_kind, peak_fp64, traffic_ratio)
+    # the whole step against the HBM peak: all algorithmic bytes of the propagation over its
+    # time; low where the sequential Volterra recursions set the pace
     try:
         sb = step_bytes(W, args.precision == "mixed")
         ach = sb * args.steps / (ms / 1000.0) / 1e9
@@ -499,9 +573,6 @@ def main():
                                        "histories, Sigma triangles, G slices) / device time of the timed steps"}
     except Exception as exc:  # the line stands without it
         step_roofline = {"error": "%s: %s" % (type(exc).__name__, exc)}
-    breakdown = {kname: {"ms": v[0] / prof_steps, "launches": v[1] // prof_steps,
-                         "share": v[0] / max(1e-9, sum(x[0] for x in prof.values()))}
-                 for kname, v in prof.items()}
 
     # end to end through the public API with host buffers
     e2e = None
@@ -541,8 +612,9 @@ def main():
         barrier(world)
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2e_steps = min(args.steps, 3)
         f0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(e2e_steps):
             workloads.upload(b, W)
             if W.lattice:
                 lattice_start()
@@ -561,8 +633,9 @@ def main():
         torch.cuda.synchronize()
         barrier(world)
         ems = allmax(f0.elapsed_time(f1), world)
-        e2e = {"value": units / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "pinned_host": pinned, "ms_per_step": ems / args.steps}
+        e2e = {"value": world * W.kpt_steps() * e2e_steps / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "pinned_host": pinned,
+               "ms_per_step": ems / e2e_steps, "steps": e2e_steps}
         if W.lattice:
             e2e["includes"] = "upload, self-consistent bootstrap, propagation, download of G_loc and G_k(nt)"
         elif last_only:
@@ -580,6 +653,19 @@ def main():
 
     groups = sorted(W.sigma.keys()) if isinstance(W.sigma, dict) else [0]
     volterra = {str(gid): b.volterra_choice(gid) for gid in groups}
+    # own kernels launched per timed step, from the launch structure of one Dyson step per group:
+    # k_prep_problem, k_prep_group, k_mat_operator, k_zgemm (Matsubara part), ret, k_les_operands_t,
+    # k_zgemm (les*adv), k_tv, k_les_operands_t, k_zgemm (tv*vt), les; ret / les are two kernels
+    # (k_*_start + k_volterra_cl) on the cluster path and one otherwise.  A lattice step adds
+    # k_extrapolate, per corrector k_gloc + k_gloc_final + k_sigma_2b, and the final k-average.
+    per_group = [10 + (2 if v[0] == 100 else 1) + (2 if v[1] == 100 else 1) for v in volterra.values()]
+    if W.lattice:
+        gpu_launches = (nt - k) * (1 + W.ncorr * (3 + sum(per_group)) + 2) * args.steps
+    else:
+        nts = {}
+        for d in W.descs:
+            nts.setdefault(d.get("sigma_group", 0), []).append(d["nt"])
+        gpu_launches = sum((max(nts[int(g)]) - k) * c for g, c in zip(volterra.keys(), per_group)) * args.steps
     mixed_err = None
     if args.mixed_error and args.precision == "mixed":
         mixed_err = compare_with_fp64(b, W, run_step, nt, k)
@@ -587,7 +673,7 @@ def main():
     # carries the mixed path measured on the same inputs
     mixed_line = None
     closed = False
-    if args.precision == "fp64" and not W.lattice and not isinstance(W.sigma, dict) and not args.no_mixed:
+    if args.precision == "fp64" and sharded is None and not args.no_mixed:
         try:
             mixed_line = mixed_companion(b, W, nt, k, value, args, world, stream)
         except Exception as exc:  # the FP64 line stands on its own
@@ -607,7 +693,8 @@ def main():
                                           "dyson_start iterations (set-up, untimed)" % boot_iters) if W.lattice else
                                "free propagator of H_k(-1) for mat and steps 0..k (set-up, untimed)",
                                **W.info),
-                "roofline": roofline, "step_roofline": step_roofline, "kernels": breakdown, "cpu_baseline": cpu,
+                "roofline": roofline, "step_roofline": step_roofline, "kernels": breakdown,
+                "fp64_peak_tflops_in_run": peak_fp64, "cpu_baseline": cpu,
                 "e2e": e2e,
                 "gpu_launches": gpu_launches, "clocks": clk,
                 "launch": "CUDA graph of the whole propagation, replayed each step" if use_graph else "eager",

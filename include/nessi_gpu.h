@@ -33,7 +33,7 @@ extern "C" {
 #define NESSI_OK 0
 #define NESSI_ERR_ARG 1       /* bad argument or state */
 #define NESSI_ERR_OOM 2       /* device allocation failed */
-#define NESSI_ERR_CUDA 3      /* CUDA / cuBLAS runtime error */
+#define NESSI_ERR_CUDA 3      /* CUDA runtime error */
 #define NESSI_ERR_SINGULAR 4  /* a step matrix had a zero pivot */
 #define NESSI_ERR_TIMEOUT 5   /* a bounded device wait gave up */
 
@@ -131,31 +131,35 @@ int nessi_gpu_set_stream(nessi_batch *b, void *stream);
 #define NESSI_KERNEL_RET 1           /* G^R(n, .) Volterra recursion */
 #define NESSI_KERNEL_TV 2            /* G^tv(n, .) history stream + solve */
 #define NESSI_KERNEL_LES_OPERANDS 3  /* operands of the Sigma-shared products */
-#define NESSI_KERNEL_GEMM 4          /* K_n G^mat, tv*vt and les*adv products (cuBLAS ZGEMM) */
+#define NESSI_KERNEL_GEMM 4          /* K_n G^mat, tv*vt and les*adv products (k_zgemm, FP64 tensor cores) */
 #define NESSI_KERNEL_LES 5           /* G^<(., n) Volterra recursion */
 #define NESSI_KERNEL_MATOP 6         /* Matsubara operator K_n of the tv row */
 #define NESSI_KERNEL_LATTICE 7       /* predictor, G_loc and Sigma_2B of the lattice driver */
 #define NESSI_KERNEL_COUNT 8
 /* Turn timing on/off (resets counters).  No reference counterpart. */
 int nessi_gpu_set_profiling(nessi_batch *b, int on);
-/* Total device time (ms), launches and algorithmic bytes (flops for GEMM) recorded for one
- * kernel id since the last read; resets that counter.  No reference counterpart. */
+/* Total device time (ms), launches and algorithmic bytes recorded for one kernel id since the
+ * last read (flops for GEMM, RET and LES: 8 per complex multiply-add); resets that counter.
+ * No reference counterpart. */
 int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *launches, double *bytes);
 
 /* dyson_mat (fixpoint method) for ONE problem, allocating nothing.  No counterpart in the
- * reference.  It is meant for callers that cannot let a library call cudaMalloc: code running
- * while its stream is captured, or applications whose device memory is owned by another
- * allocator.  Every input and output is a device pointer owned by the caller:
+ * reference.  It is meant for callers that cannot let a library call cudaMalloc: applications
+ * whose device memory is owned by another allocator (a framework's memory pool, an arena sized
+ * at start-up), or that must not take the device-wide synchronisation a cudaMalloc / cudaFree can
+ * bring.  Every input and output is a device pointer owned by the caller:
  *   H          cntr::function data starting at H(-1) (at least one size1 x size1 block)
  *   sigma_mat  Sigma^mat, (ntau+1) blocks;   gmat  G^mat, (ntau+1) blocks, written
  * The work is queued on `stream` (a cudaStream_t, NULL = legacy default stream) and the call
  * returns without waiting.  Scratch is a fixed device array of 131072 complex<double>
  * (2 MiB) that every GPU loading the library holds until exit; sizes with
- * 6(ntau+1)size1^2 + 2 ntau size1^2 above that limit are rejected with NESSI_ERR_ARG.  The first
- * call on a device looks up the array's device address and uploads the integration tables, so
- * make that first call before any stream capture.  All calls share the one array: calls whose
- * work overlaps on the GPU race.  Every scratch element is written before it is read, so
- * nothing left by an earlier call leaks into a result.  ntau must be even. */
+ * 6(ntau+1)size1^2 + 2 ntau size1^2 above that limit are rejected with NESSI_ERR_ARG, and so is an
+ * ntau whose 2 ntau twiddle factors (32 ntau bytes of shared memory per block) exceed the
+ * device's per-block shared-memory limit (about ntau > 7000 on a B200).  The first call on a
+ * device looks up the array's device address and uploads the integration tables (under a lock,
+ * waiting for the upload), so make that first call before any stream capture.  All calls share
+ * the one array: calls whose work overlaps on the GPU race.  Every scratch element is written
+ * before it is read, so nothing left by an earlier call leaks into a result.  ntau must be even. */
 int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int solve_order, double beta, double mu, const void *H,
                                 const void *sigma_mat, void *gmat, void *stream);
 
@@ -235,7 +239,8 @@ int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, c
                                int sig_a, int sig_b, int solve_order, double beta, double h);
 
 /* Volterra kernels in use for a group: -1 = one problem per CTA, 2/4/8 = problems per CTA of the
- * tensor-core kernels, 0 = not chosen yet (the autotuner decides at the first eager step with
+ * tensor-core kernels, 100 = the group-wide blocked recursion by thread-block clusters (trailing
+ * updates on the FP64 tensor cores), 0 = not chosen yet (the autotuner decides at the first eager step with
  * n >= min(128, nt); the environment variable NESSI_VOLTERRA_PP read at batch creation fixes
  * the choice).  No reference counterpart. */
 int nessi_gpu_get_volterra_choice(nessi_batch *b, int group, int *pp_ret, int *pp_les);

@@ -56,7 +56,7 @@ def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     tmp = LIB + ".tmp"
-    cmd = [NVCC] + FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcublas"]
+    cmd = [NVCC] + FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd, cwd=CSRC)

@@ -8,8 +8,9 @@
 //   k_ret            G^R(n, 0..n): k-block start + Volterra recursion in t'   (:80-222)
 //   k_tv             G^tv(n, 0..ntau): history stream + Matsubara integral + solve (:651-741)
 //   k_les_operands_t right-hand operands of the Sigma-shared products
-//   2 x ZGEMM        tv*vt + les*adv convolutions for all problems at once (conv_impl :1075-1394)
+//   2 x k_zgemm      tv*vt + les*adv convolutions for all problems at once (conv_impl :1075-1394)
 //   k_les            G^<(0..n, n): k-block start + Volterra recursion in t (:893-1056)
+// The Volterra recursions also run group-wide (k_ret_start / k_les_start + k_volterra_cl).
 #pragma once
 #include "device_common.cuh"
 
@@ -618,3 +619,4 @@ __global__ void __launch_bounds__(256) k_les_operands_t(GroupDev g, const ProbDe
 
 #include "kernels_volterra.cuh"
 #include "kernels_volterra_mp.cuh"
+#include "kernels_volterra_cl.cuh"

@@ -1,11 +1,11 @@
 // libnessi_gpu.so: batches of Kadanoff-Baym problems advanced on one B200.
 // Host side of the C ABI declared in include/nessi_gpu.h.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -37,6 +37,7 @@ struct NvtxRange {
 int g_device = 0;
 std::atomic<int> g_live_batches{0};  // created and not yet destroyed
 std::vector<int> g_tables_ready;  // devices whose c_tab was filled
+std::mutex g_setup_mutex;         // guards the per-device set-up state (tables, scratch address)
 
 void set_err(const char *fmt, ...) {
     char buf[512];
@@ -57,15 +58,6 @@ void set_err(const char *fmt, ...) {
         }                                                                                       \
     } while (0)
 
-#define CKB(x)                                                                      \
-    do {                                                                            \
-        cublasStatus_t s_ = (x);                                                    \
-        if (s_ != CUBLAS_STATUS_SUCCESS) {                                          \
-            set_err("cuBLAS error %d at %s:%d", (int)s_, __FILE__, __LINE__);       \
-            return NESSI_ERR_CUDA;                                                  \
-        }                                                                           \
-    } while (0)
-
 #define CKR(x)                      \
     do {                            \
         int r_ = (x);               \
@@ -74,7 +66,10 @@ void set_err(const char *fmt, ...) {
 
 inline long tri_h(long t) { return t * (t + 1) / 2; }
 
+// Integration tables into c_tab of device `dev` (current), once per device.  The upload is waited
+// for, so that a kernel on any stream of the caller sees the tables.
 int ensure_tables(int dev) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (std::find(g_tables_ready.begin(), g_tables_ready.end(), dev) != g_tables_ready.end()) return NESSI_OK;
     IntegTables t;
     std::memcpy(t.greg, cntr_tab_gregory, sizeof t.greg);
@@ -85,7 +80,25 @@ int ensure_tables(int dev) {
     std::memcpy(t.bd, cntr_tab_bd, sizeof t.bd);
     std::memcpy(t.rcorr, cntr_tab_rcorr, sizeof t.rcorr);
     CK(cudaMemcpyToSymbol(c_tab, &t, sizeof t));
+    CK(cudaDeviceSynchronize());
     g_tables_ready.push_back(dev);
+    return NESSI_OK;
+}
+
+// The Matsubara solvers keep 2 ntau twiddle factors in dynamic shared memory next to the
+// kernel's static shared memory; check that against the device's opt-in limit per block.
+int check_twiddle_smem(const void *kernel, int ntau, const char *name) {
+    int dev = 0, optin = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    const size_t need = 2 * (size_t)ntau * 16 + fa.sharedSizeBytes;
+    if (need > (size_t)optin) {
+        set_err("%s: ntau = %d needs %zu bytes of shared memory per block (2 ntau twiddles), above the device "
+                "limit of %d", name, ntau, need, optin);
+        return NESSI_ERR_ARG;
+    }
     return NESSI_OK;
 }
 
@@ -118,6 +131,7 @@ struct Group {
     int pp_ret = 0, pp_les = 0;      // Volterra kernel chosen by the autotuner (0: not yet)
     double2 *fccret = nullptr, *fccles = nullptr;
     double2 *U = nullptr;            // diagonal interaction U(t), (ntmax+2) x s, t = -1 first
+    double2 *accr = nullptr, *accl = nullptr, *panel = nullptr;  // cluster Volterra path
     std::vector<int> members;        // problem indices, nt descending
     std::vector<ProbDev> h_probs;    // same order; col = position
     ProbDev *d_probs = nullptr;
@@ -142,8 +156,6 @@ struct nessi_batch {
     cudaStream_t side = nullptr;       // runs the retarded component concurrently with tv
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool own_stream = true;
-    cublasHandle_t cublas = nullptr, cublas_side = nullptr;
-    void *cublas_ws = nullptr, *cublas_ws_side = nullptr;  // fixed cuBLAS workspaces (capture-safe)
     cudaGraphExec_t graph = nullptr;                     // recorded time steps (nessi_gpu_graph_record)
     std::vector<Prob> probs;
     std::vector<Group> groups;
@@ -237,10 +249,95 @@ template <int S> size_t les_smem(int k) {
     return std::max(start, phase);
 }
 
+// C (M x N) = A (M x K) B (K x N) on the repo's DMMA GEMM (kernels_gemm.cuh): 64 x 64 tiles, or
+// 128 x 32 when the problem columns are few.
+template <class LA, class LB, class ST>
+int zgemm_launch(const LA &la, const LB &lb, const ST &st, int M, int N, int K, cudaStream_t s) {
+    if (M <= 0 || N <= 0) return NESSI_OK;
+    if (N > 32) {
+        const dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
+        const size_t sm = (size_t)zg::Smem<64, 64>::total * sizeof(double2);
+        CK(cudaFuncSetAttribute(k_zgemm<64, 64, LA, LB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_zgemm<64, 64><<<grid, 128, sm, s>>>(la, lb, st, K);
+    } else {
+        const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((M + 127) / 128));
+        const size_t sm = (size_t)zg::Smem<128, 32>::total * sizeof(double2);
+        CK(cudaFuncSetAttribute(k_zgemm<128, 32, LA, LB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_zgemm<128, 32><<<grid, 128, sm, s>>>(la, lb, st, K);
+    }
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+// Volterra choice code of the group-wide cluster path (k_ret_start / k_les_start + k_volterra_cl)
+#define NESSI_VOLTERRA_CLUSTER 100
+#define NESSI_CL 8  // CTAs per cluster (portable cluster size)
+
+template <int S> size_t ret_start_smem(int k) {
+    return (size_t)(k * k * S * S + k * S * S + (k * S) * (k * S) + k * S * S) * 16 + 16;
+}
+template <int S> size_t les_start_smem(int k) {
+    const int K1 = k + 1;
+    return (size_t)((K1 * S) * (K1 * S) + K1 * S * S) * 16 + 16;
+}
+
+template <int S, bool VIE, bool RET, int BN>
+int cluster_kernel_launch(const GroupDev &gd, const Group &g, int n, int nact, int PT, int ncl, double2 *acc,
+                          double2 *panel, cudaStream_t st) {
+    const size_t sm = (size_t)std::max(ClSmem<S>::diag, ClGemm<BN>::smem) * sizeof(double2);
+    auto kern = k_volterra_cl<S, VIE, RET, BN>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(NESSI_CL * ncl));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = NESSI_CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kern, gd, (const ProbDev *)g.d_probs, n, nact, PT, acc, panel));
+    return NESSI_OK;
+}
+
+// Group-wide recursion: the start block of every problem (one CTA each), then the blocked
+// recursion by clusters of NESSI_CL CTAs, each owning PT problems (about 18 clusters fill the
+// 148 SMs; at most NESSI_CL x ClCfg::DWMAX problems, one chain warp each).
+template <int S, bool VIE>
+int cluster_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret, cudaStream_t st) {
+    if (ret) {
+        const size_t sm = ret_start_smem<S>(gd.k);
+        CK(cudaFuncSetAttribute(k_ret_start<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_ret_start<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+    } else {
+        const size_t sm = les_start_smem<S>(gd.k);
+        CK(cudaFuncSetAttribute(k_les_start<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_les_start<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+    }
+    CK(cudaGetLastError());
+    if (n - gd.k <= 0) return NESSI_OK;  // no unknowns below / above the start block
+    int PT = (nact + 17) / 18;
+    PT = std::max(1, std::min(PT, NESSI_CL * ClCfg<S>::DWMAX));
+    const int ncl = (nact + PT - 1) / PT;
+    double2 *acc = ret ? g.accr : g.accl;
+    if constexpr (S <= 2) {
+        if (PT * S > 32) {
+            if (ret) return cluster_kernel_launch<S, VIE, true, 64>(gd, g, n, nact, PT, ncl, acc, g.panel, st);
+            return cluster_kernel_launch<S, VIE, false, 64>(gd, g, n, nact, PT, ncl, acc, g.panel, st);
+        }
+    }
+    if (ret) return cluster_kernel_launch<S, VIE, true, 32>(gd, g, n, nact, PT, ncl, acc, g.panel, st);
+    return cluster_kernel_launch<S, VIE, false, 32>(gd, g, n, nact, PT, ncl, acc, g.panel, st);
+}
+
 // One Volterra recursion (ret or les) of a step: the one-problem kernels (pp = -1) or the
 // multi-problem tensor-core kernels with pp problems per CTA (size1 <= 2).
 template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret, int pp,
                                                cudaStream_t st) {
+    if (pp == NESSI_VOLTERRA_CLUSTER) return cluster_launch<S, VIE>(gd, g, n, nact, ret, st);
     if constexpr (S <= 2) {
         if (pp > 0) {
             const size_t sm = (size_t)MpCfg<S>::total * sizeof(double2);
@@ -281,17 +378,20 @@ template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const Gro
     if (choice != 0) return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cap));
-    if (S > 2) choice = -1;
-    if (S > 2 || cap != cudaStreamCaptureStatusNone || n < std::min(128, g.ntmax))
+    if (cap != cudaStreamCaptureStatusNone || n < std::min(128, g.ntmax))
         return volterra_launch<S, VIE>(gd, g, n, nact, ret, -1, st);
-    const int cand[4] = {-1, 2, 4, 8};
+    // candidates: one problem per CTA, the per-CTA tensor-core kernels (size1 <= 2), the cluster path
+    const int cand_small[5] = {-1, 2, 4, 8, NESSI_VOLTERRA_CLUSTER}, cand_big[2] = {-1, NESSI_VOLTERRA_CLUSTER};
+    const int *cand = S <= 2 ? cand_small : cand_big;
+    const int ncand = S <= 2 ? 5 : 2;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
     int bestc = -1;
     for (int pass = 0; pass < 2; pass++)  // the first pass warms up every variant
-        for (int c : cand) {
+        for (int ic = 0; ic < ncand; ic++) {
+            const int c = cand[ic];
             CK(cudaEventRecord(e0, st));
             CKR((volterra_launch<S, VIE>(gd, g, n, nact, ret, c, st)));
             CK(cudaEventRecord(e1, st));
@@ -327,9 +427,8 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
         b->prof_end(NESSI_KERNEL_PREP, 0.0);
         g.dense_valid = n - 1;
     }
-    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
     // VIE2 moves the convolution to the right-hand side: gles = -(tv*vt + les*adv)
-    const cuDoubleComplex alpha = make_cuDoubleComplex(VIE ? -1.0 : 1.0, 0.0);
+    const double alpha = VIE ? -1.0 : 1.0;
     // Matsubara part of the tv row: Cmat = K_n Gmat_all (one GEMM for the group)
     {
         const long M = g.ntau + 1;
@@ -345,9 +444,9 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_MATOP, 16.0 * (double)work + 16.0 * M * S * S);
         b->prof_mark(NESSI_KERNEL_GEMM);
-        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, nact * S, (int)(M * S), (int)(M * S), &one,
-                        (const cuDoubleComplex *)g.Gmat_all, g.ldc, (const cuDoubleComplex *)g.Kmat, (int)(M * S),
-                        &zero, (cuDoubleComplex *)g.Cmat, g.ldc));
+        const int MS = (int)(M * S);
+        CKR(zgemm_launch(LdRowK{g.Kmat, MS, MS, MS}, LdRowN{g.Gmat_all, g.ldc, MS, nact * S},
+                         StRow{g.Cmat, g.ldc, MS, nact * S, 1.0, 0}, MS, nact * S, MS, st));
         b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)nact * S * (M * S) * (M * S));
     }
     const int m = nact * S, nn = (n + 1) * S;
@@ -358,17 +457,16 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
     {
         b->prof_mark(NESSI_KERNEL_RET, b->side);
         CKR((volterra_step<S, VIE>(b, g, gd, n, nact, true, b->side)));
-        // G^R row n written; Sigma^R triangle rows <= n read (shared by the group)
-        b->prof_end(NESSI_KERNEL_RET, 16.0 * S * S * ((double)nact * (n + 1) + tri_h(n + 1)), b->side);
+        // flops: every pair m > j of the row, an s x s complex product (8 s^3) per problem
+        b->prof_end(NESSI_KERNEL_RET, 8.0 * S * S * S * (double)nact * tri_h(n), b->side);
         b->prof_mark(NESSI_KERNEL_LES_OPERANDS, b->side);
         dim3 grid((unsigned)((n + 1 + LoCfg<S>::LOR - 1) / LoCfg<S>::LOR), (unsigned)((nact + LOT - 1) / LOT));
         k_les_operands_t<S><<<grid, 256, 0, b->side>>>(gd, g.d_probs, n, 1, nact);
         CK(cudaGetLastError());
         b->prof_end(NESSI_KERNEL_LES_OPERANDS, 32.0 * S * S * (double)nact * (n + 1), b->side);
         b->prof_mark(NESSI_KERNEL_GEMM, b->side);
-        CKB(cublasZgemm(b->cublas_side, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (n + 1) * S, &alpha,
-                        (const cuDoubleComplex *)g.badv, g.ldc, (const cuDoubleComplex *)g.Ldense, (int)ldL, &zero,
-                        (cuDoubleComplex *)g.gles, g.ldc));
+        CKR(zgemm_launch(LdRowK{g.Ldense, ldL, nn, nn}, LdRowN{g.badv, g.ldc, nn, m},
+                         StRow{g.gles, g.ldc, nn, m, alpha, 0}, nn, m, nn, b->side));
         b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)m * nn * ((n + 1) * S), b->side);
     }
     CK(cudaEventRecord(b->ev_join, b->side));
@@ -397,16 +495,16 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
     {
         b->prof_mark(NESSI_KERNEL_GEMM);
         const double2 *T = S == 1 ? g.stv : g.Tdense;
-        CKB(cublasZgemm(b->cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nn, (g.ntau + 1) * S, &alpha,
-                        (const cuDoubleComplex *)g.btv, g.ldc, (const cuDoubleComplex *)T, (int)ldT, &one,
-                        (cuDoubleComplex *)g.gles, g.ldc));
+        const int MS = (g.ntau + 1) * S;
+        CKR(zgemm_launch(LdRowK{T, ldT, nn, MS}, LdRowN{g.btv, g.ldc, MS, m}, StRow{g.gles, g.ldc, nn, m, alpha, 1},
+                         nn, m, MS, st));
         b->prof_end(NESSI_KERNEL_GEMM, 8.0 * (double)m * nn * ((g.ntau + 1) * S));
     }
     // lesser column
     {
         b->prof_mark(NESSI_KERNEL_LES);
         CKR((volterra_step<S, VIE>(b, g, gd, n, nact, false, st)));
-        b->prof_end(NESSI_KERNEL_LES, 16.0 * S * S * ((double)nact * 2.0 * (n + 1) + tri_h(n + 1)));
+        b->prof_end(NESSI_KERNEL_LES, 8.0 * S * S * S * (double)nact * tri_h(n));
     }
     return NESSI_OK;
 }
@@ -447,6 +545,7 @@ static int ensure_mat_scratch(nessi_batch *b, Group &g) {
 
 template <int S> int mat_group(nessi_batch *b, Group &g) {
     const GroupDev gd = group_dev(g);
+    CKR(check_twiddle_smem((const void *)k_dyson_mat<S>, g.ntau, "dyson_mat"));
     CKR(ensure_mat_scratch(b, g));
     const size_t sm = 2 * (size_t)g.ntau * sizeof(double2);
     CK(cudaFuncSetAttribute(k_dyson_mat<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -459,6 +558,7 @@ template <int S> int mat_group(nessi_batch *b, Group &g) {
 // vie2_mat of a VIE2 group: Q^mat of every member is copied into its scratch slot G0 first
 template <int S> int vie2_mat_group(nessi_batch *b, Group &g) {
     const GroupDev gd = group_dev(g);
+    CKR(check_twiddle_smem((const void *)k_vie2_mat<S>, g.ntau, "vie2_mat"));
     CKR(ensure_mat_scratch(b, g));
     const long M = g.ntau + 1, s2 = (long)g.s * g.s;
     for (size_t c = 0; c < g.members.size(); c++) {
@@ -602,7 +702,8 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
     b->precision = precision;
     if (const char *v = getenv("NESSI_VOLTERRA_PP")) {
         const int pp = atoi(v);
-        if (pp == -1 || pp == 0 || pp == 1 || pp == 2 || pp == 4 || pp == 8) b->volterra_pp = pp;
+        if (pp == -1 || pp == 0 || pp == 1 || pp == 2 || pp == 4 || pp == 8 || pp == NESSI_VOLTERRA_CLUSTER)
+            b->volterra_pp = pp;
     }
     auto fail = [&](int r) { nessi_gpu_batch_destroy(b); return r; };
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -614,24 +715,6 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
         cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         set_err("stream/event creation failed");
         return fail(NESSI_ERR_CUDA);
-    }
-    if (cublasCreate(&b->cublas) != CUBLAS_STATUS_SUCCESS) { set_err("cublasCreate failed"); return fail(NESSI_ERR_CUDA); }
-    cublasSetStream(b->cublas, b->stream);
-    cublasSetMathMode(b->cublas, CUBLAS_DEFAULT_MATH);
-    if (cublasCreate(&b->cublas_side) != CUBLAS_STATUS_SUCCESS) { set_err("cublasCreate failed"); return fail(NESSI_ERR_CUDA); }
-    cublasSetStream(b->cublas_side, b->side);
-    cublasSetMathMode(b->cublas_side, CUBLAS_DEFAULT_MATH);
-    {
-        // fixed workspaces, so that cuBLAS allocates nothing while a graph is being recorded
-        const size_t wsz = 32u << 20;
-        if (cudaMalloc(&b->cublas_ws, wsz) != cudaSuccess || cudaMalloc(&b->cublas_ws_side, wsz) != cudaSuccess) {
-            set_err("cudaMalloc of the cuBLAS workspaces failed");
-            return fail(NESSI_ERR_OOM);
-        }
-        b->allocs.push_back(b->cublas_ws);
-        b->allocs.push_back(b->cublas_ws_side);
-        cublasSetWorkspace(b->cublas, b->cublas_ws, wsz);
-        cublasSetWorkspace(b->cublas_side, b->cublas_ws_side, wsz);
     }
     b->probs.resize(count);
     // groups
@@ -694,7 +777,8 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
             (r = b->alloc(&g.tvcoef, N * s2)) || (r = b->alloc(&g.badv, N * S * g.ldc)) ||
             (r = b->alloc(&g.btv, M * S * g.ldc)) || (r = b->alloc(&g.gles, N * S * g.ldc)) ||
             (r = b->alloc(&g.Kmat, M * S * M * S)) || (r = b->alloc(&g.Gmat_all, M * S * g.ldc)) ||
-            (r = b->alloc(&g.Cmat, M * S * g.ldc)))
+            (r = b->alloc(&g.Cmat, M * S * g.ldc)) || (r = b->alloc(&g.accr, N * S * g.ldc)) ||
+            (r = b->alloc(&g.accl, N * S * g.ldc)) || (r = b->alloc(&g.panel, (32 + NESSI_K1MAX) * S * g.ldc)))
             return fail(r);
         for (size_t c = 0; c < g.members.size(); c++) {
             const Prob &p = b->probs[g.members[c]];
@@ -728,8 +812,6 @@ int nessi_gpu_batch_destroy(nessi_batch *b) {
     for (void *q : b->allocs) cudaFree(q);
     for (auto &k : b->kp)
         for (cudaEvent_t e : k.ev) cudaEventDestroy(e);
-    if (b->cublas) cublasDestroy(b->cublas);
-    if (b->cublas_side) cublasDestroy(b->cublas_side);
     if (b->side) { cudaStreamSynchronize(b->side); cudaStreamDestroy(b->side); }
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
@@ -949,7 +1031,6 @@ int nessi_gpu_set_stream(nessi_batch *b, void *stream) {
         CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         b->own_stream = true;
     }
-    CKB(cublasSetStream(b->cublas, b->stream));
     return NESSI_OK;
 }
 
@@ -1384,11 +1465,13 @@ int nessi_gpu_synchronize(nessi_batch *b) {
 // =====================================================================================
 // dyson_mat without allocation
 // =====================================================================================
-// Some callers cannot let a library call cudaMalloc: code that runs while its stream is being
-// captured, or a host application whose device memory is owned by another allocator (a
-// framework's memory pool, a preallocated arena).  nessi_gpu_dyson_mat_noalloc serves them:
-// the caller passes every input and output as device pointers and the scratch lives in the
-// fixed array below, which every GPU that loads this library holds until the process exits.
+// Some callers cannot let a library call cudaMalloc: a host application whose device memory is
+// owned by another allocator (a framework's memory pool, a preallocated arena sized at start-up),
+// or one that must not take the device-wide synchronisation a cudaMalloc / cudaFree can bring.
+// nessi_gpu_dyson_mat_noalloc serves them: the caller passes every input and output as device
+// pointers and the scratch lives in the fixed array below, which every GPU that loads this
+// library holds until the process exits.  The first call on a device does the set-up (tables,
+// scratch address; guarded by a mutex), so make it before any stream capture.
 #define NESSI_NOALLOC_MAX_CPLX (1 << 17)  // 131072 complex<double> = 2 MiB
 static __device__ __align__(256) double2 g_noalloc_scratch[NESSI_NOALLOC_MAX_CPLX];
 
@@ -1403,6 +1486,7 @@ __global__ void __launch_bounds__(256) k_dyson_mat_single(GroupDev g, ProbDev p,
 
 template <int S>
 int noalloc_launch(const GroupDev &gd, const ProbDev &pd, const MatScratch &w, int ntau, cudaStream_t st) {
+    CKR(check_twiddle_smem((const void *)k_dyson_mat_single<S>, ntau, "dyson_mat_noalloc"));
     const size_t sm = 2 * (size_t)ntau * sizeof(double2);
     CK(cudaFuncSetAttribute(k_dyson_mat_single<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_dyson_mat_single<S><<<1, 256, sm, st>>>(gd, pd, w);
@@ -1430,14 +1514,18 @@ extern "C" int nessi_gpu_dyson_mat_noalloc(int ntau, int size1, int sig, int sol
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) { set_err("dyson_mat_noalloc: device index %d unsupported", dev); return NESSI_ERR_ARG; }
-    if (!g_noalloc_addr[dev]) {
+    double2 *base = nullptr;
+    {
         // set-up on the first call on this device: integration tables and the scratch address
         CKR(ensure_tables(dev));
-        void *ptr = nullptr;
-        CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        g_noalloc_addr[dev] = (double2 *)ptr;
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (!g_noalloc_addr[dev]) {
+            void *ptr = nullptr;
+            CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+            g_noalloc_addr[dev] = (double2 *)ptr;
+        }
+        base = g_noalloc_addr[dev];
     }
-    double2 *base = g_noalloc_addr[dev];
     MatScratch w;
     w.G0 = base; w.F = base + M * s2; w.Q = base + 2 * M * s2; w.dG = base + 3 * M * s2;
     w.fdft = base + 4 * M * s2; w.qdft = base + 5 * M * s2; w.Z = base + 6 * M * s2;

@@ -117,6 +117,14 @@ def test_lattice_2b_fp64(oracle, u_mat):
     assert max(worst.values()) < TOL, worst
 
 
+def test_lattice_2b_cluster_recursion(oracle, monkeypatch):
+    """The lattice step with the group-wide cluster recursion for both Volterra components."""
+    from nessi_b200 import gpu
+    monkeypatch.setenv("NESSI_VOLTERRA_PP", "100")
+    worst = _lattice_run(oracle, gpu.PREC_FP64, 3, 3, 70, 20, 0.7)
+    assert max(worst.values()) < TOL, worst
+
+
 def test_lattice_2b_mixed(oracle):
     from nessi_b200 import gpu
     worst = _lattice_run(oracle, gpu.PREC_MIXED, 4, 2, 60, 30, 0.0)

@@ -190,7 +190,7 @@ def test_vie2_errors():
     b.close()
 
 
-@pytest.mark.parametrize("pp", [-1, 1, 4, 8])
+@pytest.mark.parametrize("pp", [-1, 1, 4, 8, 100])
 def test_vie2_problems_per_cta(oracle, monkeypatch, pp):
     """The VIE2 path of the size1 <= 2 Volterra kernels with every problems-per-CTA grouping."""
     from nessi_b200 import gpu
@@ -238,6 +238,31 @@ def test_vie2_mat_and_whole_pipeline(oracle, s):
     for n in range(k + 1, nt + 1):
         b.vie2_timestep(n)
     for p in range(2):
+        Gg = herm_matrix(nt, ntau, s, -1)
+        b.get_G(p, Gg)
+        _check(Gg, ref[p][0], k, nt, TOL)
+    b.close()
+
+
+@pytest.mark.parametrize("s", [3, 5])
+def test_vie2_cluster_recursion_large_orbitals(oracle, monkeypatch, s):
+    """The VIE2 form of the cluster recursion for size1 >= 3 (element-parallel chains)."""
+    from nessi_b200 import gpu
+    monkeypatch.setenv("NESSI_VOLTERRA_PP", "100")
+    rng = np.random.default_rng(700 + s)
+    nt, ntau, beta, h, k = 30, 8, 4.0, 0.05, 5
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Qs = [_source(oracle, rng, nt, ntau, s, beta, h) for _ in range(3)]
+    ref = [_oracle_vie2(oracle, F, Fcc, Q, beta, h, k) for Q in Qs]
+    b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, beta=beta, h=h)] * 3)
+    b.set_F(0, F, Fcc)
+    for p, Q in enumerate(Qs):
+        b.set_Q(p, Q)
+        b.set_timestep(p, -1, ref[p][1].mat)
+    b.vie2_start()
+    for n in range(k + 1, nt + 1):
+        b.vie2_timestep(n)
+    for p in range(3):
         Gg = herm_matrix(nt, ntau, s, -1)
         b.get_G(p, Gg)
         _check(Gg, ref[p][0], k, nt, TOL)
