@@ -9,7 +9,7 @@ for each dataset its version-1 object header with the dataspace (0x0001), dataty
 data layout (0x0008, contiguous) messages.  That covers this fixture (two 1-d float64 datasets
 "den0" and "den1" of nt + 2 = 52 values); anything else raises.
 
-    python tests/golden/make_fkm_golden.py [path/to/fkm_bethe_quench.h5]
+    NESSI_REFERENCE_ROOT=<reference checkout> python tests/golden/make_fkm_golden.py [path/to/fkm_bethe_quench.h5]
 """
 import json
 import os
@@ -17,7 +17,9 @@ import struct
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/libcntr/test/fkm_bethe_quench.h5"
+# default source: under NESSI_REFERENCE_ROOT, the reference checkout (the directory holding
+# libcntr/); a path given as the first argument overrides it
+DEFAULT_SRC = os.path.join(os.environ.get("NESSI_REFERENCE_ROOT", "."), "libcntr/test/fkm_bethe_quench.h5")
 OUT = os.path.join(HERE, "fkm_bethe_quench.json")
 SIGNATURE = b"\x89HDF\r\n\x1a\n"
 

@@ -12,14 +12,16 @@ are the start weights and rows k+1..2k+1 hold sigma followed by omega.
 The fixture is the golden data that pins ``nessi_b200.tables`` (exact-rational
 derivation used by the CUDA library) and the oracle's own derivation.
 
-Usage:  python tests/golden/make_integration_golden.py [path/to/integration.cpp]
+Usage:  NESSI_REFERENCE_ROOT=<reference checkout> python tests/golden/make_integration_golden.py [path/to/integration.cpp]
 """
 import json
 import os
 import re
 import sys
 
-DEFAULT_SRC = "/root/reference/libcntr/cntr/integration.cpp"
+# default source: under NESSI_REFERENCE_ROOT, the reference checkout (the directory holding
+# libcntr/); a path given as the first argument overrides it
+DEFAULT_SRC = os.path.join(os.environ.get("NESSI_REFERENCE_ROOT", "."), "libcntr/cntr/integration.cpp")
 
 
 def _cases(body):

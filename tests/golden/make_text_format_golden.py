@@ -7,7 +7,7 @@ tests/test_hm_file.py then checks the writer against the text and the reader aga
 ReadCNTR.py uses np.int, which numpy 2 no longer has; the script supplies it as the builtin int
 for the duration of the call (the reference file itself is not touched).
 
-    python tests/golden/make_text_format_golden.py [path/to/libcntr/python3]
+    NESSI_REFERENCE_ROOT=<reference checkout> python tests/golden/make_text_format_golden.py [path/to/libcntr/python3]
 """
 import importlib.util
 import json
@@ -18,7 +18,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-DEFAULT_SRC = "/root/reference/libcntr/python3"
+# default source: under NESSI_REFERENCE_ROOT, the reference checkout (the directory holding
+# libcntr/); a path given as the first argument overrides it
+DEFAULT_SRC = os.path.join(os.environ.get("NESSI_REFERENCE_ROOT", "."), "libcntr/python3")
 TXT = os.path.join(HERE, "hm_text_small.txt")
 JSN = os.path.join(HERE, "hm_text_small.json")
 NT, NTAU, S, SIG = 3, 2, 2, -1
