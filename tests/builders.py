@@ -91,3 +91,60 @@ def u_matrices(U):
     for i in range(s):
         out[:, i, i] = U[:, i]
     return out
+
+
+# ---- problems of the benchmark configurations at full shape --------------------------------
+def fingerprints(G, nt, nproj=4):
+    """Projections of every time-step slice of G: for each t the ret row G^R(t, 0..t), the les
+    column G^<(0..t, t) and the tv row G^tv(t, .), flattened and projected onto nproj fixed
+    complex vectors v_j[i] = exp(2 pi i (i+1) alpha_j) / L of unit 1-norm, so that
+    |f - f_ref| <= max|x - x_ref| element by element.  Returns {comp: (nt+1, nproj) complex,
+    comp + "_max": max|x| over all slices}."""
+    alphas = np.array([0.6180339887498949, 0.4142135623730951, 0.7320508075688772, 0.2360679774997897])[:nproj]
+    out = {}
+    for comp in ("ret", "les", "tv"):
+        f = np.zeros((nt + 1, nproj), np.complex128)
+        mx = 0.0
+        for t in range(nt + 1):
+            x = (G.ret_row(t) if comp == "ret" else G.les_col(t) if comp == "les" else G.tv[t]).reshape(-1)
+            L = x.size
+            v = np.exp(2j * np.pi * np.outer(alphas, np.arange(1, L + 1))) / L
+            f[t] = v @ x
+            mx = max(mx, float(np.max(np.abs(x))))
+        out[comp] = f
+        out[comp + "_max"] = mx
+    return out
+
+
+def fingerprint_errors(fp, ref):
+    """max_t |f - f_ref| / max|x_ref| per component (a lower bound of the relative error of the
+    slices themselves)."""
+    return {c: float(np.max(np.abs(fp[c] - ref[c])) / ref[c + "_max"]) for c in ("ret", "les", "tv")}
+
+
+def config3_problem(s, nt, seed, ntau=400, beta=10.0, h=0.01, V=0.7, k=5):
+    """One problem of the uneven batch (config 3): h = (X + X^H)/2, X complex N(0, 0.5^2), a
+    rank-1 quench u u^H (u complex N(0, 0.3^2)) switched on at t = 0, Sigma = V^2 G_bath (x) 1_s;
+    bootstrap = the free propagator of h (mat and steps 0..k).  Returns (desc, H, Sigma, boot)."""
+    from nessi_b200 import equilibrium as eq
+    from nessi_b200.workloads import bootstrap_free
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, 0.5, (s, s)) + 1j * rng.normal(0, 0.5, (s, s))
+    h0 = (x + x.conj().T) / 2
+    u = rng.normal(0, 0.3, s) + 1j * rng.normal(0, 0.3, s)
+    H = np.zeros((nt + 2, s, s), np.complex128)
+    H[0] = h0
+    H[1:] = h0 + np.outer(u, u.conj())
+    Sig = eq.kron_identity(eq.semicircle_bath(nt, ntau, beta, h), s, V * V)
+    boot = bootstrap_free(h0, 0.0, beta, h, k, ntau)
+    desc = dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, sigma_group=0, beta=beta, h=h, mu=0.0)
+    return desc, H, Sig, boot
+
+
+def boot_to_full(boot, desc, k=5):
+    """herm_matrix(nt) holding mat and steps 0..k of a bootstrap."""
+    G = herm_matrix(desc["nt"], desc["ntau"], desc["size1"], desc["sig"])
+    G.mat[...] = boot.mat
+    for t in range(k + 1):
+        G.set_timestep_data(t, boot.get_timestep(t))
+    return G
