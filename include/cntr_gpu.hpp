@@ -168,13 +168,86 @@ inline void require_fixpoint(int method, bool force_hermitian = true) {
 }
 
 // ---- single-problem drop-ins (cntr_dyson_decl.hpp:78-92) -------------------------------
+namespace detail {
+// The device copy of the last problem stepped by cntr_gpu::dyson_timestep, kept between calls
+// (one per host thread), and the bytes the single-call functions moved across PCIe.
+struct StepCache {
+    nessi_batch *b = nullptr;
+    const void *G = nullptr, *Sigma = nullptr, *H = nullptr;
+    int nt = 0, ntau = 0, s = 0, sig = 0, k = 0, last_n = -2;
+    double mu = 0, beta = 0, h = 0;
+    void release() {
+        if (b) nessi_gpu_batch_destroy(b);
+        b = nullptr;
+        last_n = -2;
+    }
+    ~StepCache() { release(); }
+};
+inline StepCache &step_cache() {
+    thread_local StepCache c;
+    return c;
+}
+inline long long &transfer_bytes_counter() {
+    thread_local long long n = 0;
+    return n;
+}
+}  // namespace detail
+
+// Bytes copied between host and device by cntr_gpu::dyson_timestep on this thread so far.
+inline long long transfer_bytes() { return detail::transfer_bytes_counter(); }
+// Forget the device copy kept by cntr_gpu::dyson_timestep; the next call uploads everything.
+inline void dyson_timestep_reset() { detail::step_cache().release(); }
+
+// cntr::dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder).  The first call on a problem
+// uploads G, H and Sigma whole and keeps them on the device; a following call on the same objects
+// (same addresses and parameters) for the same n (a corrector iteration) or for n + 1 (the next
+// step) uploads only Sigma's time step n and H, and every call downloads only G's time step n.
+// So between such calls the caller may change Sigma's time step n and H -- as libcntr's
+// predictor-corrector drivers do -- but not G's or Sigma's earlier time steps; after changing
+// those, call dyson_timestep_reset() (any other n, or other objects, start over by themselves).
 template <class HM, class FN>
 void dyson_timestep(int n, HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveOrder = 5) {
-    Batch<HM, FN> b;
-    b.add(G, H, mu, beta, h, SolveOrder);
-    b.build(Sigma);
-    b.dyson_timestep(n);
-    b.download_timestep(0, n);
+    detail::StepCache &c = detail::step_cache();
+    const long es = (long)G.size1() * G.size1();
+    const bool same = c.b && c.G == (const void *)&G && c.Sigma == (const void *)&Sigma && c.H == (const void *)&H &&
+                      c.nt == G.nt() && c.ntau == G.ntau() && c.s == G.size1() && c.sig == G.sig() &&
+                      c.k == SolveOrder && c.mu == mu && c.beta == beta && c.h == h &&
+                      (n == c.last_n || n == c.last_n + 1);
+    const long tri = (long)(G.nt() + 1) * (G.nt() + 2) / 2 * es, tvn = (long)(G.nt() + 1) * (G.ntau() + 1) * es;
+    const long fn = (long)(G.nt() + 2) * es, matn = (long)(G.ntau() + 1) * es;
+    if (!same) {
+        c.release();
+        nessi_problem_desc d;
+        d.nt = G.nt(); d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
+        d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = h; d.mu = mu;
+        check(nessi_gpu_batch_create(&c.b, &d, 1, NESSI_PREC_FP64));
+        check(nessi_gpu_set_G(c.b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0)));
+        check(nessi_gpu_set_H(c.b, 0, H.ptr(-1)));
+        check(nessi_gpu_set_sigma(c.b, 0, Sigma.retptr(0, 0), Sigma.lesptr(0, 0), Sigma.tvptr(0, 0), Sigma.matptr(0)));
+        c.G = &G; c.Sigma = &Sigma; c.H = &H;
+        c.nt = G.nt(); c.ntau = G.ntau(); c.s = G.size1(); c.sig = G.sig(); c.k = SolveOrder;
+        c.mu = mu; c.beta = beta; c.h = h;
+        detail::transfer_bytes_counter() += 16 * (4 * tri + 2 * tvn + 2 * matn + fn);
+    } else {
+        std::vector<std::complex<double>> sl(slice_len(Sigma, n));
+        const long n1 = n + 1, M = G.ntau() + 1;
+        std::copy(Sigma.retptr(n, 0), Sigma.retptr(n, 0) + n1 * es, sl.begin());
+        std::copy(Sigma.tvptr(n, 0), Sigma.tvptr(n, 0) + M * es, sl.begin() + n1 * es);
+        for (long j = 0; j <= n; j++) std::copy(Sigma.lesptr(j, n), Sigma.lesptr(j, n) + es, sl.begin() + (n1 + M + j) * es);
+        check(nessi_gpu_set_sigma_timestep(c.b, 0, n, sl.data()));
+        check(nessi_gpu_set_H(c.b, 0, H.ptr(-1)));
+        detail::transfer_bytes_counter() += 16 * ((long)sl.size() + fn);
+    }
+    c.last_n = -2;  // a failure below leaves no reusable state
+    check(nessi_gpu_dyson_timestep(c.b, n));
+    std::vector<std::complex<double>> out(slice_len(G, n));
+    check(nessi_gpu_get_timestep(c.b, 0, n, out.data()));
+    const long n1 = n + 1, M = G.ntau() + 1;
+    std::copy(out.begin(), out.begin() + n1 * es, G.retptr(n, 0));
+    std::copy(out.begin() + n1 * es, out.begin() + (n1 + M) * es, G.tvptr(n, 0));
+    for (long j = 0; j <= n; j++) std::copy(out.begin() + (n1 + M + j) * es, out.begin() + (n1 + M + j + 1) * es, G.lesptr(j, n));
+    detail::transfer_bytes_counter() += 16 * (long)out.size();
+    c.last_n = n;
 }
 
 template <class HM, class FN>

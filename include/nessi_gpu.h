@@ -238,6 +238,15 @@ int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, c
                                const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1,
                                int sig_a, int sig_b, int solve_order, double beta, double h);
 
+/* cntr::distance_norm2(tstp, g1, g2) (cntr_utilities_decl.hpp, cntr_utilities_impl.hpp:607-650) between two
+ * herm_matrix held on the device (libcntr layout, caller-owned device pointers, tv as
+ * (t(ntau+1)+tau) s^2): the sum over the elements of time step tstp (ret row, tv row, les column;
+ * mat for tstp = -1) of the Frobenius norm of g1 - g2, written to the device double *out.  The
+ * reference's convergence measure of self-consistent loops, computed where the data are; queued
+ * on `stream` (NULL = legacy default stream), allocates nothing. */
+int nessi_gpu_distance_norm2(int tstp, const nessi_hm_ptrs *g1, const nessi_hm_ptrs *g2, int nt, int ntau, int size1,
+                             double *out, void *stream);
+
 /* Volterra kernels in use for a group: -1 = one problem per CTA, 2/4/8 = problems per CTA of the
  * tensor-core kernels, 100 = the group-wide blocked recursion by thread-block clusters (trailing
  * updates on the FP64 tensor cores), 0 = not chosen yet (the autotuner decides at the first eager step with

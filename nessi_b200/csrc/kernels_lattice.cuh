@@ -222,3 +222,46 @@ __global__ void k_sigma_2b(GroupDev g, LocDev loc, const double2 *__restrict__ u
         }
     }
 }
+
+// ---------------------------------------------------------------------------------------
+// k_distance_norm2: cntr::distance_norm2(tstp, g1, g2) (cntr_utilities_impl.hpp:607-650) on
+// device herm_matrix data in libcntr's layout: the sum over the elements of time step tstp (ret
+// row, tv row, les column; mat for tstp = -1) of the Frobenius norm of g1 - g2.  One block;
+// every thread sums a fixed strided subset and the partial sums are added in a fixed tree, so
+// the result does not depend on scheduling.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_distance_norm2(int tstp, ConvHM g1, ConvHM g2, int ntau, int s2,
+                                                        double *out) {
+    __shared__ double part[256];
+    const int M = ntau + 1;
+    const long n1 = tstp + 1;
+    const long nel = tstp < 0 ? M : 2 * n1 + M;
+    double acc = 0.0;
+    for (long e = threadIdx.x; e < nel; e += 256) {
+        const double2 *a, *b;
+        if (tstp < 0) {
+            a = g1.mat + e * s2; b = g2.mat + e * s2;
+        } else if (e < n1) {        // ret(tstp, e)
+            a = g1.ret + (tri(tstp) + e) * s2; b = g2.ret + (tri(tstp) + e) * s2;
+        } else if (e < n1 + M) {    // tv(tstp, tau)
+            const long tau = e - n1;
+            a = g1.tv + ((long)tstp * M + tau) * s2; b = g2.tv + ((long)tstp * M + tau) * s2;
+        } else {                    // les(i, tstp)
+            const long i = e - n1 - M;
+            a = g1.les + (tri(tstp) + i) * s2; b = g2.les + (tri(tstp) + i) * s2;
+        }
+        double r = 0.0;
+        for (int i = 0; i < s2; i++) {
+            const double dx = a[i].x - b[i].x, dy = a[i].y - b[i].y;
+            r += dx * dx + dy * dy;
+        }
+        acc += sqrt(r);
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = part[0];
+}

@@ -17,8 +17,8 @@
 #include "kernels_dyson.cuh"
 #include "kernels_start.cuh"
 #include "kernels_mat.cuh"
-#include "kernels_lattice.cuh"
 #include "kernels_conv.cuh"
+#include "kernels_lattice.cuh"
 
 
 
@@ -1705,4 +1705,26 @@ extern "C" int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm
                                           int sig_a, int sig_b, int solve_order, double beta, double h) {
     return convolution_host_range(-1, nt, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h,
                                   "convolution_host");
+}
+
+// =====================================================================================
+// distance_norm2 on device-resident herm_matrix data
+// =====================================================================================
+extern "C" int nessi_gpu_distance_norm2(int tstp, const nessi_hm_ptrs *g1, const nessi_hm_ptrs *g2, int nt, int ntau,
+                                        int size1, double *out, void *stream) {
+    NvtxRange nvtx_("nessi::distance_norm2");
+    if (!g1 || !g2 || !out || nt < -1 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS || tstp < -1 || tstp > nt) {
+        set_err("distance_norm2: bad arguments (tstp=%d nt=%d ntau=%d size1=%d)", tstp, nt, ntau, size1);
+        return NESSI_ERR_ARG;
+    }
+    const bool ok = tstp < 0 ? (g1->mat && g2->mat) : (g1->ret && g1->les && g1->tv && g2->ret && g2->les && g2->tv);
+    if (!ok) { set_err("distance_norm2: a component it reads is null"); return NESSI_ERR_ARG; }
+    auto conv = [](const nessi_hm_ptrs &x) {
+        ConvHM y;
+        y.ret = (double2 *)x.ret; y.les = (double2 *)x.les; y.tv = (double2 *)x.tv; y.mat = (double2 *)x.mat;
+        return y;
+    };
+    k_distance_norm2<<<1, 256, 0, (cudaStream_t)stream>>>(tstp, conv(*g1), conv(*g2), ntau, size1 * size1, out);
+    CK(cudaGetLastError());
+    return NESSI_OK;
 }

@@ -90,6 +90,8 @@ EXPORTS = {
                                             [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double]),
     "nessi_gpu_convolution_host": (ctypes.c_int, [ctypes.POINTER(HmPtrs)] * 5 + [ctypes.c_int] * 6 +
                                    [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_distance_norm2": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(HmPtrs), ctypes.POINTER(HmPtrs)] +
+                                 [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_void_p]),
     "nessi_gpu_get_volterra_choice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                      ctypes.POINTER(ctypes.c_int)]),
     "nessi_gpu_graph_record": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 4),
@@ -345,6 +347,13 @@ def dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, H_ptr, sigma_mat_
     _check(load_library().nessi_gpu_dyson_mat_noalloc(ntau, size1, sig, solve_order, beta, mu, ctypes.c_void_p(H_ptr),
                                                        ctypes.c_void_p(sigma_mat_ptr), ctypes.c_void_p(gmat_ptr),
                                                        ctypes.c_void_p(stream) if stream else None))
+
+
+def distance_norm2_dev(tstp, g1, g2, nt, ntau, size1, out_ptr, stream=0):
+    """nessi_gpu_distance_norm2 on device herm_matrix data: g1, g2 are HmPtrs (device pointers,
+    libcntr layout); the result is written to the device double at out_ptr."""
+    _check(load_library().nessi_gpu_distance_norm2(tstp, ctypes.byref(g1), ctypes.byref(g2), nt, ntau, size1,
+                                                    ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream) if stream else None))
 
 
 def convolution_timestep_dev(n, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, stream=0):

@@ -2,7 +2,7 @@
 // herm_matrix / function pair with libcntr's accessors and layout, filled from raw files
 // (complex128, libcntr layout), one cntr_gpu call, the result written back.
 //
-//   cxx_frontend <mode> <dir>      mode: echo | algebra | mat | dyson | steps | vie2 | sin | conv
+//   cxx_frontend <mode> <dir>      mode: echo | algebra | mat | dyson | steps | correct | vie2 | sin | conv
 //
 // Files in <dir>: dims.txt ("nt ntau size1 sig k beta h mu"), and <name>.{ret,les,tv,mat}
 // for the herm_matrix operands (H.fn for the function).  The result is G (or C).
@@ -69,7 +69,7 @@ static void save_hm(const HM &G, const std::string &base) {
 
 int main(int argc, char **argv) {
     if (argc != 3) {
-        std::fprintf(stderr, "usage: %s echo|algebra|mat|dyson|steps|vie2|sin|conv <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s echo|algebra|mat|dyson|steps|correct|vie2|sin|conv <dir>\n", argv[0]);
         return 2;
     }
     const std::string mode = argv[1], dir = std::string(argv[2]) + "/";
@@ -123,6 +123,33 @@ int main(int argc, char **argv) {
                 cntr_gpu::dyson_start(G, mu, H, Sigma, beta, h, k);
                 for (int n = k + 1; n <= nt; n++) cntr_gpu::dyson_timestep(n, G, mu, H, Sigma, beta, h, k);
             }
+            save_hm(G, dir + "out");
+        } else if (mode == "correct") {  // the single-call step in a predictor-corrector loop
+            HM Sigma(nt, ntau, s, sig);
+            FN H(nt, s);
+            load_hm(Sigma, dir + "Sigma");
+            load(H.d_, dir + "H.fn");
+            cntr_gpu::dyson_mat(G, mu, H, Sigma, beta, k);
+            cntr_gpu::dyson_start(G, mu, H, Sigma, beta, h, k);
+            const long es = (long)s * s;
+            long long first = -1, most = 0;
+            for (int n = k + 1; n <= nt; n++) {
+                // Sigma's time step n is recomputed between the calls (here: scaled copies of it)
+                std::vector<cplx> r0(Sigma.retptr(n, 0), Sigma.retptr(n, 0) + (n + 1) * es);
+                std::vector<cplx> t0(Sigma.tvptr(n, 0), Sigma.tvptr(n, 0) + (ntau + 1) * es);
+                std::vector<cplx> l0(Sigma.lesptr(0, n), Sigma.lesptr(0, n) + (n + 1) * es);
+                for (int it = 0; it < 3; it++) {
+                    const double f = 1.0 + 0.001 * (it - 1);
+                    for (size_t i = 0; i < r0.size(); i++) Sigma.retptr(n, 0)[i] = f * r0[i];
+                    for (size_t i = 0; i < t0.size(); i++) Sigma.tvptr(n, 0)[i] = f * t0[i];
+                    for (size_t i = 0; i < l0.size(); i++) Sigma.lesptr(0, n)[i] = f * l0[i];
+                    const long long before = cntr_gpu::transfer_bytes();
+                    cntr_gpu::dyson_timestep(n, G, mu, H, Sigma, beta, h, k);
+                    const long long moved = cntr_gpu::transfer_bytes() - before;
+                    if (first < 0) first = moved; else if (moved > most) most = moved;
+                }
+            }
+            std::ofstream(dir + "bytes.txt") << first << " " << most << "\n";
             save_hm(G, dir + "out");
         } else if (mode == "vie2") {
             HM F(nt, ntau, s, sig), Fcc(nt, ntau, s, sig), Q(nt, ntau, s, sig);

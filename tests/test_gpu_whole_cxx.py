@@ -171,6 +171,38 @@ def test_dyson_through_the_cxx_frontend(oracle, tmp_path, mode):
 
 
 @pytest.mark.gpu
+def test_single_call_step_in_a_corrector_loop(oracle, tmp_path):
+    """cntr_gpu::dyson_timestep called three times per time step with Sigma's time step n changed
+    between the calls (a predictor-corrector driver): the device copy is kept, each call after
+    the first moves O(n) data (Sigma's and G's slice n and H), and G equals the oracle's run of
+    the same call sequence."""
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(43)
+    nt, ntau, s, beta, h, k, mu = 50, 16, 2, 3.0, 0.05, 5, 0.1
+    Sig = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h)
+    H = make_H(rng, nt, s, h)
+    d = tmp_path / "correct"
+    write_case(d, (nt, ntau, s, -1, k, beta, h, mu), Sigma=Sig, H=getattr(H, "data", H))
+    run(exe, "correct", d)
+    G = read_out(d, nt, ntau, s, -1)
+    ref = herm_matrix(nt, ntau, s, -1)
+    oracle.dyson_mat(ref, Sig, mu, H, beta, k)
+    oracle.dyson_start(ref, mu, H, Sig, beta, h, k)
+    S = Sig.copy()
+    for n in range(k + 1, nt + 1):
+        orig = S.get_timestep(n).copy()
+        for it in range(3):
+            S.set_timestep_data(n, orig * (1.0 + 0.001 * (it - 1)))
+            oracle.dyson_timestep(n, ref, mu, H, S, beta, h, k)
+    e = component_errors(G, ref, 0, nt)
+    assert max(e.values()) < TOL, e
+    first, most = (int(x) for x in open(d / "bytes.txt").read().split())
+    slice_bytes = 16 * (2 * (nt + 1) + ntau + 1) * s * s
+    assert most <= 2 * slice_bytes + 16 * (nt + 2) * s * s, (first, most)
+    assert first > 20 * most
+
+
+@pytest.mark.gpu
 def test_vie2_through_the_cxx_frontend(oracle, tmp_path):
     exe = build_frontend(tmp_path)
     rng = np.random.default_rng(43)
