@@ -8,10 +8,11 @@
 // (p, d), so one product serves every k-point that shares Sigma.
 //
 // A tile group of 4 warps (128 threads) computes a BM x BN tile of C = A B (complex, row-major
-// C[r][c]); each warp owns a 32 x 32 sub-tile as 2 x 4 m16n8 fragments, real and imaginary
-// parts accumulated separately (four real MMAs per complex fragment product).  Operands are read
-// through loader objects, so that a GEMM can read a triangle, a scaled panel or a dense matrix
-// in place: get(mn, k) returns A(m, k) (or B(k, n)) and zero outside the operand; KC tells
+// C[r][c]); each warp owns a (16 MT) x (8 NT) sub-tile as MT x NT m16n8 fragments (32 x 32 or
+// 32 x 16), real and imaginary parts accumulated separately (four real MMAs per complex fragment
+// product).  The smaller warp tile doubles the tiles of a product, for shapes that give too few
+// 64 x 64 tiles to fill the 148 SMs.  Operands are read through loader objects, so that a GEMM
+// can read a triangle, a scaled panel or a dense matrix in place: get(mn, k) returns A(m, k) (or B(k, n)) and zero outside the operand; KC tells
 // whether consecutive k are adjacent in memory (then consecutive threads load consecutive k,
 // otherwise consecutive m / n).  The k loop stages BK complex columns of A and rows of B per
 // step through double-buffered shared memory, loading the next step into registers while the
@@ -47,21 +48,22 @@ __device__ __forceinline__ void zg_sync(int grp) { asm volatile("bar.sync %0, 12
 // C tile (m0.., n0..) of C = A B over k = 0..K-1, by the 128 threads t = 0..127 of tile group grp.
 // put(r, c, v) receives every element of the tile (the loaders return zero outside A and B, so
 // rows / columns beyond the matrices carry zeros; put filters them).
-template <int BM, int BN, class LA, class LB, class PUT>
+template <int BM, int BN, class LA, class LB, class PUT, int NT = 4>
 __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT &put, int m0, int n0, int K,
                                            double2 *sm, int t, int grp) {
     using namespace zg;
-    constexpr int WN = BN / 32, WM = BM / 32;
-    static_assert(WM * WN == 4, "tile group = 4 warps of 32 x 32");
+    constexpr int MT = 2, WTN = 8 * NT;  // warp tile 32 x WTN
+    constexpr int WN = BN / WTN, WM = BM / 32;
+    static_assert(WM * WN == 4, "tile group = 4 warps");
     constexpr int AE = BM * BK / NTH, BE = BN * BK / NTH;
     double2 *As0 = sm, *Bs0 = sm + BM * LDS;
     const int warp = t >> 5, lane = t & 31, wm = warp / WN, wn = warp % WN;
     const int g = lane >> 2, q = lane & 3;
-    double acc[2][4][2][4];
+    double acc[MT][NT][2][4];
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < MT; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++)
+        for (int j = 0; j < NT; j++)
 #pragma unroll
             for (int c = 0; c < 2; c++)
 #pragma unroll
@@ -106,10 +108,10 @@ __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT
         const int cur = kt & 1;
         if (kt + 1 < nk) gload((kt + 1) * BK);
         const double2 *As = As0 + cur * Smem<BM, BN>::stage + (wm * 32) * LDS;
-        const double2 *Bs = Bs0 + cur * Smem<BM, BN>::stage + (wn * 32) * LDS;
-        double ar[2][4], ai[2][4], an[2][4], br[4][2], bi[4][2];
+        const double2 *Bs = Bs0 + cur * Smem<BM, BN>::stage + (wn * WTN) * LDS;
+        double ar[MT][4], ai[MT][4], an[MT][4], br[NT][2], bi[NT][2];
 #pragma unroll
-        for (int i = 0; i < 2; i++)
+        for (int i = 0; i < MT; i++)
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 const double2 x = As[(i * 16 + g + 8 * (v & 1)) * LDS + q + 4 * (v >> 1)];
@@ -118,7 +120,7 @@ __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT
                 an[i][v] = -x.y;
             }
 #pragma unroll
-        for (int j = 0; j < 4; j++)
+        for (int j = 0; j < NT; j++)
 #pragma unroll
             for (int v = 0; v < 2; v++) {
                 const double2 x = Bs[(j * 8 + g) * LDS + q + 4 * v];
@@ -126,9 +128,9 @@ __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT
                 bi[j][v] = x.y;
             }
 #pragma unroll
-        for (int i = 0; i < 2; i++)
+        for (int i = 0; i < MT; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
+            for (int j = 0; j < NT; j++) {
                 dmma1688(acc[i][j][0], ar[i], br[j]);
                 dmma1688(acc[i][j][0], an[i], bi[j]);
                 dmma1688(acc[i][j][1], ar[i], bi[j]);
@@ -138,13 +140,13 @@ __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT
         zg_sync(grp);
     }
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < MT; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++)
+        for (int j = 0; j < NT; j++)
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const int r = m0 + wm * 32 + i * 16 + g + 8 * (e >> 1);
-                const int c = n0 + wn * 32 + j * 8 + 2 * q + (e & 1);
+                const int c = n0 + wn * WTN + j * 8 + 2 * q + (e & 1);
                 put(r, c, cmk(acc[i][j][0][e], acc[i][j][1][e]));
             }
 }
@@ -187,8 +189,8 @@ struct StRow {
 
 // Standalone product: grid (ceil(N / BN), ceil(M / BM)), 128 threads, zg::Smem<BM,BN>::total
 // complex of dynamic shared memory.
-template <int BM, int BN, class LA, class LB, class PUT>
+template <int BM, int BN, int NT, class LA, class LB, class PUT>
 __global__ void __launch_bounds__(128) k_zgemm(LA la, LB lb, PUT put, int K) {
     extern __shared__ double2 zsm[];
-    zgemm_tile<BM, BN>(la, lb, put, blockIdx.y * BM, blockIdx.x * BN, K, zsm, threadIdx.x, 0);
+    zgemm_tile<BM, BN, LA, LB, PUT, NT>(la, lb, put, blockIdx.y * BM, blockIdx.x * BN, K, zsm, threadIdx.x, 0);
 }

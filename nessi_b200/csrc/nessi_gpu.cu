@@ -249,24 +249,25 @@ template <int S> size_t les_smem(int k) {
     return std::max(start, phase);
 }
 
-// C (M x N) = A (M x K) B (K x N) on the repo's DMMA GEMM (kernels_gemm.cuh): 64 x 64 tiles, or
-// 128 x 32 when the problem columns are few.
+// C (M x N) = A (M x K) B (K x N) on the repo's DMMA GEMM (kernels_gemm.cuh): 64 x 64 tiles when
+// they fill the GPU twice over, else 64 x 32 tiles (warp tiles of 32 x 16); 128 x 32 tiles when
+// the problem columns are few.
+template <int BM, int BN, int NT, class LA, class LB, class ST>
+int zgemm_launch_tiles(const LA &la, const LB &lb, const ST &st, int M, int N, int K, cudaStream_t s) {
+    const dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
+    const size_t sm = (size_t)zg::Smem<BM, BN>::total * sizeof(double2);
+    CK(cudaFuncSetAttribute(k_zgemm<BM, BN, NT, LA, LB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_zgemm<BM, BN, NT><<<grid, 128, sm, s>>>(la, lb, st, K);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
 template <class LA, class LB, class ST>
 int zgemm_launch(const LA &la, const LB &lb, const ST &st, int M, int N, int K, cudaStream_t s) {
     if (M <= 0 || N <= 0) return NESSI_OK;
-    if (N > 32) {
-        const dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
-        const size_t sm = (size_t)zg::Smem<64, 64>::total * sizeof(double2);
-        CK(cudaFuncSetAttribute(k_zgemm<64, 64, LA, LB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_zgemm<64, 64><<<grid, 128, sm, s>>>(la, lb, st, K);
-    } else {
-        const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((M + 127) / 128));
-        const size_t sm = (size_t)zg::Smem<128, 32>::total * sizeof(double2);
-        CK(cudaFuncSetAttribute(k_zgemm<128, 32, LA, LB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_zgemm<128, 32><<<grid, 128, sm, s>>>(la, lb, st, K);
-    }
-    CK(cudaGetLastError());
-    return NESSI_OK;
+    if (N <= 32) return zgemm_launch_tiles<128, 32, 4>(la, lb, st, M, N, K, s);
+    const long tiles64 = (long)((M + 63) / 64) * ((N + 63) / 64);
+    if (tiles64 >= 2 * 148) return zgemm_launch_tiles<64, 64, 4>(la, lb, st, M, N, K, s);
+    return zgemm_launch_tiles<64, 32, 2>(la, lb, st, M, N, K, s);
 }
 
 // Volterra choice code of the group-wide cluster path (k_ret_start / k_les_start + k_volterra_cl)
