@@ -249,9 +249,9 @@ int nessi_gpu_distance_norm2(int tstp, const nessi_hm_ptrs *g1, const nessi_hm_p
 
 /* Volterra kernels in use for a group: -1 = one problem per CTA, 2/4/8 = problems per CTA of the
  * tensor-core kernels, 100 = the group-wide blocked recursion by thread-block clusters (trailing
- * updates on the FP64 tensor cores), 0 = not chosen yet (the autotuner decides at the first eager step with
- * n >= min(128, nt); the environment variable NESSI_VOLTERRA_PP read at batch creation fixes
- * the choice).  No reference counterpart. */
+ * updates on the FP64 tensor cores), 0 = not chosen yet (the autotuner decides at the first eager
+ * step with n >= max(min(128, nt), 3 nt / 4); the environment variable NESSI_VOLTERRA_PP read at
+ * batch creation fixes the choice).  No reference counterpart. */
 int nessi_gpu_get_volterra_choice(nessi_batch *b, int group, int *pp_ret, int *pp_les);
 
 /* ---- CUDA graphs of the per-step launch sequence ---------------------------------------------

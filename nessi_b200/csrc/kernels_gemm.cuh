@@ -46,8 +46,8 @@ __device__ __forceinline__ void dmma1688(double *d, const double *a, const doubl
 __device__ __forceinline__ void zg_sync(int grp) { asm volatile("bar.sync %0, 128;" ::"r"(grp + 1) : "memory"); }
 
 // C tile (m0.., n0..) of C = A B over k = 0..K-1, by the 128 threads t = 0..127 of tile group grp.
-// put(r, c, v) receives every element of the tile (the loaders return zero outside A and B, so
-// rows / columns beyond the matrices carry zeros; put filters them).
+// Every element of the tile goes through the store object `put` (the loaders return zero outside
+// A and B, so rows / columns beyond the matrices carry zeros; put filters them).
 template <int BM, int BN, class LA, class LB, class PUT, int NT = 4>
 __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT &put, int m0, int n0, int K,
                                            double2 *sm, int t, int grp) {
@@ -139,6 +139,18 @@ __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT
         if (kt + 1 < nk) sstore(cur ^ 1);
         zg_sync(grp);
     }
+    // epilogue: an accumulating store first reads every old value of the thread's fragments (the
+    // loads are independent and overlap), then writes all sums
+    double2 old[MT][NT][4];
+    if (put.accumulates()) {
+#pragma unroll
+        for (int i = 0; i < MT; i++)
+#pragma unroll
+            for (int j = 0; j < NT; j++)
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    old[i][j][e] = put.load(m0 + wm * 32 + i * 16 + g + 8 * (e >> 1), n0 + wn * WTN + j * 8 + 2 * q + (e & 1));
+    }
 #pragma unroll
     for (int i = 0; i < MT; i++)
 #pragma unroll
@@ -147,7 +159,8 @@ __device__ __forceinline__ void zgemm_tile(const LA &la, const LB &lb, const PUT
             for (int e = 0; e < 4; e++) {
                 const int r = m0 + wm * 32 + i * 16 + g + 8 * (e >> 1);
                 const int c = n0 + wn * WTN + j * 8 + 2 * q + (e & 1);
-                put(r, c, cmk(acc[i][j][0][e], acc[i][j][1][e]));
+                const double2 v = cmk(acc[i][j][0][e], acc[i][j][1][e]);
+                put.store(r, c, put.accumulates() ? put.combine(old[i][j][e], v) : put.combine(cmk(0, 0), v));
             }
 }
 
@@ -172,6 +185,8 @@ struct LdRowN {
         return (n < cols && k < rows) ? __ldg(p + (long)k * ld + n) : cmk(0, 0);
     }
 };
+// Stores of a GEMM tile: accumulates() tells whether C's old value takes part, load(r, c) reads
+// it (zero outside C), combine(old, v) forms the new value and store(r, c, x) writes it inside C.
 // C[r][c] = alpha v (+ C[r][c] when accumulate), r < rows, c < cols
 struct StRow {
     double2 *p;
@@ -179,11 +194,13 @@ struct StRow {
     int rows, cols;
     double alpha;
     int accumulate;
-    __device__ __forceinline__ void operator()(int r, int c, double2 v) const {
-        if (r >= rows || c >= cols) return;
-        double2 *q = p + (long)r * ld + c;
-        v = cscale(v, alpha);
-        *q = accumulate ? cadd(*q, v) : v;
+    __device__ __forceinline__ bool accumulates() const { return accumulate != 0; }
+    __device__ __forceinline__ double2 load(int r, int c) const {
+        return (r < rows && c < cols) ? p[(long)r * ld + c] : cmk(0, 0);
+    }
+    __device__ __forceinline__ double2 combine(double2 old, double2 v) const { return cadd(old, cscale(v, alpha)); }
+    __device__ __forceinline__ void store(int r, int c, double2 x) const {
+        if (r < rows && c < cols) p[(long)r * ld + c] = x;
     }
 };
 

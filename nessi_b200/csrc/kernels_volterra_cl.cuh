@@ -91,10 +91,13 @@ struct StCl {
     double2 *p;
     long ld;
     int M, cmax, accumulate;
-    __device__ __forceinline__ void operator()(int r, int c, double2 v) const {
-        if (r >= M || c >= cmax) return;
-        double2 *q = p + (long)r * ld + c;
-        *q = accumulate ? cadd(ldcg2(q), v) : v;
+    __device__ __forceinline__ bool accumulates() const { return accumulate != 0; }
+    __device__ __forceinline__ double2 load(int r, int c) const {
+        return (r < M && c < cmax) ? ldcg2(p + (long)r * ld + c) : cmk(0, 0);
+    }
+    __device__ __forceinline__ double2 combine(double2 old, double2 v) const { return cadd(old, v); }
+    __device__ __forceinline__ void store(int r, int c, double2 x) const {
+        if (r < M && c < cmax) p[(long)r * ld + c] = x;
     }
 };
 

@@ -282,6 +282,38 @@ template <int S> size_t les_start_smem(int k) {
     return (size_t)((K1 * S) * (K1 * S) + K1 * S * S) * 16 + 16;
 }
 
+// Clusters of k_volterra_cl that can be resident at once (8 CTAs of one SM each must fit in a
+// GPC), asked once per instantiation; the recursion uses at most that many, so that no cluster
+// waits for another to finish.
+template <int S, bool VIE, bool RET, int BN> int max_active_clusters() {
+    static int cached = -1;
+    if (cached > 0) return cached;
+    const size_t sm = (size_t)std::max(ClSmem<S>::diag, ClGemm<BN>::smem) * sizeof(double2);
+    auto kern = k_volterra_cl<S, VIE, RET, BN>;
+    int num = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(NESSI_CL * 32));
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = sm;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = NESSI_CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&num, kern, &cfg) != cudaSuccess) {
+            cudaGetLastError();  // a failed query leaves no error behind; the launch reports its own
+            num = 0;
+        }
+    } else {
+        cudaGetLastError();
+    }
+    cached = num > 0 ? num : 16;
+    return cached;
+}
+
 template <int S, bool VIE, bool RET, int BN>
 int cluster_kernel_launch(const GroupDev &gd, const Group &g, int n, int nact, int PT, int ncl, double2 *acc,
                           double2 *panel, cudaStream_t st) {
@@ -305,8 +337,8 @@ int cluster_kernel_launch(const GroupDev &gd, const Group &g, int n, int nact, i
 }
 
 // Group-wide recursion: the start block of every problem (one CTA each), then the blocked
-// recursion by clusters of NESSI_CL CTAs, each owning PT problems (about 18 clusters fill the
-// 148 SMs; at most NESSI_CL x ClCfg::DWMAX problems, one chain warp each).
+// recursion by clusters of NESSI_CL CTAs, each owning PT problems (at most NESSI_CL x
+// ClCfg::DWMAX problems, one chain warp each).
 template <int S, bool VIE>
 int cluster_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret, cudaStream_t st) {
     if (ret) {
@@ -320,7 +352,11 @@ int cluster_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret
     }
     CK(cudaGetLastError());
     if (n - gd.k <= 0) return NESSI_OK;  // no unknowns below / above the start block
-    int PT = (nact + 17) / 18;
+    // as many clusters as fit at once (about 16 on 148 SMs), each with PT problems
+    int nfit = ret ? max_active_clusters<S, VIE, true, 32>() : max_active_clusters<S, VIE, false, 32>();
+    if constexpr (S <= 2)
+        nfit = std::min(nfit, ret ? max_active_clusters<S, VIE, true, 64>() : max_active_clusters<S, VIE, false, 64>());
+    int PT = (nact + nfit - 1) / nfit;
     PT = std::max(1, std::min(PT, NESSI_CL * ClCfg<S>::DWMAX));
     const int ncl = (nact + PT - 1) / PT;
     double2 *acc = ret ? g.accr : g.accl;
@@ -367,11 +403,14 @@ template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &
 }
 
 // Autotuner of the Volterra kernels.  With volterra_pp = 0 (default), the first eager step of a
-// group with n >= min(128, ntmax) launches every candidate (one-problem kernels, and for
-// size1 <= 2 the multi-problem kernels with 2, 4, 8 problems per CTA) on the step itself --
-// each launch recomputes the same row / column from the same inputs, so the last one leaves
-// the step's result -- times them with CUDA events and keeps the fastest for the group.  Until
-// then, and while a graph is being recorded, the one-problem kernels run.
+// group with n >= the tuning step launches every candidate (one-problem kernels, for size1 <= 2
+// the multi-problem kernels with 2, 4, 8 problems per CTA, and the group-wide cluster recursion)
+// on the step itself -- each launch recomputes the same row / column from the same inputs, so the
+// last one leaves the step's result -- times them with CUDA events and keeps the fastest for the
+// group.  The tuning step is 3/4 of the group's longest history (at least min(128, ntmax)): the
+// cost of a step grows as n^2, so the late steps carry most of a propagation and the kernels'
+// ranking there is the one that counts.  Until then, and while a graph is being recorded, the
+// one-problem kernels run.
 template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const GroupDev &gd, int n, int nact, bool ret,
                                              cudaStream_t st) {
     int &choice = ret ? g.pp_ret : g.pp_les;
@@ -379,8 +418,8 @@ template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const Gro
     if (choice != 0) return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cap));
-    if (cap != cudaStreamCaptureStatusNone || n < std::min(128, g.ntmax))
-        return volterra_launch<S, VIE>(gd, g, n, nact, ret, -1, st);
+    const int tune_n = std::max(std::min(128, g.ntmax), (3 * g.ntmax) / 4);
+    if (cap != cudaStreamCaptureStatusNone || n < tune_n) return volterra_launch<S, VIE>(gd, g, n, nact, ret, -1, st);
     // candidates: one problem per CTA, the per-CTA tensor-core kernels (size1 <= 2), the cluster path
     const int cand_small[5] = {-1, 2, 4, 8, NESSI_VOLTERRA_CLUSTER}, cand_big[2] = {-1, NESSI_VOLTERRA_CLUSTER};
     const int *cand = S <= 2 ? cand_small : cand_big;
@@ -711,7 +750,12 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
         set_err("stream creation failed");
         return fail(NESSI_ERR_CUDA);
     }
-    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+    // the side stream carries the retarded recursion, the longer of the two concurrent paths of a
+    // step; at the highest priority its CTAs are scheduled ahead of the history stream's, which
+    // keeps HBM busy with whatever SMs remain
+    int prio_lo = 0, prio_hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) prio_hi = 0;
+    if (cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         set_err("stream/event creation failed");
