@@ -17,14 +17,15 @@
 #pragma once
 
 #define MP_JB 32  // rows per block (lane = row)
+#define MP_NW 16  // warps per CTA: warps 0..PP-1 own a problem's chain, all of them share phase A
 
 template <int S> struct MpCfg {
     static constexpr int s2 = S * S;
     static constexpr int TRI = MP_JB * (MP_JB - 1) / 2;    // packed strictly-lower block triangle
     static constexpr int WSW = 2 * NESSI_K1MAX * NESSI_K1MAX * s2 + 2 * NESSI_K1MAX * s2 + 2;  // start work/warp
     static constexpr int acc = 0;                           // 8 problems x 32 rows x s2: phase-A sums
-    static constexpr int red = acc + 8 * MP_JB * s2;        // 8 warps x 32 lanes x 2 double2: partial tiles
-    static constexpr int sig = red + 8 * 32 * 2;            // TRI x s2
+    static constexpr int red = acc + 8 * MP_JB * s2;        // MP_NW warps x 32 lanes x 2 double2: partial tiles
+    static constexpr int sig = red + MP_NW * 32 * 2;        // TRI x s2
     static constexpr int wb = sig + TRI * s2;               // TRI doubles
     static constexpr int total = wb + TRI / 2 + 1;
     static_assert(sig + TRI * s2 >= 8 * WSW, "start workspaces must fit below the weights");
@@ -66,15 +67,15 @@ __device__ __forceinline__ void ztile884(const FA &fa, const FB &fb, int mt, int
 }
 
 // Phase A of one block as a complex GEMM C (R x N) = A (R x K) B (K x N) on the tensor cores, the
-// 8 warps sharing the tiles (and the k-steps when there are fewer than 8 tiles, summed in warp
-// order).  put(r, c, value) stores an element of C.
+// MP_NW warps sharing the tiles (and the k-steps when there are fewer than MP_NW tiles, summed in
+// warp order).  put(r, c, value) stores an element of C.
 template <class FA, class FB, class PUT>
 __device__ void zgemm_cta(const FA &fa, const FB &fb, const PUT &put, int R, int N, int K, double2 *red, int warp,
                           int lane) {
     const int MT = (R + 7) / 8, NT = (N + 7) / 8, tiles = MT * NT;
     const int r0 = lane >> 2, c0 = 2 * (lane & 3);
-    if (tiles >= 8) {
-        for (int t = warp; t < tiles; t += 8) {
+    if (tiles >= MP_NW) {
+        for (int t = warp; t < tiles; t += MP_NW) {
             double c[4] = {0, 0, 0, 0};
             ztile884(fa, fb, t / NT, t % NT, K, 0, 1, lane, c);
             const int r = (t / NT) * 8 + r0, cc = (t % NT) * 8 + c0;
@@ -84,7 +85,7 @@ __device__ void zgemm_cta(const FA &fa, const FB &fb, const PUT &put, int R, int
         __syncthreads();
         return;
     }
-    const int ksplit = 8 / tiles, t = warp % tiles, ks0 = warp / tiles;
+    const int ksplit = MP_NW / tiles, t = warp % tiles, ks0 = warp / tiles;
     double c[4] = {0, 0, 0, 0};
     if (ks0 < ksplit) ztile884(fa, fb, t / NT, t % NT, K, ks0, ksplit, lane, c);
     red[(warp * 32 + lane) * 2] = cmk(c[0], c[2]);
@@ -240,7 +241,7 @@ __device__ void mp_les_chain(double2 *a_, const double2 *sig, const double *wb, 
 // Phase A of block [jlo, jhi] for the CTA's problems q as C[(q,a)][(jj,d)] =
 //   sum_{(m,b)} c_m G_q(n,m)[a][b] Sigma^R(m, jlo+jj)[b][d],  m = jhi+1 .. n.
 template <int S, bool VIE>
-__global__ void __launch_bounds__(256) k_ret_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
+__global__ void __launch_bounds__(MP_NW * 32) k_ret_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
                                                 int PP) {
     extern __shared__ double2 smem[];
     using C = MpCfg<S>;
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(256) k_ret_mp(GroupDev g, const ProbDev *__res
     const int jtop = n - k - 1;
     for (int jhi = jtop; jhi >= 0; jhi -= MP_JB) {
         const int jlo = jhi - MP_JB + 1 < 0 ? 0 : jhi - MP_JB + 1, nb = jhi - jlo + 1;
-        for (int e = tid; e < C::TRI * s2; e += 256) {
+        for (int e = tid; e < C::TRI * s2; e += MP_NW * 32) {
             const int q = e / s2, ab = e % s2;
             int r, r2;
             pk_inv(q, r, r2);
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(256) k_ret_mp(GroupDev g, const ProbDev *__res
 // Phase A of block [jlo, jhi] as C[(jj,a)][(q,d)] =
 //   sum_{(m,b)} Sigma^R(jlo+jj, m)[a][b] c'_m G^<_q(m,n)[b][d],  m = 0 .. jlo-1.
 template <int S, bool VIE>
-__global__ void __launch_bounds__(256) k_les_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
+__global__ void __launch_bounds__(MP_NW * 32) k_les_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
                                                 int PP) {
     extern __shared__ double2 smem[];
     using C = MpCfg<S>;
@@ -375,7 +376,7 @@ __global__ void __launch_bounds__(256) k_les_mp(GroupDev g, const ProbDev *__res
     double *wb = (double *)(smem + C::wb);
     for (int jlo = K1; jlo <= n; jlo += MP_JB) {
         const int jhi = jlo + MP_JB - 1 > n ? n : jlo + MP_JB - 1, nb = jhi - jlo + 1;
-        for (int e = tid; e < C::TRI * s2; e += 256) {
+        for (int e = tid; e < C::TRI * s2; e += MP_NW * 32) {
             const int q = e / s2, ab = e % s2;
             int r, r2;
             pk_inv(q, r, r2);

@@ -381,10 +381,10 @@ template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &
             const unsigned grid = (unsigned)((nact + pp - 1) / pp);
             if (ret) {
                 CK(cudaFuncSetAttribute(k_ret_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                k_ret_mp<S, VIE><<<grid, 256, sm, st>>>(gd, g.d_probs, n, nact, pp);
+                k_ret_mp<S, VIE><<<grid, MP_NW * 32, sm, st>>>(gd, g.d_probs, n, nact, pp);
             } else {
                 CK(cudaFuncSetAttribute(k_les_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                k_les_mp<S, VIE><<<grid, 256, sm, st>>>(gd, g.d_probs, n, nact, pp);
+                k_les_mp<S, VIE><<<grid, MP_NW * 32, sm, st>>>(gd, g.d_probs, n, nact, pp);
             }
             CK(cudaGetLastError());
             return NESSI_OK;
@@ -750,12 +750,7 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
         set_err("stream creation failed");
         return fail(NESSI_ERR_CUDA);
     }
-    // the side stream carries the retarded recursion, the longer of the two concurrent paths of a
-    // step; at the highest priority its CTAs are scheduled ahead of the history stream's, which
-    // keeps HBM busy with whatever SMs remain
-    int prio_lo = 0, prio_hi = 0;
-    if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) prio_hi = 0;
-    if (cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         set_err("stream/event creation failed");
