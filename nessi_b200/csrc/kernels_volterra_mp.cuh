@@ -25,10 +25,11 @@ template <int S> struct MpCfg {
     static constexpr int WSW = 2 * NESSI_K1MAX * NESSI_K1MAX * s2 + 2 * NESSI_K1MAX * s2 + 2;  // start work/warp
     static constexpr int acc = 0;                           // 8 problems x 32 rows x s2: phase-A sums
     static constexpr int red = acc + 8 * MP_JB * s2;        // MP_NW warps x 32 lanes x 2 double2: partial tiles
-    static constexpr int sig = red + MP_NW * 32 * 2;        // TRI x s2
-    static constexpr int wb = sig + TRI * s2;               // TRI doubles
-    static constexpr int total = wb + TRI / 2 + 1;
-    static_assert(sig + TRI * s2 >= 8 * WSW, "start workspaces must fit below the weights");
+    static constexpr int sig = red + MP_NW * 32 * 2;        // 2 x TRI x s2 (block triangle, double-buffered)
+    static constexpr int wb = sig + 2 * TRI * s2;           // 2 x TRI doubles
+    static constexpr int WBN = TRI / 2 + 1;                 // double2 units of one weight buffer
+    static constexpr int total = wb + 2 * WBN;
+    static_assert(sig + 2 * TRI * s2 >= 8 * WSW, "start workspaces must fit below the weights");
 };
 
 // D += A B on the FP64 tensor cores, one 8x8x4 tile: lane holds A[lane/4][lane%4],
@@ -112,13 +113,14 @@ __device__ __forceinline__ double les_cw(int k, int m) { return m <= k ? greg_om
 // Register chain of the retarded rows of one block (lane r = row jlo + r, solved from r = nb-1 down):
 //   Dyson x_r = (h acc_r - bdf_r) Minv_r,   VIE2 x_r = (Q_r - h acc_r) Minv_r   (left solves)
 // Rows above the block (for the backward differences) are read from grow.
+// operands of a lane's row that do not depend on the block's sums: the step inverse and the
+// backward-difference part from rows above the block (VIE2: Q(n, j))
 template <int S, bool VIE>
-__device__ void mp_ret_chain(double2 *a_, const double2 *sig, const double *wb, const ProbDev &p, const double2 *grow,
-                             int n, int jlo, int nb, int K1, const double2 *ibd, double h, int lane) {
+__device__ __forceinline__ void mp_ret_operands(const ProbDev &p, const double2 *grow, int n, int jlo, int nb, int K1,
+                                                const double2 *ibd, int lane, double2 *mi, double2 *bd) {
     constexpr int s2 = S * S;
     const int r = lane;
     const bool own = r < nb;
-    double2 bd[s2], mi[s2];
 #pragma unroll
     for (int e = 0; e < s2; e++) {
         mi[e] = own ? p.minv_ret[(long)(jlo + r) * s2 + e] : cmk(0, 0);
@@ -129,6 +131,26 @@ __device__ void mp_ret_chain(double2 *a_, const double2 *sig, const double *wb, 
             if (r + pp >= nb)
 #pragma unroll
                 for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[pp], grow[(long)(jlo + r + pp) * s2 + e], bd[e]);
+}
+
+template <int S, bool VIE>
+__device__ __forceinline__ void mp_ret_chain_core(double2 *a_, double2 *mi, double2 *bd, const double2 *sig, const double *wb,
+                                  const double2 *grow, int jlo, int nb, int K1, const double2 *ibd, double h, int lane);
+
+template <int S, bool VIE>
+__device__ void mp_ret_chain(double2 *a_, const double2 *sig, const double *wb, const ProbDev &p, const double2 *grow,
+                             int n, int jlo, int nb, int K1, const double2 *ibd, double h, int lane) {
+    constexpr int s2 = S * S;
+    double2 bd[s2], mi[s2];
+    mp_ret_operands<S, VIE>(p, grow, n, jlo, nb, K1, ibd, lane, mi, bd);
+    mp_ret_chain_core<S, VIE>(a_, mi, bd, sig, wb, grow, jlo, nb, K1, ibd, h, lane);
+}
+
+template <int S, bool VIE>
+__device__ __forceinline__ void mp_ret_chain_core(double2 *a_, double2 *mi, double2 *bd, const double2 *sig, const double *wb,
+                                  const double2 *grow, int jlo, int nb, int K1, const double2 *ibd, double h, int lane) {
+    constexpr int s2 = S * S;
+    const int r = lane;
     double2 *gout = (double2 *)grow + (long)jlo * s2;
     for (int rr = nb - 1; rr >= 0; rr--) {
         double2 x[s2];
@@ -173,14 +195,15 @@ __device__ void mp_ret_chain(double2 *a_, const double2 *sig, const double *wb, 
 // Register chain of the lesser rows of one block (lane r = row jlo + r, solved from r = 0 up):
 //   Dyson x_r = Minv_r (gl_r + h acc_r - bdf_r),   VIE2 x_r = Minv_r (gl_r + Q_r - h acc_r)
 // Rows below the block (for the backward differences) are read from xcol.
+// operands of a lane's row that do not depend on the block's sums: the step inverse, the
+// Sigma-shared products (+ Q^<(j, n) for VIE2) and the backward-difference part from rows below
 template <int S, bool VIE>
-__device__ void mp_les_chain(double2 *a_, const double2 *sig, const double *wb, const ProbDev &p, const double2 *gl,
-                             long ldc, double2 *xcol, int n, int jlo, int nb, int K1, const double2 *ibd, double h,
-                             int lane) {
+__device__ __forceinline__ void mp_les_operands(const ProbDev &p, const double2 *gl, long ldc, const double2 *xcol, int n,
+                                                int jlo, int nb, int K1, const double2 *ibd, int lane, double2 *mi,
+                                                double2 *gv, double2 *bd) {
     constexpr int s2 = S * S;
     const int r = lane;
     const bool own = r < nb;
-    double2 bd[s2], mi[s2], gv[s2];
 #pragma unroll
     for (int e = 0; e < s2; e++) {
         const int a = e / S, d = e % S;
@@ -194,6 +217,30 @@ __device__ void mp_les_chain(double2 *a_, const double2 *sig, const double *wb, 
             if (r - pp < 0)
 #pragma unroll
                 for (int e = 0; e < s2; e++) bd[e] = cfma(ibd[pp], xcol[(long)(jlo + r - pp) * s2 + e], bd[e]);
+}
+
+template <int S, bool VIE>
+__device__ __forceinline__ void mp_les_chain_core(double2 *a_, double2 *mi, double2 *gv, double2 *bd, const double2 *sig,
+                                  const double *wb, double2 *xcol, int jlo, int nb, int K1, const double2 *ibd, double h,
+                                  int lane);
+
+template <int S, bool VIE>
+__device__ void mp_les_chain(double2 *a_, const double2 *sig, const double *wb, const ProbDev &p, const double2 *gl,
+                             long ldc, double2 *xcol, int n, int jlo, int nb, int K1, const double2 *ibd, double h,
+                             int lane) {
+    constexpr int s2 = S * S;
+    double2 bd[s2], mi[s2], gv[s2];
+    mp_les_operands<S, VIE>(p, gl, ldc, xcol, n, jlo, nb, K1, ibd, lane, mi, gv, bd);
+    mp_les_chain_core<S, VIE>(a_, mi, gv, bd, sig, wb, xcol, jlo, nb, K1, ibd, h, lane);
+}
+
+template <int S, bool VIE>
+__device__ __forceinline__ void mp_les_chain_core(double2 *a_, double2 *mi, double2 *gv, double2 *bd, const double2 *sig,
+                                  const double *wb, double2 *xcol, int jlo, int nb, int K1, const double2 *ibd, double h,
+                                  int lane) {
+    constexpr int s2 = S * S;
+    const int r = lane;
+    const bool own = r < nb;
     for (int rr = 0; rr < nb; rr++) {
         double2 x[s2];
         if (r == rr) {
@@ -235,9 +282,31 @@ __device__ void mp_les_chain(double2 *a_, const double2 *sig, const double *wb, 
     }
 }
 
+// Block triangle of the recursion's matrix and its exact weights into shared memory, by threads
+// t = 0..nthr-1: ret T(jlo+r, jlo+r2) with w(n - (jlo+r2), n - (jlo+r)); les T(jlo+r, jlo+r2)
+// with w(jlo+r, jlo+r2), r2 < r < nb.
+template <int S, bool RET>
+__device__ __forceinline__ void mp_stage(const double2 *T, int k, int n, int jlo, int nb, double2 *sig, double *wb,
+                                         int t, int nthr) {
+    constexpr int s2 = S * S;
+    for (int e = t; e < MpCfg<S>::TRI * s2; e += nthr) {
+        const int q = e / s2, ab = e % s2;
+        int r, r2;
+        pk_inv(q, r, r2);
+        if (r < nb) {
+            sig[e] = T[(tri(jlo + r) + jlo + r2) * s2 + ab];
+            if (ab == 0) wb[q] = RET ? greg_w(k, n - (jlo + r2), n - (jlo + r)) : greg_w(k, jlo + r, jlo + r2);
+        }
+    }
+}
+
 // ======================================================================================
 // retarded component
 // ======================================================================================
+// Per block: the owner warps first gather the operands of their rows that do not depend on the
+// block's sums (step inverses, backward-difference parts, the exact-weight corrections of the k
+// rows next to the block), so those loads are in flight during phase A; after phase A the owners
+// run their chains while the other warps stage the next block's triangle into the second buffer.
 // Phase A of block [jlo, jhi] for the CTA's problems q as C[(q,a)][(jj,d)] =
 //   sum_{(m,b)} c_m G_q(n,m)[a][b] Sigma^R(m, jlo+jj)[b][d],  m = jhi+1 .. n.
 template <int S, bool VIE>
@@ -272,18 +341,42 @@ __global__ void __launch_bounds__(MP_NW * 32) k_ret_mp(GroupDev g, const ProbDev
         else ret_start_block<S, WarpExec>(g, p, n, ws, WarpExec{lane});
     }
     __syncthreads();
-    double2 *acc_s = smem + C::acc, *red = smem + C::red, *sig = smem + C::sig;
-    double *wb = (double *)(smem + C::wb);
+    double2 *acc_s = smem + C::acc, *red = smem + C::red;
+    auto SIG = [&](int bf) { return smem + C::sig + bf * C::TRI * s2; };
+    auto WB = [&](int bf) { return (double *)(smem + C::wb + bf * C::WBN); };
     const int jtop = n - k - 1;
-    for (int jhi = jtop; jhi >= 0; jhi -= MP_JB) {
+    {
+        const int jlo0 = jtop - MP_JB + 1 < 0 ? 0 : jtop - MP_JB + 1;
+        mp_stage<S, true>(g.rret, k, n, jlo0, jtop - jlo0 + 1, SIG(0), WB(0), tid, MP_NW * 32);
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int jhi = jtop; jhi >= 0; jhi -= MP_JB, cur ^= 1) {
         const int jlo = jhi - MP_JB + 1 < 0 ? 0 : jhi - MP_JB + 1, nb = jhi - jlo + 1;
-        for (int e = tid; e < C::TRI * s2; e += MP_NW * 32) {
-            const int q = e / s2, ab = e % s2;
-            int r, r2;
-            pk_inv(q, r, r2);
-            if (r < nb) {
-                sig[e] = g.rret[(tri(jlo + r) + jlo + r2) * s2 + ab];
-                if (ab == 0) wb[q] = greg_w(k, n - (jlo + r2), n - (jlo + r));
+        // owners: the operands of their rows that do not depend on phase A
+        double2 corr[s2], mi[s2], bd[s2];
+#pragma unroll
+        for (int e = 0; e < s2; e++) corr[e] = cmk(0, 0);
+        if (owner) {
+            const double2 *grow = rows[warp];
+            const int j = jlo + lane;
+            mp_ret_operands<S, VIE>(p, grow, n, jlo, nb, K1, ibd, lane, mi, bd);
+            if (lane < nb) {
+                // exact weights for the rows m - j <= k just above the block
+                for (int m = jhi + 1; m <= min(jhi + k, n); m++) {
+                    if (m - j > k) continue;
+                    const double dw = greg_w(k, n - j, n - m) - ret_cw(k, n, m);
+                    const double2 *gm = grow + (long)m * s2, *sm = g.rret + (tri(m) + j) * s2;
+#pragma unroll
+                    for (int aa = 0; aa < S; aa++)
+#pragma unroll
+                        for (int d = 0; d < S; d++) {
+                            double2 t = cmk(0, 0);
+#pragma unroll
+                            for (int bb = 0; bb < S; bb++) t = cfma(gm[aa * S + bb], sm[bb * S + d], t);
+                            corr[aa * S + d] = cfma(cmk(dw, 0.0), t, corr[aa * S + d]);
+                        }
+                }
             }
         }
         const int mb = jhi + 1;
@@ -303,29 +396,16 @@ __global__ void __launch_bounds__(MP_NW * 32) k_ret_mp(GroupDev g, const ProbDev
         };
         zgemm_cta(fa, fb, put, np * S, MP_JB * S, (n - jhi) * S, red, warp, lane);
         if (owner) {
-            const double2 *grow = rows[warp];
-            const int j = jlo + lane;
             double2 acc[s2];
 #pragma unroll
-            for (int e = 0; e < s2; e++) acc[e] = lane < nb ? acc_s[(warp * MP_JB + lane) * s2 + e] : cmk(0, 0);
-            if (lane < nb) {
-                // exact weights for the rows m - j <= k just above the block
-                for (int m = jhi + 1; m <= min(jhi + k, n); m++) {
-                    if (m - j > k) continue;
-                    const double dw = greg_w(k, n - j, n - m) - ret_cw(k, n, m);
-                    const double2 *gm = grow + (long)m * s2, *sm = g.rret + (tri(m) + j) * s2;
-#pragma unroll
-                    for (int aa = 0; aa < S; aa++)
-#pragma unroll
-                        for (int d = 0; d < S; d++) {
-                            double2 t = cmk(0, 0);
-#pragma unroll
-                            for (int bb = 0; bb < S; bb++) t = cfma(gm[aa * S + bb], sm[bb * S + d], t);
-                            acc[aa * S + d] = cfma(cmk(dw, 0.0), t, acc[aa * S + d]);
-                        }
-                }
-            }
-            mp_ret_chain<S, VIE>(acc, sig, wb, p, grow, n, jlo, nb, K1, ibd, h, lane);
+            for (int e = 0; e < s2; e++)
+                acc[e] = lane < nb ? cadd(acc_s[(warp * MP_JB + lane) * s2 + e], corr[e]) : cmk(0, 0);
+            mp_ret_chain_core<S, VIE>(acc, mi, bd, SIG(cur), WB(cur), rows[warp], jlo, nb, K1, ibd, h, lane);
+        } else if (warp >= 8 && jlo > 0) {
+            // the next block's triangle, while the owners solve this one
+            const int jhi2 = jlo - 1, jlo2 = jhi2 - MP_JB + 1 < 0 ? 0 : jhi2 - MP_JB + 1;
+            mp_stage<S, true>(g.rret, k, n, jlo2, jhi2 - jlo2 + 1, SIG(cur ^ 1), WB(cur ^ 1), tid - 256,
+                              MP_NW * 32 - 256);
         }
         __syncthreads();
     }
@@ -372,17 +452,38 @@ __global__ void __launch_bounds__(MP_NW * 32) k_les_mp(GroupDev g, const ProbDev
     }
     __syncthreads();
     if (n <= k) return;
-    double2 *acc_s = smem + C::acc, *red = smem + C::red, *sig = smem + C::sig;
-    double *wb = (double *)(smem + C::wb);
-    for (int jlo = K1; jlo <= n; jlo += MP_JB) {
+    double2 *acc_s = smem + C::acc, *red = smem + C::red;
+    auto SIG = [&](int bf) { return smem + C::sig + bf * C::TRI * s2; };
+    auto WB = [&](int bf) { return (double *)(smem + C::wb + bf * C::WBN); };
+    mp_stage<S, false>(g.sret, k, n, K1, min(n, K1 + MP_JB - 1) - K1 + 1, SIG(0), WB(0), tid, MP_NW * 32);
+    __syncthreads();
+    int cur = 0;
+    for (int jlo = K1; jlo <= n; jlo += MP_JB, cur ^= 1) {
         const int jhi = jlo + MP_JB - 1 > n ? n : jlo + MP_JB - 1, nb = jhi - jlo + 1;
-        for (int e = tid; e < C::TRI * s2; e += MP_NW * 32) {
-            const int q = e / s2, ab = e % s2;
-            int r, r2;
-            pk_inv(q, r, r2);
-            if (r < nb) {
-                sig[e] = g.sret[(tri(jlo + r) + jlo + r2) * s2 + ab];
-                if (ab == 0) wb[q] = greg_w(k, jlo + r, jlo + r2);
+        // owners: the operands of their rows that do not depend on phase A
+        double2 corr[s2], mi[s2], gv[s2], bd[s2];
+#pragma unroll
+        for (int e = 0; e < s2; e++) corr[e] = cmk(0, 0);
+        if (owner) {
+            const double2 *xcol = cols[warp];
+            const int j = jlo + lane;
+            mp_les_operands<S, VIE>(p, gl, ldc, xcol, n, jlo, nb, K1, ibd, lane, mi, gv, bd);
+            if (lane < nb) {
+                // exact weights for the columns j - m <= k just below the block
+                for (int m = max(0, jlo - k); m < jlo; m++) {
+                    if (j - m > k) continue;
+                    const double dw = greg_w(k, j, m) - les_cw(k, m);
+                    const double2 *sm = g.sret + (tri(j) + m) * s2, *xm = xcol + (long)m * s2;
+#pragma unroll
+                    for (int aa = 0; aa < S; aa++)
+#pragma unroll
+                        for (int d = 0; d < S; d++) {
+                            double2 t = cmk(0, 0);
+#pragma unroll
+                            for (int bb = 0; bb < S; bb++) t = cfma(sm[aa * S + bb], xm[bb * S + d], t);
+                            corr[aa * S + d] = cfma(cmk(dw, 0.0), t, corr[aa * S + d]);
+                        }
+                }
             }
         }
         auto fa = [&](int r, int kk) -> double2 {
@@ -401,29 +502,16 @@ __global__ void __launch_bounds__(MP_NW * 32) k_les_mp(GroupDev g, const ProbDev
         };
         zgemm_cta(fa, fb, put, MP_JB * S, np * S, jlo * S, red, warp, lane);
         if (owner) {
-            double2 *xcol = cols[warp];
-            const int j = jlo + lane;
             double2 acc[s2];
 #pragma unroll
-            for (int e = 0; e < s2; e++) acc[e] = lane < nb ? acc_s[(warp * MP_JB + lane) * s2 + e] : cmk(0, 0);
-            if (lane < nb) {
-                // exact weights for the columns j - m <= k just below the block
-                for (int m = max(0, jlo - k); m < jlo; m++) {
-                    if (j - m > k) continue;
-                    const double dw = greg_w(k, j, m) - les_cw(k, m);
-                    const double2 *sm = g.sret + (tri(j) + m) * s2, *xm = xcol + (long)m * s2;
-#pragma unroll
-                    for (int aa = 0; aa < S; aa++)
-#pragma unroll
-                        for (int d = 0; d < S; d++) {
-                            double2 t = cmk(0, 0);
-#pragma unroll
-                            for (int bb = 0; bb < S; bb++) t = cfma(sm[aa * S + bb], xm[bb * S + d], t);
-                            acc[aa * S + d] = cfma(cmk(dw, 0.0), t, acc[aa * S + d]);
-                        }
-                }
-            }
-            mp_les_chain<S, VIE>(acc, sig, wb, p, gl, ldc, xcol, n, jlo, nb, K1, ibd, h, lane);
+            for (int e = 0; e < s2; e++)
+                acc[e] = lane < nb ? cadd(acc_s[(warp * MP_JB + lane) * s2 + e], corr[e]) : cmk(0, 0);
+            mp_les_chain_core<S, VIE>(acc, mi, gv, bd, SIG(cur), WB(cur), cols[warp], jlo, nb, K1, ibd, h, lane);
+        } else if (warp >= 8 && jhi < n) {
+            // the next block's triangle, while the owners solve this one
+            const int jlo2 = jhi + 1, jhi2 = jlo2 + MP_JB - 1 > n ? n : jlo2 + MP_JB - 1;
+            mp_stage<S, false>(g.sret, k, n, jlo2, jhi2 - jlo2 + 1, SIG(cur ^ 1), WB(cur ^ 1), tid - 256,
+                               MP_NW * 32 - 256);
         }
         __syncthreads();
     }
