@@ -247,6 +247,20 @@ int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, c
 int nessi_gpu_distance_norm2(int tstp, const nessi_hm_ptrs *g1, const nessi_hm_ptrs *g2, int nt, int ntau, int size1,
                              double *out, void *stream);
 
+/* The GW self-energy diagrams of the momentum-resolved example
+ * (examples/programs/gw_selfene_impl.cpp:114-153) at time step tstp, for all nk momenta of a 1-d
+ * grid k_i = (i - nk/2) 2 pi / nk (gw_latt_impl.cpp:46-51) in one launch, element by element:
+ *   polarisation  P_q = -sum_k w_k Bubble1(G_{k-q}, G_k)   (get_Polarization_Bubble)
+ *   self-energy   Sigma_k = sum_q w_q Bubble2(G_{k-q}, W_q)  (sigma_GW)
+ * with libcntr's bubbles (cntr_bubble_impl.hpp:17-330).  G, W, P, S and w are DEVICE arrays of nk
+ * entries (herm_matrix pointers in libcntr's layout, tv as (t(ntau+1)+tau) s^2; weights); sig_g
+ * is G's statistics.  tstp = -1 gives the Matsubara branch.  Queued on `stream`, allocates
+ * nothing. */
+int nessi_gpu_gw_polarization_timestep(int tstp, int nk, const nessi_hm_ptrs *G, const nessi_hm_ptrs *P, const double *w,
+                                       int nt, int ntau, int size1, int sig_g, void *stream);
+int nessi_gpu_gw_sigma_timestep(int tstp, int nk, const nessi_hm_ptrs *G, const nessi_hm_ptrs *W, const nessi_hm_ptrs *S,
+                                const double *w, int nt, int ntau, int size1, void *stream);
+
 /* Volterra kernels in use for a group: -1 = one problem per CTA, 2/4/8 = problems per CTA of the
  * tensor-core kernels, 100 = the group-wide blocked recursion by thread-block clusters (trailing
  * updates on the FP64 tensor cores), 0 = not chosen yet (the autotuner decides at the first eager

@@ -265,3 +265,103 @@ __global__ void __launch_bounds__(256) k_distance_norm2(int tstp, ConvHM g1, Con
     }
     if (threadIdx.x == 0) *out = part[0];
 }
+
+// ---------------------------------------------------------------------------------------
+// GW self-energy diagrams of the momentum-resolved example (examples/programs/gw_selfene_impl.cpp:
+// 114-153) on device herm_matrix data in libcntr's layout, for all momenta in one launch:
+//   polarisation  P_q(tstp) = -sum_k w_k Bubble1(G_{k-q}, G_k)          (get_Polarization_Bubble)
+//   self-energy   Sigma_k(tstp) = sum_q w_q Bubble2(G_{k-q}, W_q)        (sigma_GW)
+// element by element (C_{i1 i2} from A_{i1 i2}, B_{i1 i2}), with the bubbles of
+// cntr_bubble_impl.hpp:17-130 (Bubble1: i A(t,t') B(t',t); Bubble2: i A(t,t') B(t,t'); the
+// continuations to t' > t from the hermitian partners, here the functions themselves) and the
+// momentum index of k - q on the grid k_i = (i - nk/2) 2 pi / nk (gw_latt_impl.cpp:46-51).
+// Thread per (time index m of the slice, element); grid.y = the output momentum.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ int gw_k_minus_q(int nk, int k, int q) {
+    const int g = nk / 2;
+    int i = (k - g) - (q - g) + g;
+    i %= nk;
+    return i < 0 ? i + nk : i;
+}
+
+// C_{c}(t, m), C_{c}(m, t) [ret / les] or C_{c}(t, tau) [tv] or C_{c}(tau) [mat] of Bubble1 with
+// A = Acc = a, B = Bcc = b, at element c = (i1, i2) (e12) and its transpose e21
+__device__ __forceinline__ void gw_bubble1(int tstp, int m, int part, const ConvHM &A, const ConvHM &B, int ntau, int s2,
+                                           int e12, int e21, double sigb, double2 *c_ret, double2 *c_les) {
+    const double2 I = cmk(0.0, 1.0);
+    const int M = ntau + 1;
+    if (tstp < 0) {
+        *c_ret = cscale(cmul(A.mat[(long)m * s2 + e12], B.mat[(long)(ntau - m) * s2 + e21]), -sigb);
+        return;
+    }
+    if (part == 0) {
+        const long rt = (tri(tstp) + m) * s2, lm = (tri(tstp) + m) * s2;  // ret(t, m) and les(m, t)
+        const double2 bles21_tt1 = cneg(cconj(B.les[lm + e12]));
+        const double2 bgtr21_tt1 = cadd(B.ret[rt + e21], bles21_tt1);
+        const double2 bles21_t1t = B.les[lm + e21];
+        const double2 bgtr21_t1t = cadd(cneg(cconj(B.ret[rt + e12])), bles21_t1t);
+        const double2 ales12_tt1 = cneg(cconj(A.les[lm + e21]));
+        const double2 agtr12_tt1 = cadd(A.ret[rt + e12], ales12_tt1);
+        *c_ret = csub(cmul(I, cmul(agtr12_tt1, bles21_t1t)), cmul(I, cmul(ales12_tt1, bgtr21_t1t)));
+        *c_les = cmul(I, cmul(A.les[lm + e12], bgtr21_tt1));
+    } else {
+        const double2 bvt21 = cscale(cconj(B.tv[((long)tstp * M + ntau - m) * s2 + e12]), -sigb);
+        *c_ret = cmul(I, cmul(A.tv[((long)tstp * M + m) * s2 + e12], bvt21));
+    }
+}
+
+__device__ __forceinline__ void gw_bubble2(int tstp, int m, int part, const ConvHM &A, const ConvHM &B, int ntau, int s2,
+                                           int e12, int e21, double2 *c_ret, double2 *c_les) {
+    const double2 I = cmk(0.0, 1.0);
+    const int M = ntau + 1;
+    if (tstp < 0) {
+        *c_ret = cneg(cmul(A.mat[(long)m * s2 + e12], B.mat[(long)m * s2 + e12]));
+        return;
+    }
+    if (part == 0) {
+        const long rt = (tri(tstp) + m) * s2, lm = (tri(tstp) + m) * s2;
+        const double2 bgtr12 = csub(B.ret[rt + e12], cconj(B.les[lm + e21]));
+        const double2 agtr12 = csub(A.ret[rt + e12], cconj(A.les[lm + e21]));
+        const double2 cles = cmul(I, cmul(cconj(A.les[lm + e21]), cconj(B.les[lm + e21])));
+        *c_ret = csub(cmul(I, cmul(agtr12, bgtr12)), cles);
+        *c_les = cmul(I, cmul(A.les[lm + e12], B.les[lm + e12]));
+    } else {
+        *c_ret = cmul(I, cmul(A.tv[((long)tstp * M + m) * s2 + e12], B.tv[((long)tstp * M + m) * s2 + e12]));
+    }
+}
+
+// which = 1: out[q] = P_q from G (B = G_k, A = G_{k-q}), sign -w_k;  which = 2: out[k] = Sigma_k
+// from G and W (A = G_{k-q}, B = W_q), sign +w_q.  Items: m = 0..tstp for ret/les (part 0) then
+// m = 0..ntau for tv (part 1); tstp = -1: m = 0..ntau of mat.
+__global__ void __launch_bounds__(128) k_gw_bubbles(int which, int tstp, int nk, const ConvHM *__restrict__ G,
+                                                    const ConvHM *__restrict__ W, const ConvHM *__restrict__ out,
+                                                    const double *__restrict__ w, int ntau, int s, double sigb) {
+    const int s2 = s * s, M = ntau + 1;
+    const int o = blockIdx.y;  // output momentum
+    const long nitem = tstp < 0 ? (long)M * s2 : (long)(tstp + 1 + M) * s2;
+    const ConvHM C = out[o];
+    for (long it = blockIdx.x * (long)blockDim.x + threadIdx.x; it < nitem; it += (long)gridDim.x * blockDim.x) {
+        const int e = (int)(it % s2);
+        const long mi = it / s2;
+        const int part = tstp < 0 ? 0 : (mi <= tstp ? 0 : 1);
+        const int m = tstp < 0 ? (int)mi : (part == 0 ? (int)mi : (int)(mi - tstp - 1));
+        const int i1 = e / s, i2 = e % s, e12 = e, e21 = i2 * s + i1;
+        double2 r = cmk(0, 0), l = cmk(0, 0);
+        for (int x = 0; x < nk; x++) {  // x = k (polarisation) or q (self-energy)
+            double2 cr = cmk(0, 0), cl = cmk(0, 0);
+            if (which == 1) gw_bubble1(tstp, m, part, G[gw_k_minus_q(nk, x, o)], G[x], ntau, s2, e12, e21, sigb, &cr, &cl);
+            else gw_bubble2(tstp, m, part, G[gw_k_minus_q(nk, o, x)], W[x], ntau, s2, e12, e21, &cr, &cl);
+            const double f = which == 1 ? -w[x] : w[x];
+            r = cfma(cmk(f, 0.0), cr, r);
+            l = cfma(cmk(f, 0.0), cl, l);
+        }
+        if (tstp < 0) {
+            C.mat[(long)m * s2 + e] = r;
+        } else if (part == 0) {
+            C.ret[(tri(tstp) + m) * s2 + e] = r;
+            C.les[(tri(tstp) + m) * s2 + e] = l;
+        } else {
+            C.tv[((long)tstp * M + m) * s2 + e] = r;
+        }
+    }
+}

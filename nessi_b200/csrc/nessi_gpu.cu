@@ -1768,3 +1768,37 @@ extern "C" int nessi_gpu_distance_norm2(int tstp, const nessi_hm_ptrs *g1, const
     CK(cudaGetLastError());
     return NESSI_OK;
 }
+
+// =====================================================================================
+// GW diagrams on device herm_matrix data
+// =====================================================================================
+static int gw_launch(int which, int tstp, int nk, const nessi_hm_ptrs *G, const nessi_hm_ptrs *W,
+                     const nessi_hm_ptrs *out, const double *w, int nt, int ntau, int size1, int sig_b, void *stream,
+                     const char *name) {
+    if (!G || !out || !w || (which == 2 && !W) || nk < 1 || nt < -1 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS ||
+        tstp < -1 || tstp > nt || (sig_b != 1 && sig_b != -1)) {
+        set_err("%s: bad arguments (tstp=%d nk=%d nt=%d ntau=%d size1=%d)", name, tstp, nk, nt, ntau, size1);
+        return NESSI_ERR_ARG;
+    }
+    const long items = tstp < 0 ? (long)(ntau + 1) * size1 * size1 : (long)(tstp + 1 + ntau + 1) * size1 * size1;
+    const dim3 grid((unsigned)std::min<long>((items + 127) / 128, 1024), (unsigned)nk);
+    static_assert(sizeof(nessi_hm_ptrs) == sizeof(ConvHM), "pointer tables share one layout");
+    k_gw_bubbles<<<grid, 128, 0, (cudaStream_t)stream>>>(which, tstp, nk, (const ConvHM *)G, (const ConvHM *)W,
+                                                         (const ConvHM *)out, w, ntau, size1, (double)sig_b);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+extern "C" int nessi_gpu_gw_polarization_timestep(int tstp, int nk, const nessi_hm_ptrs *G, const nessi_hm_ptrs *P,
+                                                  const double *w, int nt, int ntau, int size1, int sig_g,
+                                                  void *stream) {
+    NvtxRange nvtx_("nessi::gw_polarization_timestep");
+    return gw_launch(1, tstp, nk, G, nullptr, P, w, nt, ntau, size1, sig_g, stream, "gw_polarization_timestep");
+}
+
+extern "C" int nessi_gpu_gw_sigma_timestep(int tstp, int nk, const nessi_hm_ptrs *G, const nessi_hm_ptrs *W,
+                                           const nessi_hm_ptrs *S, const double *w, int nt, int ntau, int size1,
+                                           void *stream) {
+    NvtxRange nvtx_("nessi::gw_sigma_timestep");
+    return gw_launch(2, tstp, nk, G, W, S, w, nt, ntau, size1, 1, stream, "gw_sigma_timestep");
+}

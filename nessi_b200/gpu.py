@@ -92,6 +92,10 @@ EXPORTS = {
                                    [ctypes.c_double, ctypes.c_double]),
     "nessi_gpu_distance_norm2": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(HmPtrs), ctypes.POINTER(HmPtrs)] +
                                  [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_void_p]),
+    "nessi_gpu_gw_polarization_timestep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p] + [ctypes.c_int] * 4 + [ctypes.c_void_p]),
+    "nessi_gpu_gw_sigma_timestep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 4 +
+                                    [ctypes.c_int] * 3 + [ctypes.c_void_p]),
     "nessi_gpu_get_volterra_choice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                      ctypes.POINTER(ctypes.c_int)]),
     "nessi_gpu_graph_record": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 4),
@@ -354,6 +358,21 @@ def distance_norm2_dev(tstp, g1, g2, nt, ntau, size1, out_ptr, stream=0):
     libcntr layout); the result is written to the device double at out_ptr."""
     _check(load_library().nessi_gpu_distance_norm2(tstp, ctypes.byref(g1), ctypes.byref(g2), nt, ntau, size1,
                                                     ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream) if stream else None))
+
+
+def gw_polarization_timestep_dev(tstp, nk, G_table, P_table, w_ptr, nt, ntau, size1, sig_g=-1, stream=0):
+    """nessi_gpu_gw_polarization_timestep: the tables are device addresses of nk HmPtrs (and of nk
+    float64 weights)."""
+    _check(load_library().nessi_gpu_gw_polarization_timestep(tstp, nk, ctypes.c_void_p(G_table), ctypes.c_void_p(P_table),
+                                                              ctypes.c_void_p(w_ptr), nt, ntau, size1, sig_g,
+                                                              ctypes.c_void_p(stream) if stream else None))
+
+
+def gw_sigma_timestep_dev(tstp, nk, G_table, W_table, S_table, w_ptr, nt, ntau, size1, stream=0):
+    """nessi_gpu_gw_sigma_timestep on device tables (see gw_polarization_timestep_dev)."""
+    _check(load_library().nessi_gpu_gw_sigma_timestep(tstp, nk, ctypes.c_void_p(G_table), ctypes.c_void_p(W_table),
+                                                       ctypes.c_void_p(S_table), ctypes.c_void_p(w_ptr), nt, ntau,
+                                                       size1, ctypes.c_void_p(stream) if stream else None))
 
 
 def convolution_timestep_dev(n, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, stream=0):
