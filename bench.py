@@ -217,6 +217,8 @@ def step_bytes(W, mixed):
 def build_workload(name, rank, world):
     from nessi_b200 import workloads
     shift = 0.0 if world == 1 else (2 * math.pi / 256) * rank / world
+    if name == "config0":  # one impurity problem (the CPU-sized case)
+        return workloads.config0()
     if name == "config1":
         return workloads.config1(kshift=shift)
     if name == "config1-small":

@@ -279,8 +279,18 @@ int nessi_gpu_get_volterra_choice(nessi_batch *b, int group, int *pp_ret, int *p
 int nessi_gpu_graph_record(nessi_batch *b, int kind, int n0, int n1, int corrector_steps);
 int nessi_gpu_graph_launch(nessi_batch *b);
 
-/* Wait for all work queued on the batch. */
+/* Wait for all work queued on the batch.  Returns NESSI_ERR_TIMEOUT (and clears the condition)
+ * when a bounded wait inside one of the batch's kernels gave up since the last call: the kernel
+ * then returned without writing its results, so the time steps queued since the last check are
+ * invalid.  No reference counterpart (libcntr's host loops have no device waits). */
 int nessi_gpu_synchronize(nessi_batch *b);
+
+/* Bound, in nanoseconds of the device clock, of every wait of the batch's kernels on an mbarrier
+ * (the tv history stream waits for its bulk copies and for its consumers).  Default 2e9; a launch
+ * reads the value when it is queued (a recorded graph keeps the value of its recording).  A
+ * bound of 0 makes every wait give up at once, so that the next synchronize reports
+ * NESSI_ERR_TIMEOUT: a way to exercise the timeout path.  No reference counterpart. */
+int nessi_gpu_set_wait_limit(nessi_batch *b, long long ns);
 
 #ifdef __cplusplus
 }

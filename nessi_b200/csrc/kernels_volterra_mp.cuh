@@ -18,6 +18,11 @@
 
 #define MP_JB 32  // rows per block (lane = row)
 #define MP_NW 16  // warps per CTA: warps 0..PP-1 own a problem's chain, all of them share phase A
+// Registers per thread of the multi-problem kernels.  For size1 = 1, 512 threads x 96 leave 16384
+// of an SM's 65536 registers to a CTA of the tv history stream (k_tv_stream), which runs beside
+// them on the main stream while they run on the side stream (at the cost of ~100-250 bytes of
+// spills per thread); size1 = 2 would spill over 1 KB at 96 and keeps the 128 of 512 threads.
+#define MP_MAXREG(S) ((S) == 1 ? 96 : 128)
 
 template <int S> struct MpCfg {
     static constexpr int s2 = S * S;
@@ -310,7 +315,7 @@ __device__ __forceinline__ void mp_stage(const double2 *T, int k, int n, int jlo
 // Phase A of block [jlo, jhi] for the CTA's problems q as C[(q,a)][(jj,d)] =
 //   sum_{(m,b)} c_m G_q(n,m)[a][b] Sigma^R(m, jlo+jj)[b][d],  m = jhi+1 .. n.
 template <int S, bool VIE>
-__global__ void __launch_bounds__(MP_NW * 32) k_ret_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
+__global__ void __maxnreg__(MP_MAXREG(S)) k_ret_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
                                                 int PP) {
     extern __shared__ double2 smem[];
     using C = MpCfg<S>;
@@ -417,7 +422,7 @@ __global__ void __launch_bounds__(MP_NW * 32) k_ret_mp(GroupDev g, const ProbDev
 // Phase A of block [jlo, jhi] as C[(jj,a)][(q,d)] =
 //   sum_{(m,b)} Sigma^R(jlo+jj, m)[a][b] c'_m G^<_q(m,n)[b][d],  m = 0 .. jlo-1.
 template <int S, bool VIE>
-__global__ void __launch_bounds__(MP_NW * 32) k_les_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
+__global__ void __maxnreg__(MP_MAXREG(S)) k_les_mp(GroupDev g, const ProbDev *__restrict__ probs, int n, int nact,
                                                 int PP) {
     extern __shared__ double2 smem[];
     using C = MpCfg<S>;

@@ -15,6 +15,7 @@
 
 #include "../../include/nessi_gpu.h"
 #include "kernels_dyson.cuh"
+#include "kernels_tv_stream.cuh"
 #include "kernels_start.cuh"
 #include "kernels_mat.cuh"
 #include "kernels_conv.cuh"
@@ -168,6 +169,12 @@ struct nessi_batch {
     int volterra_pp = 0;
     double2 *scratch = nullptr;  // G^tv in libcntr layout during layout conversion (size1 > 1)
     long scratch_n = 0;
+    // kernel of the tv row for size1 <= 4: 0 (default) = k_tv_stream (history through shared
+    // memory by bulk copies), 1 = k_tv (register loads); size1 > 4 always uses k_tv
+    int tv_kernel = 0;
+    int nsm = 0;                        // SMs of the device
+    int *d_err = nullptr;               // set by a device wait that gave up (NESSI_ERR_TIMEOUT)
+    long long wait_ns = 2000000000LL;   // bound of every mbarrier wait in the batch's kernels
 
     void prof_mark(int id, cudaStream_t st = nullptr) {
         if (!prof) return;
@@ -379,11 +386,17 @@ template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &
         if (pp > 0) {
             const size_t sm = (size_t)MpCfg<S>::total * sizeof(double2);
             const unsigned grid = (unsigned)((nact + pp - 1) / pp);
+            // the largest shared-memory carveout, so that an SM holding one of these CTAs can also
+            // take a k_tv_stream CTA without reconfiguring
             if (ret) {
                 CK(cudaFuncSetAttribute(k_ret_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                CK(cudaFuncSetAttribute(k_ret_mp<S, VIE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared));
                 k_ret_mp<S, VIE><<<grid, MP_NW * 32, sm, st>>>(gd, g.d_probs, n, nact, pp);
             } else {
                 CK(cudaFuncSetAttribute(k_les_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                CK(cudaFuncSetAttribute(k_les_mp<S, VIE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared));
                 k_les_mp<S, VIE><<<grid, MP_NW * 32, sm, st>>>(gd, g.d_probs, n, nact, pp);
             }
             CK(cudaGetLastError());
@@ -446,6 +459,53 @@ template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const Gro
     return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);  // the kept variant writes last
 }
 
+// Decomposition of k_tv_stream: tau chunk width tw <= TWMAX chosen to balance the items
+// (problem, chunk) over the CTAs (one per SM): the makespan in rounds of items times the chunk's
+// cost (tw plus a fixed cost per segment) is minimised.  Stages hold whole history rows.
+TvsPlan tv_stream_plan(int S, int M, int nact, int nsm, int twmax) {
+    TvsPlan pl{};
+    double best = 1e300;
+    const int nch0 = (M + twmax - 1) / twmax;
+    for (int nch = nch0; nch < nch0 + 16; nch++) {
+        const int tw = (M + nch - 1) / nch, nchr = (M + tw - 1) / tw;
+        const long items = (long)nact * nchr, grid = std::min<long>(items, nsm);
+        const double cost = (double)((items + grid - 1) / grid) * (tw + 16);
+        if (cost < best - 1e-9) {
+            best = cost;
+            pl.tw = tw;
+            pl.nch = nchr;
+            pl.items = (int)items;
+        }
+    }
+    const int s2 = S * S;
+    pl.slot64 = pl.tw * 16;
+    pl.slot32 = ((pl.tw + 2) * 8 + 15) & ~15;
+    pl.r64 = std::max(1, tvs::STAGE_TARGET / (s2 * pl.slot64));
+    pl.stb = std::max(pl.r64 * s2 * pl.slot64, s2 * pl.slot32);
+    pl.r32 = pl.stb / (s2 * pl.slot32);
+    return pl;
+}
+
+template <int S, bool MIXED, bool VIE>
+int tv_stream_launch(nessi_batch *b, const GroupDev &gd, const Group &g, int n, int nact, cudaStream_t st) {
+    TvsPlan pl = tv_stream_plan(S, g.ntau + 1, nact, b->nsm, TvsCfg<S>::TWMAX);
+    pl.wait_ns = b->wait_ns;
+    pl.err = b->d_err;
+    const size_t sm = (size_t)tvs::STAGES * pl.stb;
+    static bool attr_set[64] = {false};  // per device
+    if (!attr_set[b->device & 63]) {
+        CK(cudaFuncSetAttribute(k_tv_stream<S, MIXED, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tvs::STAGES * tvs::STAGE_TARGET));
+        CK(cudaFuncSetAttribute(k_tv_stream<S, MIXED, VIE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared));
+        attr_set[b->device & 63] = true;
+    }
+    const int grid = std::min(pl.items, b->nsm);
+    k_tv_stream<S, MIXED, VIE><<<grid, tvs::NTH, sm, st>>>(gd, g.d_probs, n, pl);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
 template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int nact) {
     const GroupDev gd = group_dev(g);
     cudaStream_t st = b->stream;
@@ -467,6 +527,8 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
         b->prof_end(NESSI_KERNEL_PREP, 0.0);
         g.dense_valid = n - 1;
     }
+    CK(cudaEventRecord(b->ev_fork, st));
+    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     // VIE2 moves the convolution to the right-hand side: gles = -(tv*vt + les*adv)
     const double alpha = VIE ? -1.0 : 1.0;
     // Matsubara part of the tv row: Cmat = K_n Gmat_all (one GEMM for the group)
@@ -491,9 +553,8 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
     }
     const int m = nact * S, nn = (n + 1) * S;
     const long ldL = (long)(g.ntmax + 1) * S, ldT = (long)(g.ntau + 1) * S;
-    // side stream: retarded row, then les*adv = Ldense * badv (needs only G^R(n, .))
-    CK(cudaEventRecord(b->ev_fork, st));
-    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+    // side stream: retarded row, then les*adv = Ldense * badv (needs only G^R(n, .)); forked
+    // before the Matsubara operator and its GEMM, which only the tv row reads
     {
         b->prof_mark(NESSI_KERNEL_RET, b->side);
         CKR((volterra_step<S, VIE>(b, g, gd, n, nact, true, b->side)));
@@ -515,9 +576,19 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
         dim3 grid((g.ntau + 1 + 31) / 32, nact);
         b->prof_mark(NESSI_KERNEL_TV);
         const bool mixed = b->precision == NESSI_PREC_MIXED;
-        if (mixed) k_tv<S, true, VIE><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
-        else k_tv<S, false, VIE><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
-        CK(cudaGetLastError());
+        bool streamed = false;
+        if constexpr (S <= 4) {
+            if (b->tv_kernel == 0) {
+                if (mixed) CKR((tv_stream_launch<S, true, VIE>(b, gd, g, n, nact, st)));
+                else CKR((tv_stream_launch<S, false, VIE>(b, gd, g, n, nact, st)));
+                streamed = true;
+            }
+        }
+        if (!streamed) {
+            if (mixed) k_tv<S, true, VIE><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+            else k_tv<S, false, VIE><<<grid, 256, 0, st>>>(gd, g.d_probs, n);
+            CK(cudaGetLastError());
+        }
         // per problem: G^tv history rows 0..n-1 read (FP32 below the k+1 BDF rows when mixed),
         // row n written, Cmat column read; shared: the n coefficient blocks
         const double M = g.ntau + 1;
@@ -745,7 +816,21 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
         if (pp == -1 || pp == 0 || pp == 1 || pp == 2 || pp == 4 || pp == 8 || pp == NESSI_VOLTERRA_CLUSTER)
             b->volterra_pp = pp;
     }
+    if (const char *v = getenv("NESSI_TV_KERNEL")) b->tv_kernel = strcmp(v, "regs") == 0 ? 1 : 0;
     auto fail = [&](int r) { nessi_gpu_batch_destroy(b); return r; };
+    if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess || b->nsm <= 0) {
+        set_err("SM count query failed");
+        return fail(NESSI_ERR_CUDA);
+    }
+    {
+        void *q = nullptr;
+        if (cudaMalloc(&q, sizeof(int)) != cudaSuccess || cudaMemset(q, 0, sizeof(int)) != cudaSuccess) {
+            set_err("cudaMalloc of the error word failed");
+            return fail(NESSI_ERR_OOM);
+        }
+        b->allocs.push_back(q);
+        b->d_err = (int *)q;
+    }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
         set_err("stream creation failed");
         return fail(NESSI_ERR_CUDA);
@@ -1497,6 +1582,20 @@ int nessi_gpu_graph_launch(nessi_batch *b) {
 int nessi_gpu_synchronize(nessi_batch *b) {
     CKR(check_batch(b));
     CK(cudaStreamSynchronize(b->stream));
+    int err = 0;
+    CK(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        CK(cudaMemset(b->d_err, 0, sizeof(int)));
+        set_err("a bounded device wait gave up; the time steps since the last check are invalid");
+        return NESSI_ERR_TIMEOUT;
+    }
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_wait_limit(nessi_batch *b, long long ns) {
+    CKR(check_batch(b));
+    if (ns < 0) { set_err("wait limit %lld < 0", ns); return NESSI_ERR_ARG; }
+    b->wait_ns = ns;
     return NESSI_OK;
 }
 

@@ -62,6 +62,7 @@ EXPORTS = {
     "nessi_gpu_dyson_mat": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_dyson_start": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "nessi_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "nessi_gpu_dyson_mat_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
@@ -219,6 +220,10 @@ class Batch:
 
     def synchronize(self):
         _check(load_library().nessi_gpu_synchronize(self._h))
+
+    def set_wait_limit(self, ns):
+        """Bound (device nanoseconds) of every mbarrier wait in this batch's kernels."""
+        _check(load_library().nessi_gpu_set_wait_limit(self._h, int(ns)))
 
     # ---- VIE2: [1 + F] G = Q ---------------------------------------------------------
     def set_F(self, group, F, Fcc):

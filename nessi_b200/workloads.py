@@ -17,6 +17,8 @@ uneven (independent problems of mixed orbital size and length): size1 drawn from
     u u^H (u complex N(0, 0.3^2)) switched on at t = 0; Sigma = 0.49 G_bath (x) 1_s shared by the
     problems of one size (sigma_group = size1).  Every problem is a Dyson problem: VIE2 problems
     would each carry a source term Q as large as G, which does not fit next to ~150 GB of G.
+impurity (config 0): one size1 = 1 level quenched from 0 to 1 at t = 0 in the semicircular bath
+    with V = 1, beta = 10, nt = 200, ntau = 400, h = 0.02.
 lattice2b (square lattice, size1 = 1, nkx x nky k-points in [-pi, pi)^2):
     eps_k = -2(cos kx + cos ky), mu = 0 (half filling), free equilibrium (U = 0 on the Matsubara
     branch), U(t) = min(t, 2) switched on at t = 0; Sigma = Sigma_2B[G_loc, U] recomputed from the
@@ -108,6 +110,22 @@ def chain(nk, nt, ntau, beta, h, size1, k=5, V=0.5, mu=0.0, kshift=0.0, kslice=N
         info["k_chunk"] = "k-points %d..%d of %d (one chunk; G of the whole grid is 2.5 TB)" % (
             kslice.start, kslice.stop - 1, nk)
     return Workload("chain%d" % size1, descs, sigma, H, boot, k, info)
+
+
+def config0(nt=200, ntau=400, beta=10.0, h=0.02, k=5, V=1.0, eps0=1.0):
+    """Impurity quench, the CPU-sized case: one size1 = 1 level quenched from 0 to eps0 at t = 0
+    (H(-1) = 0, H(t >= 0) = eps0), coupled with V = 1 to the semicircular bath (half-bandwidth 2,
+    201 levels): Sigma = V^2 G_bath; beta = 10, nt = 200, ntau = 400, h = 0.02.  The bootstrap
+    given here is the free propagator of H(-1); the parity test solves dyson_mat and dyson_start
+    on the device instead."""
+    H = np.zeros((1, nt + 2, 1, 1), np.complex128)
+    H[0, 1:, 0, 0] = eps0
+    sigma = eq.kron_identity(eq.semicircle_bath(nt, ntau, beta, h), 1, V * V)
+    boot = [bootstrap_free(H[0, 0], 0.0, beta, h, k, ntau)]
+    descs = [dict(nt=nt, ntau=ntau, size1=1, sig=-1, solve_order=k, sigma_group=0, beta=beta, h=h, mu=0.0)]
+    info = dict(model="impurity level quenched 0 -> %g in a semicircular bath" % eps0, size1=1, nk=1, nt=nt,
+                ntau=ntau, beta=beta, h=h, solve_order=k, sigma="V^2 G_bath, V=%g" % V)
+    return Workload("impurity", descs, sigma, H, boot, k, info)
 
 
 def config1(nk=256, nt=1000, ntau=600, kshift=0.0):

@@ -2,6 +2,8 @@
 histories).  FP64 within 1e-10 and mixed precision within 1e-8 of the oracle, max|x - x_ref| /
 max|x_ref| per component over every time step:
 
+* config 0: the impurity quench end to end on the device (Matsubara solve, bootstrap and all
+  steps) against the oracle run in the test;
 * config 1: three k-points of the 2-band chain at its full shape (size1 2, nt 1000, ntau 600),
   every element against the oracle run in the test (OpenMP over the k-points);
 * config 3: a size1 = 5 and a size1 = 8 problem at nt 500, ntau 400, and config 4: a 2 x 3
@@ -30,6 +32,37 @@ def _golden(case):
             v = d[key]
             out[name] = float(v) if v.ndim == 0 else v
     return out
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_config0_impurity(oracle, prec):
+    """Config 0 end to end on the device (dyson_mat, dyson_start, dyson_timestep n = 6..200)
+    against the oracle's dyson_mat / dyson_start / dyson_timestep on the same Sigma and H."""
+    from nessi_b200 import function, gpu
+    W = workloads.config0()
+    d = W.descs[0]
+    nt, ntau, k = d["nt"], d["ntau"], W.k
+    H = function(nt, 1)
+    for t in range(-1, nt + 1):
+        H.set_value(t, W.H[0, t + 1])
+    ref = herm_matrix(nt, ntau, 1, -1)
+    oracle.dyson_mat(ref, W.sigma, d["mu"], H, d["beta"], k)
+    oracle.dyson_start(ref, d["mu"], H, W.sigma, d["beta"], d["h"], k)
+    for n in range(k + 1, nt + 1):
+        oracle.dyson_timestep(n, ref, d["mu"], H, W.sigma, d["beta"], d["h"], k)
+    b = gpu.Batch(W.descs, precision=prec)
+    b.set_sigma(0, W.sigma)
+    b.set_H(0, H)
+    b.dyson_mat()
+    b.dyson_start()
+    for n in range(k + 1, nt + 1):
+        b.dyson_timestep(n)
+    G = herm_matrix(nt, ntau, 1, -1)
+    b.get_G(0, G)
+    b.close()
+    e = component_errors(G, ref, 0, nt)
+    e["mat"] = float(np.max(np.abs(G.mat - ref.mat)) / np.max(np.abs(ref.mat)))
+    assert max(e.values()) < (TOL64 if prec == 0 else TOLMIX), e
 
 
 def test_config1_shape(oracle):
