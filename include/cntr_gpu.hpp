@@ -97,7 +97,7 @@ template <class HM, class FN> class Batch {
     void set_Q(int p, HM &Q) {
         check(nessi_gpu_set_Q(b_, p, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0)));
     }
-    void vie2_mat() { check(nessi_gpu_vie2_mat(b_)); }
+    void vie2_mat(int method = 2) { check(nessi_gpu_vie2_mat_method(b_, method)); }
     void vie2_start() { check(nessi_gpu_vie2_start(b_)); }
     void vie2_timestep(int n) { check(nessi_gpu_vie2_timestep(b_, n)); }
     // self-consistent lattice with the local second-order self-energy of G_loc
@@ -109,7 +109,9 @@ template <class HM, class FN> class Batch {
         return it;
     }
     void lattice_2b_timestep(int n, int corrector_steps) { check(nessi_gpu_lattice_2b_timestep(b_, n, corrector_steps)); }
-    void dyson_mat() { check(nessi_gpu_dyson_mat(b_)); }
+    void dyson_mat(int method = 2, bool force_hermitian = true) {
+        check(nessi_gpu_dyson_mat_method(b_, method, force_hermitian ? 1 : 0));
+    }
     void dyson_start() { check(nessi_gpu_dyson_start(b_)); }
     void dyson_timestep(int n) { check(nessi_gpu_dyson_timestep(b_, n)); }
     // copy time step n of problem p back into its herm_matrix
@@ -159,12 +161,14 @@ template <class HM, class FN> class Batch {
     std::vector<FN *> H_;
 };
 
-// Matsubara methods of libcntr (cntr_global_settings.hpp): the device solves by the default one
+// Matsubara methods of libcntr (cntr_global_settings.hpp); the device solves by the Fourier and
+// the fixpoint (default) methods, not by steepest descent (CNTR_MAT_CG = 1)
+constexpr int MAT_FOURIER = 0;
 constexpr int MAT_FIXPOINT = 2;
-inline void require_fixpoint(int method, bool force_hermitian = true) {
-    if (method != MAT_FIXPOINT || !force_hermitian)
-        throw std::invalid_argument("cntr_gpu: only the default Matsubara solve (CNTR_MAT_FIXPOINT, force_hermitian) "
-                                    "runs on the device");
+inline void require_device_method(int method) {
+    if (method != MAT_FOURIER && method != MAT_FIXPOINT)
+        throw std::invalid_argument("cntr_gpu: Matsubara method " + std::to_string(method) +
+                                    " is not available on the device (0 = Fourier, 2 = fixpoint)");
 }
 
 // ---- single-problem drop-ins (cntr_dyson_decl.hpp:78-92) -------------------------------
@@ -265,7 +269,7 @@ void dyson_start(HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int 
 template <class HM, class FN>
 void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT,
                bool force_hermitian = true) {
-    require_fixpoint(method, force_hermitian);
+    require_device_method(method);
     nessi_problem_desc d;
     d.nt = SolveOrder; d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
     d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = 1.0; d.mu = mu;
@@ -276,7 +280,7 @@ void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder =
     check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
     int rc = nessi_gpu_set_H(b, 0, h0.data());
     if (!rc) rc = nessi_gpu_set_sigma(b, 0, nullptr, nullptr, nullptr, Sigma.matptr(0));
-    if (!rc) rc = nessi_gpu_dyson_mat(b);
+    if (!rc) rc = nessi_gpu_dyson_mat_method(b, method, force_hermitian ? 1 : 0);
     if (!rc) rc = nessi_gpu_get_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
     nessi_gpu_batch_destroy(b);
     check(rc);
@@ -288,11 +292,11 @@ void dyson_mat(HM &G, double mu, FN &H, HM &Sigma, double beta, int SolveOrder =
 template <class HM, class FN>
 void dyson(HM &G, double mu, FN &H, HM &Sigma, double beta, double h, int SolveOrder = 5,
            int matsubara_method = MAT_FIXPOINT, bool force_hermitian = true) {
-    require_fixpoint(matsubara_method, force_hermitian);
+    require_device_method(matsubara_method);
     Batch<HM, FN> b;
     b.add(G, H, mu, beta, h, SolveOrder);
     b.build(Sigma);
-    b.dyson_mat();
+    b.dyson_mat(matsubara_method, force_hermitian);
     b.dyson_start();
     for (int n = SolveOrder + 1; n <= G.nt(); n++) b.dyson_timestep(n);
     b.download_all();
@@ -344,7 +348,7 @@ template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double
 // (only the Matsubara branches take part, so the matrices may hold it alone, nt = -1)
 template <class HM>
 void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT) {
-    require_fixpoint(method);
+    require_device_method(method);
     (void)Fcc;  // F^mat alone enters the Matsubara equation
     nessi_problem_desc d;
     d.nt = SolveOrder; d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
@@ -353,7 +357,7 @@ void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int
     check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
     int rc = nessi_gpu_set_F(b, 0, nullptr, nullptr, nullptr, F.matptr(0), nullptr, nullptr);
     if (!rc) rc = nessi_gpu_set_Q(b, 0, nullptr, nullptr, nullptr, Q.matptr(0));
-    if (!rc) rc = nessi_gpu_vie2_mat(b);
+    if (!rc) rc = nessi_gpu_vie2_mat_method(b, method);
     if (!rc) rc = nessi_gpu_get_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
     nessi_gpu_batch_destroy(b);
     check(rc);
@@ -363,9 +367,9 @@ void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int
 // vie2_mat, vie2_start and every time step on the device from one upload.
 template <class HM>
 void vie2(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5, int matsubara_method = MAT_FIXPOINT) {
-    require_fixpoint(matsubara_method);
+    require_device_method(matsubara_method);
     nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, h, SolveOrder, false);
-    int rc = nessi_gpu_vie2_mat(b);
+    int rc = nessi_gpu_vie2_mat_method(b, matsubara_method);
     if (!rc) rc = nessi_gpu_vie2_start(b);
     for (int n = SolveOrder + 1; n <= G.nt() && !rc; n++) rc = nessi_gpu_vie2_timestep(b, n);
     if (!rc) rc = nessi_gpu_get_G(b, 0, G.retptr(0, 0), G.lesptr(0, 0), G.tvptr(0, 0), G.matptr(0));

@@ -88,6 +88,11 @@ int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void
  * method and force_hermitian (cntr_dyson_decl.hpp:78, cntr_dyson_impl.hpp:1393-1450): G^mat of
  * every problem from H(-1) and the group's Sigma^mat.  ntau must be even. */
 int nessi_gpu_dyson_mat(nessi_batch *b);
+/* The same with libcntr's method argument (cntr_dyson_impl.hpp:1393-1450, dispatch :1209-1230):
+ * 0 = CNTR_MAT_FOURIER (dyson_mat_fourier_dispatch, :356-446: 21 oversampling copies of the
+ * Matsubara frequencies, first-order tail), 2 = CNTR_MAT_FIXPOINT; force_hermitian as libcntr's.
+ * Method 1 (CNTR_MAT_CG, steepest descent) is not built: NESSI_ERR_ARG. */
+int nessi_gpu_dyson_mat_method(nessi_batch *b, int method, int force_hermitian);
 /* cntr::dyson_start(G, mu, H, Sigma, beta, h, SolveOrder) (cntr_dyson_decl.hpp:88,
  * cntr_dyson_impl.hpp:1502-1535): time steps 0..k of every problem from G^mat. */
 int nessi_gpu_dyson_start(nessi_batch *b);
@@ -115,6 +120,10 @@ int nessi_gpu_set_Q_timestep(nessi_batch *b, int p, int tstp, const void *slice)
  * (cntr_vie2_decl.hpp:63, cntr_vie2_impl.hpp:460-484, 1091-1160): G^mat of every VIE2 problem
  * from the group's F^mat and the problem's Q^mat.  ntau must be even. */
 int nessi_gpu_vie2_mat(nessi_batch *b);
+/* The same with libcntr's method argument (cntr_vie2_impl.hpp:1280-1336): 0 = CNTR_MAT_FOURIER
+ * (vie2_mat_fourier with 20 oversampling copies, no corrections), 2 = CNTR_MAT_FIXPOINT.
+ * Method 1 (steepest descent) is not built: NESSI_ERR_ARG. */
+int nessi_gpu_vie2_mat_method(nessi_batch *b, int method);
 /* cntr::vie2_start(G, F, Fcc, Q, SolveOrder, beta, h) (cntr_vie2_decl.hpp:67,
  * cntr_vie2_impl.hpp:1338-1420): time steps 0..k of every VIE2 problem from G^mat. */
 int nessi_gpu_vie2_start(nessi_batch *b);

@@ -257,10 +257,84 @@ __device__ void vie2_mat_fourier_dev(double2 *G, const double2 *F, const double2
     __syncthreads();
 }
 
-// Body of dyson_mat for one problem (one CTA): reads g.smat, g.k, g.ntau, g.sig, g.beta and
-// p.H, p.mu; writes p.gmat; uses the scratch vectors of w.
+// force_matsubara_hermitian (cntr_utilities_impl.hpp:2077-2090): G(tau) = (G(tau) + G(tau)^dagger) / 2
 template <int S>
-__device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScratch &w) {
+__device__ void force_mat_hermitian_dev(double2 *G, double2 *tmp, int ntau) {
+    constexpr int s2 = S * S;
+    for (int e = threadIdx.x; e < (ntau + 1) * s2; e += blockDim.x) {
+        const int m = e / s2, ab = e % s2, a = ab / S, b = ab % S;
+        tmp[e] = cscale(cadd(G[e], cconj(G[(long)m * s2 + b * S + a])), 0.5);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (ntau + 1) * s2; e += blockDim.x) G[e] = tmp[e];
+    __syncthreads();
+}
+
+// G^mat by the Fourier method (dyson_mat_fourier_dispatch, cntr_dyson_impl.hpp:356-446):
+//   G(tau_r) = first-order tail - 1/2 (+ tau_r / beta for bosons)
+//            + (1/beta) sum_{m=-ntau/2}^{ntau/2-1} sum_{p=-10}^{10} z(mm) e^{-i omega_mm tau_r},  mm = m + p ntau,
+//   z(mm) = (i omega - x)^{-1} x / (i omega),  x = H(-1) - mu + Sigma(i omega_mm)
+//   (bosons at mm = 0: z = -x^{-1}); Sigma(i omega) = matsubara_ft with cubic endpoint corrections.
+// The sum over (m, p) is taken per phase class q = (2 mm + one) mod 2 ntau as in vie2_mat_fourier_dev.
+// hj = H(-1) - mu (shared, s^2), sdft = DFT of Sigma^mat (mat_dft_dev).
+template <int S>
+__device__ void dyson_mat_fourier_dev(double2 *G, const double2 *Sig, const double2 *sdft, const double2 *hj,
+                                      double2 *Z, int ntau, int sig, double beta, const double2 *tw) {
+    constexpr int s2 = S * S;
+    const int one = sig == -1 ? 1 : 0, m2 = ntau / 2, NQ = 2 * ntau, pcf = 10;
+    const double pi = 3.14159265358979323846, dtau = beta / ntau;
+    for (int q = threadIdx.x; q < NQ; q += blockDim.x) {
+        double2 acc[s2];
+        for (int ab = 0; ab < s2; ab++) acc[ab] = cmk(0, 0);
+        if (((q - one) & 1) == 0) {
+            const int mres = ((q - one) / 2) % ntau;  // m + p ntau = mres (mod ntau)
+            const int lo = -m2, hi = m2 - 1;
+            for (int p = -pcf; p <= pcf; p++) {
+                for (int m = lo + ((mres - lo) % ntau + ntau) % ntau; m <= hi; m += ntau) {
+                    const int mm = m + p * ntau;
+                    const double omn = (2.0 * mm + one) * pi / (ntau * dtau);
+                    double2 x[s2], y[s2], yinv[s2];
+                    mat_ft_dev<S>(x, mm, Sig, sdft, ntau, sig, beta, one);
+                    for (int ab = 0; ab < s2; ab++) x[ab] = cadd(x[ab], hj[ab]);
+                    if (sig == 1 && mm == 0) {
+                        small_inverse<S>(x, yinv);
+                        for (int ab = 0; ab < s2; ab++) acc[ab] = cfma(cmk(-1.0 / beta, 0), yinv[ab], acc[ab]);
+                    } else {
+                        for (int ab = 0; ab < s2; ab++) y[ab] = cneg(x[ab]);
+                        for (int a = 0; a < S; a++) y[a * S + a] = cadd(y[a * S + a], cmk(0, omn));
+                        small_inverse<S>(y, yinv);
+                        // (1/beta) (1/(i omega)) yinv x
+                        const double2 f = cmk(0.0, -1.0 / (omn * beta));
+                        for (int a = 0; a < S; a++)
+                            for (int d = 0; d < S; d++) {
+                                double2 t = cmk(0, 0);
+                                for (int b = 0; b < S; b++) t = cfma(yinv[a * S + b], x[b * S + d], t);
+                                acc[a * S + d] = cfma(f, t, acc[a * S + d]);
+                            }
+                    }
+                }
+            }
+        }
+        for (int ab = 0; ab < s2; ab++) Z[(long)q * s2 + ab] = acc[ab];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (ntau + 1) * s2; e += blockDim.x) {
+        const int r = e / s2, ab = e % s2;
+        const bool diag = ab / S == ab % S;
+        double2 v = cmk(diag ? -0.5 : 0.0, 0);
+        if (sig == 1 && diag) v = cadd(v, cmk((r * dtau) / beta, 0));
+        for (int q = one; q < NQ; q += 2) v = cfma(Z[(long)q * s2 + ab], twid(tw, -(long)q * r, ntau), v);
+        G[e] = v;
+    }
+    __syncthreads();
+}
+
+// Body of dyson_mat for one problem (one CTA): reads g.smat, g.k, g.ntau, g.sig, g.beta and
+// p.H, p.mu; writes p.gmat; uses the scratch vectors of w.  method: 0 = Fourier
+// (dyson_mat_fourier_dispatch), 2 = fixpoint (the default); force_herm: force_matsubara_hermitian.
+template <int S>
+__device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScratch &w, int method = 2,
+                               int force_herm = 1) {
     constexpr int s2 = S * S;
     __shared__ double ev[S];
     __shared__ double2 V[S * S], qmasy[S * S];
@@ -271,6 +345,16 @@ __device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScr
         double sn, cs;
         sincospi((double)q / (double)ntau, &sn, &cs);
         tw[q] = cmk(cs, sn);
+    }
+    if (method == 0) {
+        __shared__ double2 hj[S * S];
+        if (threadIdx.x < s2) hj[threadIdx.x] = csub(p.H[threadIdx.x], cmk(threadIdx.x / S == threadIdx.x % S ? p.mu : 0.0, 0));
+        __syncthreads();
+        mat_dft_dev<S>(w.fdft, g.smat, ntau, sig == -1 ? 1 : 0, tw);
+        __syncthreads();
+        dyson_mat_fourier_dev<S>(p.gmat, g.smat, w.fdft, hj, w.Z, ntau, sig, beta, tw);
+        if (force_herm) force_mat_hermitian_dev<S>(p.gmat, w.dG, ntau);
+        return;
     }
     // G0 = green_from_H(H(-1), mu): G0(tau) = -V fexp(tau, e) V^dag (fermions), V bexp V^dag (bosons)
     if (threadIdx.x == 0) {
@@ -313,27 +397,23 @@ __device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScr
         for (int e = threadIdx.x; e < M * s2; e += blockDim.x) p.gmat[e] = csub(p.gmat[e], w.dG[e]);
         __syncthreads();
     }
-    // force_matsubara_hermitian
-    for (int e = threadIdx.x; e < M * s2; e += blockDim.x) {
-        const int m = e / s2, ab = e % s2, a = ab / S, b = ab % S;
-        const double2 x = p.gmat[e], y = p.gmat[(long)m * s2 + b * S + a];
-        w.dG[e] = cscale(cadd(x, cconj(y)), 0.5);
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < M * s2; e += blockDim.x) p.gmat[e] = w.dG[e];
+    if (force_herm) force_mat_hermitian_dev<S>(p.gmat, w.dG, ntau);
 }
 
 template <int S>
-__global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr) {
-    dyson_mat_body<S>(g, probs[blockIdx.x], scr[blockIdx.x]);
+__global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr,
+                                                   int method, int force_herm) {
+    dyson_mat_body<S>(g, probs[blockIdx.x], scr[blockIdx.x], method, force_herm);
 }
 
 // vie2_mat on the device (cntr::vie2_mat with the default fixpoint method, cntr_vie2_impl.hpp:
 // 460-484, 1091-1160): G^mat = vie2_mat_fourier(F, Q) (:305-455), then 6 corrections
 // G -= fourier(F, F*G + G - Q).  F^mat is the group's (g.smat), Q^mat of the problem is in w.G0.
 // One CTA per problem.
+// method 0: the Fourier solve alone with 20 oversampling copies (vie2_mat_fourier, :1280-1336).
 template <int S>
-__global__ void __launch_bounds__(256) k_vie2_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr) {
+__global__ void __launch_bounds__(256) k_vie2_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr,
+                                                  int method) {
     constexpr int s2 = S * S;
     __shared__ double2 qmasy[S * S];
     extern __shared__ double2 tw[];  // 2 ntau twiddles e^{i pi q / ntau}
@@ -349,6 +429,10 @@ __global__ void __launch_bounds__(256) k_vie2_mat(GroupDev g, const ProbDev *__r
     __syncthreads();
     mat_dft_dev<S>(w.fdft, g.smat, ntau, sig == -1 ? 1 : 0, tw);
     __syncthreads();
+    if (method == 0) {
+        vie2_mat_fourier_dev<S>(p.gmat, g.smat, w.G0, w.fdft, w.qdft, w.Z, qmasy, ntau, sig, beta, 20, tw);
+        return;
+    }
     const int pcf = 5;
     vie2_mat_fourier_dev<S>(p.gmat, g.smat, w.G0, w.fdft, w.qdft, w.Z, qmasy, ntau, sig, beta, pcf, tw);
     for (int it = 0; it < 6; it++) {

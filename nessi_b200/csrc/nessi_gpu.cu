@@ -654,20 +654,20 @@ static int ensure_mat_scratch(nessi_batch *b, Group &g) {
     return NESSI_OK;
 }
 
-template <int S> int mat_group(nessi_batch *b, Group &g) {
+template <int S> int mat_group(nessi_batch *b, Group &g, int method, int force_herm) {
     const GroupDev gd = group_dev(g);
     CKR(check_twiddle_smem((const void *)k_dyson_mat<S>, g.ntau, "dyson_mat"));
     CKR(ensure_mat_scratch(b, g));
     const size_t sm = 2 * (size_t)g.ntau * sizeof(double2);
     CK(cudaFuncSetAttribute(k_dyson_mat<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_dyson_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat);
+    k_dyson_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat, method, force_herm);
     CK(cudaGetLastError());
     g.gmat_valid = false;
     return NESSI_OK;
 }
 
 // vie2_mat of a VIE2 group: Q^mat of every member is copied into its scratch slot G0 first
-template <int S> int vie2_mat_group(nessi_batch *b, Group &g) {
+template <int S> int vie2_mat_group(nessi_batch *b, Group &g, int method) {
     const GroupDev gd = group_dev(g);
     CKR(check_twiddle_smem((const void *)k_vie2_mat<S>, g.ntau, "vie2_mat"));
     CKR(ensure_mat_scratch(b, g));
@@ -680,7 +680,7 @@ template <int S> int vie2_mat_group(nessi_batch *b, Group &g) {
     }
     const size_t sm = 2 * (size_t)g.ntau * sizeof(double2);
     CK(cudaFuncSetAttribute(k_vie2_mat<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_vie2_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat);
+    k_vie2_mat<S><<<(unsigned)g.members.size(), 256, sm, b->stream>>>(gd, g.d_probs, g.d_mat, method);
     CK(cudaGetLastError());
     g.gmat_valid = false;
     return NESSI_OK;
@@ -752,8 +752,10 @@ int start_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(start_group, b,
 int extrap_dispatch(nessi_batch *b, Group &g, int n) { NESSI_SIZE_SWITCH(extrap_group, b, g, n) }
 int gloc_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(gloc_group, b, g, tstp) }
 int sigma2b_dispatch(nessi_batch *b, Group &g, int tstp) { NESSI_SIZE_SWITCH(sigma2b_group, b, g, tstp) }
-int mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(mat_group, b, g) }
-int vie2_mat_dispatch(nessi_batch *b, Group &g) { NESSI_SIZE_SWITCH(vie2_mat_group, b, g) }
+int mat_dispatch(nessi_batch *b, Group &g, int method, int force_herm) {
+    NESSI_SIZE_SWITCH(mat_group, b, g, method, force_herm)
+}
+int vie2_mat_dispatch(nessi_batch *b, Group &g, int method) { NESSI_SIZE_SWITCH(vie2_mat_group, b, g, method) }
 
 template <int S> int step_group_any(nessi_batch *b, Group &g, int n, int nact) {
     return g.vie ? step_group<S, true>(b, g, n, nact) : step_group<S, false>(b, g, n, nact);
@@ -1185,17 +1187,28 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
     return NESSI_OK;
 }
 
-int nessi_gpu_dyson_mat(nessi_batch *b) {
+// libcntr's Matsubara methods (cntr_global_settings.hpp): 0 Fourier, 1 steepest descent (CG), 2 fixpoint
+static int check_mat_method(int method, const char *name) {
+    if (method == 0 || method == 2) return NESSI_OK;
+    set_err("%s: method %d not available (0 = Fourier, 2 = fixpoint; the steepest-descent method 1 is not built)",
+            name, method);
+    return NESSI_ERR_ARG;
+}
+
+int nessi_gpu_dyson_mat_method(nessi_batch *b, int method, int force_hermitian) {
     NvtxRange nvtx_("nessi::dyson_mat");
     CKR(check_batch(b));
+    CKR(check_mat_method(method, "dyson_mat"));
     for (Group &g : b->groups) {
         if (g.vie) continue;  // VIE2 groups take G^mat from the caller
         if (g.ntau % 2) { set_err("dyson_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
-        CKR(mat_dispatch(b, g));
+        CKR(mat_dispatch(b, g, method, force_hermitian ? 1 : 0));
     }
     CK(cudaStreamSynchronize(b->stream));
     return NESSI_OK;
 }
+
+int nessi_gpu_dyson_mat(nessi_batch *b) { return nessi_gpu_dyson_mat_method(b, 2, 1); }
 
 static int start_kind(nessi_batch *b, bool vie, const char *name) {
     NvtxRange nvtx_(vie ? "nessi::vie2_start" : "nessi::dyson_start");
@@ -1225,15 +1238,18 @@ int nessi_gpu_dyson_start(nessi_batch *b) { return start_kind(b, false, "dyson_s
 
 int nessi_gpu_vie2_start(nessi_batch *b) { return start_kind(b, true, "vie2_start"); }
 
-int nessi_gpu_vie2_mat(nessi_batch *b) {
+int nessi_gpu_vie2_mat(nessi_batch *b) { return nessi_gpu_vie2_mat_method(b, 2); }
+
+int nessi_gpu_vie2_mat_method(nessi_batch *b, int method) {
     NvtxRange nvtx_("nessi::vie2_mat");
     CKR(check_batch(b));
+    CKR(check_mat_method(method, "vie2_mat"));
     bool any = false;
     for (Group &g : b->groups) {
         if (!g.vie) continue;
         any = true;
         if (g.ntau % 2) { set_err("vie2_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
-        CKR(vie2_mat_dispatch(b, g));
+        CKR(vie2_mat_dispatch(b, g, method));
     }
     if (!any) { set_err("vie2_mat: the batch has no VIE2 group (nessi_gpu_set_F)"); return NESSI_ERR_ARG; }
     CK(cudaStreamSynchronize(b->stream));

@@ -61,6 +61,8 @@ EXPORTS = {
     "nessi_gpu_dyson_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_dyson_mat": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_dyson_start": (ctypes.c_int, [ctypes.c_void_p]),
+    "nessi_gpu_dyson_mat_method": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "nessi_gpu_vie2_mat_method": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "nessi_gpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "nessi_gpu_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "nessi_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -210,9 +212,9 @@ class Batch:
     def dyson_timestep(self, n):
         _check(load_library().nessi_gpu_dyson_timestep(self._h, n))
 
-    def dyson_mat(self):
-        """G^mat of every problem (cntr::dyson_mat, fixpoint method)."""
-        _check(load_library().nessi_gpu_dyson_mat(self._h))
+    def dyson_mat(self, method=2, force_hermitian=True):
+        """G^mat of every problem (cntr::dyson_mat; method 0 = Fourier, 2 = fixpoint, the default)."""
+        _check(load_library().nessi_gpu_dyson_mat_method(self._h, int(method), int(bool(force_hermitian))))
 
     def dyson_start(self):
         """Time steps 0..k of every problem (cntr::dyson_start)."""
@@ -243,9 +245,9 @@ class Batch:
         _check(load_library().nessi_gpu_set_Q_timestep(self._h, p, tstp, _ptr(np.ascontiguousarray(data,
                                                                                                     np.complex128))))
 
-    def vie2_mat(self):
-        """G^mat of every VIE2 problem (cntr::vie2_mat, fixpoint method)."""
-        _check(load_library().nessi_gpu_vie2_mat(self._h))
+    def vie2_mat(self, method=2):
+        """G^mat of every VIE2 problem (cntr::vie2_mat; method 0 = Fourier, 2 = fixpoint, the default)."""
+        _check(load_library().nessi_gpu_vie2_mat_method(self._h, int(method)))
 
     def vie2_start(self):
         """Time steps 0..k of every VIE2 problem (cntr::vie2_start)."""
@@ -439,17 +441,17 @@ def dyson_timestep(n, G, mu, H, Sigma, beta, h, SolveOrder=5):
     b.close()
 
 
-def dyson(G, mu, H, Sigma, beta, h, SolveOrder=5):
-    """cntr::dyson(G, mu, H, Sigma, beta, h, SolveOrder) (cntr_dyson_decl.hpp:95-98,
-    cntr_dyson_impl.hpp:1725-1734): dyson_mat (fixpoint), dyson_start and every time step on the
-    GPU from one upload; all of G is written."""
+def dyson(G, mu, H, Sigma, beta, h, SolveOrder=5, matsubara_method=2, force_hermitian=True):
+    """cntr::dyson(G, mu, H, Sigma, beta, h, SolveOrder, matsubara_method, force_hermitian)
+    (cntr_dyson_decl.hpp:95-98, cntr_dyson_impl.hpp:1725-1734): dyson_mat (method 0 Fourier or
+    2 fixpoint), dyson_start and every time step on the GPU from one upload; all of G is written."""
     b = Batch([dict(nt=G.nt, ntau=G.ntau, size1=G.size1, sig=G.sig, solve_order=SolveOrder, beta=beta, h=h,
                     mu=mu)])
     try:
         b.set_G(0, G)
         b.set_H(0, H)
         b.set_sigma(0, Sigma)
-        b.dyson_mat()
+        b.dyson_mat(matsubara_method, force_hermitian)
         b.dyson_start()
         for n in range(SolveOrder + 1, G.nt + 1):
             b.dyson_timestep(n)
@@ -458,14 +460,15 @@ def dyson(G, mu, H, Sigma, beta, h, SolveOrder=5):
         b.close()
 
 
-def vie2(G, F, Fcc, Q, beta, h, SolveOrder=5):
-    """cntr::vie2(G, F, Fcc, Q, beta, h, SolveOrder) (cntr_vie2_decl.hpp:85-86): [1 + F] G = Q by
-    vie2_mat (fixpoint), vie2_start and every time step on the GPU from one upload."""
+def vie2(G, F, Fcc, Q, beta, h, SolveOrder=5, matsubara_method=2):
+    """cntr::vie2(G, F, Fcc, Q, beta, h, SolveOrder, matsubara_method) (cntr_vie2_decl.hpp:85-86):
+    [1 + F] G = Q by vie2_mat (method 0 Fourier or 2 fixpoint), vie2_start and every time step on
+    the GPU from one upload."""
     b = Batch([dict(nt=G.nt, ntau=G.ntau, size1=G.size1, sig=G.sig, solve_order=SolveOrder, beta=beta, h=h)])
     try:
         b.set_F(0, F, Fcc)
         b.set_Q(0, Q)
-        b.vie2_mat()
+        b.vie2_mat(matsubara_method)
         b.vie2_start()
         for n in range(SolveOrder + 1, G.nt + 1):
             b.vie2_timestep(n)
@@ -480,16 +483,21 @@ def _value_at_minus1(X, s):
     return np.ascontiguousarray(a, np.complex128).reshape(s, s)
 
 
-def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None):
-    """cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder) with the default fixpoint method and
-    force_hermitian (cntr_dyson_decl.hpp:77-79): writes G^mat.  With ``SigmaMF`` (a
-    cntr::function or the (s, s) matrix of its value at -1) it is the mean-field overload
-    dyson_mat(G, mu, H, SigmaMF, Sigma, beta, SolveOrder) (:81-83; cntr_dyson_impl.hpp:472-492,
-    1270-1298): with G0 the free propagator of H(-1), [1 + F] G = G0 is solved by the fixpoint
-    with F = -(G0 * Sigma + G0 SigmaMF(-1)); the convolution and the fixpoint run on the GPU."""
+def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None, method=2, force_hermitian=True):
+    """cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder, method, force_hermitian)
+    (cntr_dyson_decl.hpp:77-79): writes G^mat; method 0 = Fourier (dyson_mat_fourier_dispatch,
+    cntr_dyson_impl.hpp:356-446), 2 = fixpoint (the default).  With ``SigmaMF`` (a cntr::function
+    or the (s, s) matrix of its value at -1) it is the mean-field overload
+    dyson_mat(G, mu, H, SigmaMF, Sigma, beta, SolveOrder, method) (:81-83; cntr_dyson_impl.hpp:
+    472-492, 1270-1298): the Fourier method takes H(-1) + SigmaMF(-1) as the one-body part; the
+    fixpoint method, with G0 the free propagator of H(-1), solves [1 + F] G = G0 with
+    F = -(G0 * Sigma + G0 SigmaMF(-1)); the convolution and the solves run on the GPU."""
     from .equilibrium import green_from_H
     k, s, ntau, sig = SolveOrder, G.size1, G.ntau, G.sig
     h0 = _value_at_minus1(H, s)
+    if SigmaMF is not None and method == 0:
+        h0 = h0 + _value_at_minus1(SigmaMF, s)
+        SigmaMF = None
     Sk = herm_matrix(k, ntau, s, sig)  # only the Matsubara branch takes part
     Sk.mat[...] = Sigma.mat
     desc = dict(nt=k, ntau=ntau, size1=s, sig=sig, solve_order=k, beta=beta, h=1.0, mu=mu)
@@ -499,7 +507,7 @@ def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None):
         try:
             b.set_H(0, np.broadcast_to(h0, (k + 2, s, s)).copy())
             b.set_sigma(0, Sk)
-            b.dyson_mat()
+            b.dyson_mat(method, force_hermitian)
             b.get_G(0, out)
         finally:
             b.close()
@@ -520,7 +528,10 @@ def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None):
         b.get_G(0, out)
     finally:
         b.close()
-    G.mat[...] = 0.5 * (out.mat + out.mat.conj().transpose(0, 2, 1))  # force_matsubara_hermitian
+    if force_hermitian:
+        G.mat[...] = 0.5 * (out.mat + out.mat.conj().transpose(0, 2, 1))  # force_matsubara_hermitian
+    else:
+        G.mat[...] = out.mat
 
 
 def vie2_timestep_sin(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, SolveOrder=5):

@@ -1,0 +1,86 @@
+"""The Matsubara solvers' method argument on the GPU against the oracle: dyson_mat with
+CNTR_MAT_FOURIER (dyson_mat_fourier_dispatch, cntr_dyson_impl.hpp:356-446) and with the fixpoint,
+force_hermitian on and off (:1393-1450), and vie2_mat with the Fourier method
+(cntr_vie2_impl.hpp:1280-1336).  Bar: 1e-10 relative."""
+import numpy as np
+import pytest
+
+from builders import make_H, make_sigma, rand_herm, rel_err
+from nessi_b200 import herm_matrix
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+FOURIER, CG, FIXPOINT = 0, 1, 2
+
+
+def _dyson_mat_pair(oracle, s, sig, method, force_herm, ntau=24, seed=0):
+    from nessi_b200 import gpu
+    rng = np.random.default_rng(seed)
+    nt, beta, h, mu, k = 6, 5.0, 0.05, 0.1, 5
+    Sig = make_sigma(oracle, rng, nt, ntau, s, sig, beta, h)
+    H = make_H(rng, nt, s, h)
+    if sig == 1:  # bosonic levels above zero
+        for t in range(-1, nt + 1):
+            H.data[t + 1] += 3.0 * np.eye(s)
+    Go = herm_matrix(nt, ntau, s, sig)
+    oracle.dyson_mat(Go, Sig, mu, H, beta, k, method=method, force_hermitian=force_herm)
+    b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=s, sig=sig, solve_order=k, beta=beta, h=h, mu=mu)])
+    b.set_sigma(0, Sig)
+    b.set_H(0, H)
+    b.dyson_mat(method, force_herm)
+    Gg = herm_matrix(nt, ntau, s, sig)
+    b.get_G(0, Gg)
+    b.close()
+    return Gg.mat, Go.mat
+
+
+@pytest.mark.parametrize("s,sig", [(1, -1), (2, -1), (3, -1), (1, 1), (2, 1), (5, -1)])
+def test_dyson_mat_fourier(oracle, s, sig):
+    g, o = _dyson_mat_pair(oracle, s, sig, FOURIER, True, seed=11 * s + sig)
+    assert rel_err(g, o) < TOL
+
+
+@pytest.mark.parametrize("method", [FOURIER, FIXPOINT])
+def test_dyson_mat_without_force_hermitian(oracle, method):
+    g, o = _dyson_mat_pair(oracle, 2, -1, method, False, seed=5)
+    assert rel_err(g, o) < TOL
+
+
+def test_dyson_mat_fourier_and_fixpoint_agree(oracle):
+    """Two discretisations of the same equation: close, not equal (the Fourier tail is first order)."""
+    g0, _ = _dyson_mat_pair(oracle, 2, -1, FOURIER, True, ntau=200, seed=3)
+    g2, _ = _dyson_mat_pair(oracle, 2, -1, FIXPOINT, True, ntau=200, seed=3)
+    assert rel_err(g0, g2) < 1e-3
+
+
+def test_dyson_mat_steepest_descent_refused():
+    from nessi_b200 import gpu
+    b = gpu.Batch([dict(nt=6, ntau=10, size1=1, sig=-1, solve_order=5, beta=5.0, h=0.05, mu=0.0)])
+    with pytest.raises(gpu.NessiGpuError) as ei:
+        b.dyson_mat(CG)
+    assert ei.value.code == 1
+    b.close()
+
+
+@pytest.mark.parametrize("s", [1, 2, 3])
+def test_vie2_mat_fourier(oracle, s):
+    from nessi_b200 import gpu
+    rng = np.random.default_rng(900 + s)
+    nt, ntau, beta, h, k = 6, 16, 4.0, 0.05, 5
+    A = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.6)
+    B = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.5)
+    F = herm_matrix(nt, ntau, s, -1)
+    oracle.convolution_matsubara(F, A, B, beta, k)
+    F.mat[...] *= -1.0
+    Q = herm_matrix(nt, ntau, s, -1)
+    oracle.green_from_H(Q, 0.1, rand_herm(rng, s, 0.8), beta, h)
+    Go = herm_matrix(nt, ntau, s, -1)
+    oracle.vie2_mat(Go, F, F, Q, beta, k, method=FOURIER)
+    b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, beta=beta, h=h)])
+    b.set_F(0, F, F)
+    b.set_Q(0, Q)
+    b.vie2_mat(FOURIER)
+    m = np.zeros((ntau + 1, s, s), np.complex128)
+    b.get_timestep(0, -1, m)
+    b.close()
+    assert rel_err(m, Go.mat) < TOL
