@@ -161,14 +161,15 @@ template <class HM, class FN> class Batch {
     std::vector<FN *> H_;
 };
 
-// Matsubara methods of libcntr (cntr_global_settings.hpp); the device solves by the Fourier and
-// the fixpoint (default) methods, not by steepest descent (CNTR_MAT_CG = 1)
+// Matsubara methods of libcntr (cntr_global_settings.hpp); dyson_mat solves by all three on the
+// device, vie2_mat by the Fourier and the fixpoint methods (steepest descent needs Fcc^mat)
 constexpr int MAT_FOURIER = 0;
+constexpr int MAT_CG = 1;
 constexpr int MAT_FIXPOINT = 2;
-inline void require_device_method(int method) {
-    if (method != MAT_FOURIER && method != MAT_FIXPOINT)
+inline void require_device_method(int method, bool vie = false) {
+    if (method != MAT_FOURIER && method != MAT_FIXPOINT && (vie || method != MAT_CG))
         throw std::invalid_argument("cntr_gpu: Matsubara method " + std::to_string(method) +
-                                    " is not available on the device (0 = Fourier, 2 = fixpoint)");
+                                    " is not available on the device for " + (vie ? "vie2_mat" : "dyson_mat"));
 }
 
 // ---- single-problem drop-ins (cntr_dyson_decl.hpp:78-92) -------------------------------
@@ -348,7 +349,7 @@ template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double
 // (only the Matsubara branches take part, so the matrices may hold it alone, nt = -1)
 template <class HM>
 void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT) {
-    require_device_method(method);
+    require_device_method(method, true);
     (void)Fcc;  // F^mat alone enters the Matsubara equation
     nessi_problem_desc d;
     d.nt = SolveOrder; d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
@@ -367,7 +368,7 @@ void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int
 // vie2_mat, vie2_start and every time step on the device from one upload.
 template <class HM>
 void vie2(HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h, int SolveOrder = 5, int matsubara_method = MAT_FIXPOINT) {
-    require_device_method(matsubara_method);
+    require_device_method(matsubara_method, true);
     nessi_batch *b = vie2_batch(G, F, Fcc, Q, beta, h, SolveOrder, false);
     int rc = nessi_gpu_vie2_mat_method(b, matsubara_method);
     if (!rc) rc = nessi_gpu_vie2_start(b);

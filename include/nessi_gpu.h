@@ -90,8 +90,9 @@ int nessi_gpu_set_sigma_timestep(nessi_batch *b, int group, int tstp, const void
 int nessi_gpu_dyson_mat(nessi_batch *b);
 /* The same with libcntr's method argument (cntr_dyson_impl.hpp:1393-1450, dispatch :1209-1230):
  * 0 = CNTR_MAT_FOURIER (dyson_mat_fourier_dispatch, :356-446: 21 oversampling copies of the
- * Matsubara frequencies, first-order tail), 2 = CNTR_MAT_FIXPOINT; force_hermitian as libcntr's.
- * Method 1 (CNTR_MAT_CG, steepest descent) is not built: NESSI_ERR_ARG. */
+ * Matsubara frequencies, first-order tail), 1 = CNTR_MAT_CG (dyson_mat_steep_dispatch, :519-540:
+ * conjugate gradients from a Fourier start, 40 iterations, tol 1e-12), 2 = CNTR_MAT_FIXPOINT;
+ * force_hermitian as libcntr's.  Other methods: NESSI_ERR_ARG. */
 int nessi_gpu_dyson_mat_method(nessi_batch *b, int method, int force_hermitian);
 /* cntr::dyson_start(G, mu, H, Sigma, beta, h, SolveOrder) (cntr_dyson_decl.hpp:88,
  * cntr_dyson_impl.hpp:1502-1535): time steps 0..k of every problem from G^mat. */
@@ -120,9 +121,9 @@ int nessi_gpu_set_Q_timestep(nessi_batch *b, int p, int tstp, const void *slice)
  * (cntr_vie2_decl.hpp:63, cntr_vie2_impl.hpp:460-484, 1091-1160): G^mat of every VIE2 problem
  * from the group's F^mat and the problem's Q^mat.  ntau must be even. */
 int nessi_gpu_vie2_mat(nessi_batch *b);
-/* The same with libcntr's method argument (cntr_vie2_impl.hpp:1280-1336): 0 = CNTR_MAT_FOURIER
+/* The same with libcntr's method argument (cntr_vie2_impl.hpp:1229-1250): 0 = CNTR_MAT_FOURIER
  * (vie2_mat_fourier with 20 oversampling copies, no corrections), 2 = CNTR_MAT_FIXPOINT.
- * Method 1 (steepest descent) is not built: NESSI_ERR_ARG. */
+ * Method 1 (steepest descent) needs Fcc^mat, which nessi_gpu_set_F does not take: NESSI_ERR_ARG. */
 int nessi_gpu_vie2_mat_method(nessi_batch *b, int method);
 /* cntr::vie2_start(G, F, Fcc, Q, SolveOrder, beta, h) (cntr_vie2_decl.hpp:67,
  * cntr_vie2_impl.hpp:1338-1420): time steps 0..k of every VIE2 problem from G^mat. */

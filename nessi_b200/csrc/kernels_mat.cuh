@@ -329,9 +329,84 @@ __device__ void dyson_mat_fourier_dev(double2 *G, const double2 *Sig, const doub
     __syncthreads();
 }
 
+// <X, Y> = sum_r w_r sum_ab Re (X(r)^dagger Y(r))_ab, w_r the Gregory omega at both ends of the tau
+// grid (the inner product of vie2_mat_steep_dispatch, cntr_vie2_impl.hpp:519-533); a fixed-order
+// tree over the CTA's threads (red: blockDim.x doubles, a power of two); every thread gets the sum.
+template <int S>
+__device__ double mat_dot_dev(const double2 *X, const double2 *Y, int ntau, int k, double *red) {
+    constexpr int s2 = S * S;
+    double acc = 0.0;
+    for (int r = threadIdx.x; r <= ntau; r += blockDim.x) {
+        const double w = r <= k ? greg_omega(k, r) : (r >= ntau - k ? greg_omega(k, ntau - r) : 1.0);
+        const double2 *x = X + (long)r * s2, *y = Y + (long)r * s2;
+        double t = 0.0;
+        for (int a = 0; a < S; a++)
+            for (int b = 0; b < S; b++)
+                for (int l = 0; l < S; l++) t += x[l * S + a].x * y[l * S + b].x + x[l * S + a].y * y[l * S + b].y;
+        acc += w * t;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    const double v = red[0];
+    __syncthreads();
+    return v;
+}
+
+// vie2_mat by steepest descent (vie2_mat_steep_dispatch, cntr_vie2_impl.hpp:486-600): a Fourier
+// solve with 3 oversampling copies as the start, then conjugate-gradient iterations on
+// A X = X + (F*X + X*Fcc)/2, at most maxiter, until sqrt(<R, R>) < tol (none when <R, R> <= tol).
+// fdft holds the DFT of F; qdft, Z the Fourier scratch; R, P, AP, T are (ntau+1) s^2 buffers
+// (T may overlap Z: it is used after the Fourier solve).
+template <int S>
+__device__ void vie2_mat_steep_dev(double2 *G, const double2 *F, const double2 *Fcc, const double2 *Q,
+                                   const double2 *fdft, double2 *qdft, double2 *Z, double2 *qmasy, double2 *R,
+                                   double2 *P, double2 *AP, double2 *T, double *red, int k, int ntau, int sig,
+                                   double beta, int maxiter, double tol, const double2 *tw) {
+    constexpr int s2 = S * S;
+    const int n = (ntau + 1) * s2;
+    const double dtau = beta / ntau;
+    vie2_mat_fourier_dev<S>(G, F, Q, fdft, qdft, Z, qmasy, ntau, sig, beta, 3, tw);
+    if (maxiter <= 0) return;
+    conv_mat_dev<S>(AP, F, G, k, ntau, sig, dtau);
+    conv_mat_dev<S>(T, G, Fcc, k, ntau, sig, dtau);
+    __syncthreads();
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const double2 x = cneg(csub(cadd(cscale(cadd(AP[e], T[e]), 0.5), G[e]), Q[e]));
+        R[e] = x;
+        P[e] = x;
+    }
+    __syncthreads();
+    double rsold = mat_dot_dev<S>(R, R, ntau, k, red);
+    if (rsold <= tol) return;
+    for (int iter = 0; iter < maxiter; iter++) {
+        conv_mat_dev<S>(AP, F, P, k, ntau, sig, dtau);
+        conv_mat_dev<S>(T, P, Fcc, k, ntau, sig, dtau);
+        __syncthreads();
+        for (int e = threadIdx.x; e < n; e += blockDim.x) AP[e] = cadd(cscale(cadd(AP[e], T[e]), 0.5), P[e]);
+        __syncthreads();
+        const double alpha = rsold / mat_dot_dev<S>(P, AP, ntau, k, red);
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            G[e] = cadd(G[e], cscale(P[e], alpha));
+            R[e] = csub(R[e], cscale(AP[e], alpha));
+        }
+        __syncthreads();
+        const double rsnew = mat_dot_dev<S>(R, R, ntau, k, red);
+        for (int e = threadIdx.x; e < n; e += blockDim.x) P[e] = cadd(R[e], cscale(P[e], rsnew / rsold));
+        __syncthreads();
+        rsold = rsnew;
+        if (sqrt(rsold) < tol) break;
+    }
+}
+
 // Body of dyson_mat for one problem (one CTA): reads g.smat, g.k, g.ntau, g.sig, g.beta and
 // p.H, p.mu; writes p.gmat; uses the scratch vectors of w.  method: 0 = Fourier
-// (dyson_mat_fourier_dispatch), 2 = fixpoint (the default); force_herm: force_matsubara_hermitian.
+// (dyson_mat_fourier_dispatch), 1 = steepest descent (dyson_mat_steep_dispatch, cntr_dyson_impl.hpp:
+// 519-540: F = -G0*Sigma, Fcc = -Sigma*G0, 40 iterations, tol 1e-12), 2 = fixpoint (the default);
+// force_herm: force_matsubara_hermitian.
 template <int S>
 __device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScratch &w, int method = 2,
                                int force_herm = 1) {
@@ -386,6 +461,19 @@ __device__ void dyson_mat_body(const GroupDev &g, const ProbDev &p, const MatScr
     __syncthreads();
     mat_dft_dev<S>(w.fdft, w.F, ntau, sig == -1 ? 1 : 0, tw);
     __syncthreads();
+    if (method == 1) {
+        __shared__ double red[256];  // blockDim.x = 256
+        // Fcc = -Sigma * G0 into Q (unused by the Fourier start); after the start the Fourier
+        // buffers hold the iteration: R = dG, P = fdft, AP = qdft, T = Z
+        conv_mat_dev<S>(w.Q, g.smat, w.G0, k, ntau, sig, dtau);
+        __syncthreads();
+        for (int e = threadIdx.x; e < M * s2; e += blockDim.x) w.Q[e] = cneg(w.Q[e]);
+        __syncthreads();
+        vie2_mat_steep_dev<S>(p.gmat, w.F, w.Q, w.G0, w.fdft, w.qdft, w.Z, qmasy, w.dG, w.fdft, w.qdft, w.Z, red, k,
+                              ntau, sig, beta, 40, 1.0e-12, tw);
+        if (force_herm) force_mat_hermitian_dev<S>(p.gmat, w.dG, ntau);
+        return;
+    }
     const int pcf = 5;
     vie2_mat_fourier_dev<S>(p.gmat, w.F, w.G0, w.fdft, w.qdft, w.Z, qmasy, ntau, sig, beta, pcf, tw);
     for (int it = 0; it < 6; it++) {

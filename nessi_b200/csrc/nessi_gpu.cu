@@ -1187,18 +1187,20 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
     return NESSI_OK;
 }
 
-// libcntr's Matsubara methods (cntr_global_settings.hpp): 0 Fourier, 1 steepest descent (CG), 2 fixpoint
-static int check_mat_method(int method, const char *name) {
-    if (method == 0 || method == 2) return NESSI_OK;
-    set_err("%s: method %d not available (0 = Fourier, 2 = fixpoint; the steepest-descent method 1 is not built)",
-            name, method);
+// libcntr's Matsubara methods (cntr_global_settings.hpp): 0 Fourier, 1 steepest descent (CG), 2 fixpoint.
+// vie2_mat by steepest descent needs Fcc^mat, which a VIE2 group does not hold (set_F takes Fcc's
+// retarded and lesser components only), so it is refused there.
+static int check_mat_method(int method, bool vie, const char *name) {
+    if (method == 0 || method == 2 || (method == 1 && !vie)) return NESSI_OK;
+    set_err("%s: method %d not available (%s)", name, method,
+            vie ? "0 = Fourier, 2 = fixpoint" : "0 = Fourier, 1 = steepest descent, 2 = fixpoint");
     return NESSI_ERR_ARG;
 }
 
 int nessi_gpu_dyson_mat_method(nessi_batch *b, int method, int force_hermitian) {
     NvtxRange nvtx_("nessi::dyson_mat");
     CKR(check_batch(b));
-    CKR(check_mat_method(method, "dyson_mat"));
+    CKR(check_mat_method(method, false, "dyson_mat"));
     for (Group &g : b->groups) {
         if (g.vie) continue;  // VIE2 groups take G^mat from the caller
         if (g.ntau % 2) { set_err("dyson_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
@@ -1243,7 +1245,7 @@ int nessi_gpu_vie2_mat(nessi_batch *b) { return nessi_gpu_vie2_mat_method(b, 2);
 int nessi_gpu_vie2_mat_method(nessi_batch *b, int method) {
     NvtxRange nvtx_("nessi::vie2_mat");
     CKR(check_batch(b));
-    CKR(check_mat_method(method, "vie2_mat"));
+    CKR(check_mat_method(method, true, "vie2_mat"));
     bool any = false;
     for (Group &g : b->groups) {
         if (!g.vie) continue;

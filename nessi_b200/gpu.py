@@ -213,7 +213,8 @@ class Batch:
         _check(load_library().nessi_gpu_dyson_timestep(self._h, n))
 
     def dyson_mat(self, method=2, force_hermitian=True):
-        """G^mat of every problem (cntr::dyson_mat; method 0 = Fourier, 2 = fixpoint, the default)."""
+        """G^mat of every problem (cntr::dyson_mat; method 0 = Fourier, 1 = steepest descent,
+        2 = fixpoint, the default)."""
         _check(load_library().nessi_gpu_dyson_mat_method(self._h, int(method), int(bool(force_hermitian))))
 
     def dyson_start(self):
@@ -486,7 +487,8 @@ def _value_at_minus1(X, s):
 def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None, method=2, force_hermitian=True):
     """cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder, method, force_hermitian)
     (cntr_dyson_decl.hpp:77-79): writes G^mat; method 0 = Fourier (dyson_mat_fourier_dispatch,
-    cntr_dyson_impl.hpp:356-446), 2 = fixpoint (the default).  With ``SigmaMF`` (a cntr::function
+    cntr_dyson_impl.hpp:356-446), 1 = steepest descent (dyson_mat_steep_dispatch, :519-540; not with
+    SigmaMF), 2 = fixpoint (the default).  With ``SigmaMF`` (a cntr::function
     or the (s, s) matrix of its value at -1) it is the mean-field overload
     dyson_mat(G, mu, H, SigmaMF, Sigma, beta, SolveOrder, method) (:81-83; cntr_dyson_impl.hpp:
     472-492, 1270-1298): the Fourier method takes H(-1) + SigmaMF(-1) as the one-body part; the
@@ -495,6 +497,8 @@ def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None, method=2, force
     from .equilibrium import green_from_H
     k, s, ntau, sig = SolveOrder, G.size1, G.ntau, G.sig
     h0 = _value_at_minus1(H, s)
+    if SigmaMF is not None and method == 1:
+        raise ValueError("dyson_mat: the steepest-descent method with SigmaMF is not available on the device")
     if SigmaMF is not None and method == 0:
         h0 = h0 + _value_at_minus1(SigmaMF, s)
         SigmaMF = None

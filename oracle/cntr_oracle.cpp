@@ -933,6 +933,76 @@ void vie2_mat_fourier_t(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int pcf, int 
     std::memcpy(G.matptr(0), xmat.data(), sizeof(cplx) * xmat.size());
 }
 
+// vie2_mat_steep_dispatch (cntr_vie2_impl.hpp:486-600): a Fourier solve with pcf = 3 as the start,
+// then conjugate-gradient iterations on A X = X + (F*X + X*Fcc)/2 with the inner product
+// <X, Y> = sum_r w_r sum_ab Re (X(r)^dagger Y(r))_ab, w_r = Gregory omega at both ends of the tau
+// grid; stops after maxiter iterations or when sqrt(<R, R>) < tol; no iteration when <R, R> <= tol.
+template <int S1>
+void vie2_mat_steep_t(HM &G, HM &F, HM &Fcc, HM &Q, double beta, const Integ &In, int maxiter, double tol) {
+    vie2_mat_fourier_t<S1>(G, F, Fcc, Q, beta, 3, 3);
+    if (maxiter <= 0) return;
+    const int ntau = G.ntau(), es = G.es, k = In.k;
+    El<S1> E(G.s);
+    auto buf = [&](std::vector<cplx> &v, orc_hm &h) {
+        v.assign((long)(ntau + 1) * es, 0.0);
+        h = {-1, ntau, G.s, G.sig(), nullptr, nullptr, nullptr, v.data()};
+    };
+    std::vector<cplx> vr, vap, vp, vc1, vc2;
+    orc_hm hr, hap, hp, hc1, hc2;
+    buf(vr, hr); buf(vap, hap); buf(vp, hp); buf(vc1, hc1); buf(vc2, hc2);
+    HM R(&hr), AP(&hap), P(&hp), C1(&hc1), C2(&hc2);
+    std::vector<cplx> tmp(es), xcc(es);
+    auto dot = [&](HM &X, HM &Y) {
+        double acc = 0.0;
+        for (int r = 0; r <= ntau; r++) {
+            const double w = r <= k ? In.gregory_omega(r) : (r >= ntau - k ? In.gregory_omega(ntau - r) : 1.0);
+            E.conj(xcc.data(), X.matptr(r));
+            E.mult(tmp.data(), xcc.data(), Y.matptr(r));
+            for (int l = 0; l < es; l++) acc += w * tmp[l].real();
+        }
+        return acc;
+    };
+    // R = Q - (G + (F*G + G*Fcc)/2), P = R
+    convolution_matsubara_t<S1>(C1, F, G, In, beta);
+    convolution_matsubara_t<S1>(C2, G, Fcc, In, beta);
+    for (int r = 0; r <= ntau; r++) {
+        cplx *x = R.matptr(r);
+        E.set(x, C1.matptr(r));
+        E.incr(x, C2.matptr(r));
+        E.smul(x, 0.5);
+        E.incr(x, G.matptr(r));
+        E.incr(x, -1.0, Q.matptr(r));
+        E.smul(x, -1.0);
+        E.set(P.matptr(r), x);
+    }
+    double rsold = dot(R, R);
+    if (rsold <= tol) return;
+    for (int iter = 0; iter < maxiter; iter++) {
+        convolution_matsubara_t<S1>(C1, F, P, In, beta);
+        convolution_matsubara_t<S1>(C2, P, Fcc, In, beta);
+        for (int r = 0; r <= ntau; r++) {
+            cplx *x = AP.matptr(r);
+            E.set(x, C1.matptr(r));
+            E.incr(x, C2.matptr(r));
+            E.smul(x, 0.5);
+            E.incr(x, P.matptr(r));
+        }
+        const double alpha = rsold / dot(P, AP);
+        for (int r = 0; r <= ntau; r++) {
+            E.incr(G.matptr(r), alpha, P.matptr(r));
+            E.incr(R.matptr(r), -alpha, AP.matptr(r));
+        }
+        const double rsnew = dot(R, R);
+        for (int r = 0; r <= ntau; r++) {
+            E.set(tmp.data(), R.matptr(r));
+            E.incr(tmp.data(), rsnew / rsold, P.matptr(r));
+            E.set(P.matptr(r), tmp.data());
+        }
+        rsold = rsnew;
+        if (std::sqrt(rsold) < tol) break;
+    }
+}
+
 template <int S1>
 void vie2_mat_fixpoint_t(HM &G, HM &F, HM &Fcc, HM &Q, double beta, const Integ &In, int nfix, int pcf,
                          int order) {
@@ -1536,15 +1606,19 @@ void orc_force_matsubara_hermitian(orc_hm *Gh) {
     }
 }
 
-// vie2_mat (cntr_vie2_impl.hpp:1280-1336): method 0 = Fourier (pcf 20), 2 = fixpoint (6 corrections, pcf 5)
+// vie2_mat (cntr_vie2_impl.hpp:1229-1250): method 0 = Fourier (pcf 20), 1 = steepest descent
+// (40 iterations, tol 1e-12), 2 = fixpoint (6 corrections, pcf 5)
 void orc_vie2_mat(orc_hm *G, orc_hm *F, orc_hm *Fcc, orc_hm *Q, double beta, int k, int method) {
     HM g(G), f(F), fcc(Fcc), q(Q);
     int s1 = g.s;
     if (method == 0) ORC_DISPATCH(vie2_mat_fourier_t, g, f, fcc, q, beta, 20, 3);
+    else if (method == 1) ORC_DISPATCH(vie2_mat_steep_t, g, f, fcc, q, beta, I(k), 40, 1.0e-12);
     else ORC_DISPATCH(vie2_mat_fixpoint_t, g, f, fcc, q, beta, I(k), 6, 5, 3);
 }
 
-// dyson_mat (cntr_dyson_impl.hpp:1393-1450); method 0 = Fourier, 2 = fixpoint (default)
+// dyson_mat (cntr_dyson_impl.hpp:1393-1450); method 0 = Fourier, 1 = steepest descent
+// (dyson_mat_steep_dispatch, :519-540: F = -G0*Sigma, Fcc = -Sigma*G0, 40 iterations, tol 1e-12),
+// 2 = fixpoint (default)
 void orc_dyson_mat(orc_hm *Gh, orc_hm *Sh, double mu, const cplx *H, int k, double beta, int method,
                    int force_hermitian) {
     HM G(Gh), S(Sh);
@@ -1560,7 +1634,16 @@ void orc_dyson_mat(orc_hm *Gh, orc_hm *Sh, double mu, const cplx *H, int k, doub
         orc_convolution_matsubara(&gf, &g0, Sh, k, beta);
         for (auto &x : fm) x = -x;
         HM hg0(&g0), hf(&gf);
-        ORC_DISPATCH(vie2_mat_fixpoint_t, G, hf, hf, hg0, beta, I(k), 6, 5, 3);
+        if (method == 1) {
+            std::vector<cplx> fcm((long)(ntau + 1) * es);
+            orc_hm gfc = {-1, ntau, G.s, G.sig(), nullptr, nullptr, nullptr, fcm.data()};
+            orc_convolution_matsubara(&gfc, Sh, &g0, k, beta);
+            for (auto &x : fcm) x = -x;
+            HM hfc(&gfc);
+            ORC_DISPATCH(vie2_mat_steep_t, G, hf, hfc, hg0, beta, I(k), 40, 1.0e-12);
+        } else {
+            ORC_DISPATCH(vie2_mat_fixpoint_t, G, hf, hf, hg0, beta, I(k), 6, 5, 3);
+        }
     }
     if (force_hermitian) orc_force_matsubara_hermitian(Gh);
 }

@@ -18,6 +18,7 @@ _SO = os.path.join(_HERE, "libcntr_oracle.so")
 _lib = None
 
 CNTR_MAT_FOURIER = 0
+CNTR_MAT_CG = 1
 CNTR_MAT_FIXPOINT = 2
 
 

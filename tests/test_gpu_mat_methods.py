@@ -1,7 +1,8 @@
 """The Matsubara solvers' method argument on the GPU against the oracle: dyson_mat with
-CNTR_MAT_FOURIER (dyson_mat_fourier_dispatch, cntr_dyson_impl.hpp:356-446) and with the fixpoint,
-force_hermitian on and off (:1393-1450), and vie2_mat with the Fourier method
-(cntr_vie2_impl.hpp:1280-1336).  Bar: 1e-10 relative."""
+CNTR_MAT_FOURIER (dyson_mat_fourier_dispatch, cntr_dyson_impl.hpp:356-446), CNTR_MAT_CG
+(dyson_mat_steep_dispatch, :519-540) and the fixpoint, force_hermitian on and off (:1393-1450),
+and vie2_mat with the Fourier method (cntr_vie2_impl.hpp:1229-1250).  Bar: 1e-10 relative; and
+libcntr's own known answer for all three dyson_mat methods with its bounds."""
 import numpy as np
 import pytest
 
@@ -53,11 +54,46 @@ def test_dyson_mat_fourier_and_fixpoint_agree(oracle):
     assert rel_err(g0, g2) < 1e-3
 
 
-def test_dyson_mat_steepest_descent_refused():
+@pytest.mark.parametrize("s,sig", [(1, -1), (2, -1), (3, -1), (2, 1)])
+def test_dyson_mat_steepest_descent(oracle, s, sig):
+    g, o = _dyson_mat_pair(oracle, s, sig, CG, True, seed=17 * s + sig)
+    assert rel_err(g, o) < TOL
+
+
+@pytest.mark.parametrize("method,tol", [(FOURIER, 1e-3), (FIXPOINT, 1e-7), (CG, 1e-7)])
+def test_dyson_mat_methods_known_answer(oracle, method, tol):
+    """libcntr's own known answer (libcntr/test/matsubara.cpp:33-106) with its bounds, on the GPU."""
+    from test_oracle_mat_methods import embedding_case
+    from nessi_b200 import distance_norm2, gpu
+    exact, Sig, h1, beta = embedding_case(oracle)
+    ntau = exact.ntau
+    b = gpu.Batch([dict(nt=5, ntau=ntau, size1=1, sig=-1, solve_order=5, beta=beta, h=1.0, mu=0.0)])
+    b.set_sigma(0, _padded(Sig, 5))
+    b.set_H(0, np.broadcast_to(h1, (7, 1, 1)).copy())
+    b.dyson_mat(method)
+    m = np.zeros((ntau + 1, 1, 1), np.complex128)
+    b.get_timestep(0, -1, m)
+    b.close()
+    G = herm_matrix(-1, ntau, 1, -1)
+    G.mat[...] = m
+    assert distance_norm2(-1, exact, G) < tol
+
+
+def _padded(S, nt):
+    """A Matsubara-only herm_matrix as one with nt time steps (zero real-time components)."""
+    P = herm_matrix(nt, S.ntau, S.size1, S.sig)
+    P.mat[...] = S.mat
+    return P
+
+
+def test_vie2_mat_steepest_descent_refused():
     from nessi_b200 import gpu
     b = gpu.Batch([dict(nt=6, ntau=10, size1=1, sig=-1, solve_order=5, beta=5.0, h=0.05, mu=0.0)])
+    F = herm_matrix(6, 10, 1, -1)
+    b.set_F(0, F, F)
+    b.set_Q(0, F)
     with pytest.raises(gpu.NessiGpuError) as ei:
-        b.dyson_mat(CG)
+        b.vie2_mat(CG)
     assert ei.value.code == 1
     b.close()
 
