@@ -28,7 +28,7 @@
 #include "kernels_gemm.cuh"
 
 template <int S> struct ClCfg {
-    static constexpr int JB = S <= 2 ? 32 : 8;        // rows per block (>= k+1)
+    static constexpr int JB = S <= 2 ? 32 : (S <= 4 ? 16 : 8);  // rows per block (>= k+1)
     static constexpr int s2 = S * S;
     static constexpr int TRI = JB * (JB - 1) / 2;     // packed strictly-lower block triangle
     static constexpr int DWMAX = S <= 2 ? 8 : 2;      // chain warps (problems) per CTA
@@ -52,6 +52,11 @@ __device__ __forceinline__ unsigned cl_nrank() {
     return r;
 }
 __device__ __forceinline__ double2 ldcg2(const double2 *p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned long long global_ns_cl() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // ---- trailing-update operands -------------------------------------------------------------
 // ret: A(r = (j, d), kk = (i, b)) = T(m = mlo + i, j)[b][d] (triangle rows m, contiguous in j)
@@ -424,22 +429,21 @@ template <int BN> struct ClGemm {
     static constexpr int smem = 2 * zg::Smem<BM, BN>::total;  // two tile groups
 };
 
-// Grid: CL x nclusters CTAs of 256 threads (cluster dimension CL along x); cluster c owns the
-// problems c*PT .. min(nact, (c+1)*PT)-1 of the group (group order = descending nt, so the active
-// problems are a prefix).  acc: far-sum accumulators, rows (t, .) x columns (p, .), leading
-// dimension ldc (ret: [(j, d)][(p, a)], les: [(j, a)][(p, d)]); panel: the solved block's
-// weighted rows.  Every CTA runs the same block loop, so all reach every cluster barrier.
-template <int S, bool VIE, bool RET, int BN>
-__global__ void __launch_bounds__(256, 1) k_volterra_cl(GroupDev g, const ProbDev *__restrict__ probs, int n,
-                                                        int nact, int PT, double2 *acc, double2 *panel) {
+// The block loop of one group of CTAs (a cluster, or the whole grid of a cooperative launch)
+// owning the problems p0 .. p0+np-1 of the group (group order = descending nt, so the active
+// problems are a prefix); PT >= np sets the chain warps per CTA.  acc: far-sum accumulators, rows
+// (t, .) x columns (p, .), leading dimension ldc (ret: [(j, d)][(p, a)], les: [(j, a)][(p, d)]);
+// panel: the solved block's weighted rows.  Every CTA runs the same block loop, so all reach every
+// barrier; SY provides rank(), nrank() and sync() (false: a bounded wait gave up, leave the loop).
+template <int S, bool VIE, bool RET, int BN, class SY>
+__device__ __forceinline__ void volterra_blocked(const GroupDev &g, const ProbDev *__restrict__ probs, int n, int p0,
+                                                 int np, int PT, double2 *acc, double2 *panel, const SY &sy) {
     extern __shared__ double2 smem[];
     constexpr int s2 = S * S, JB = ClCfg<S>::JB, BM = ClGemm<BN>::BM;
     constexpr int DW = ClCfg<S>::DWMAX;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int rank = (int)cl_rank(), CL = (int)cl_nrank();
-    const int cid = blockIdx.x / CL;
-    const int p0 = cid * PT, np = min(PT, nact - p0);
-    const int cmax = (p0 + np) * S, c0 = p0 * S;  // GEMM columns of the cluster
+    const int rank = sy.rank(), CL = sy.nrank();
+    const int cmax = (p0 + np) * S, c0 = p0 * S;  // GEMM columns of the group of CTAs
     const int k = g.k, K1 = k + 1;
     const double h = g.h;
     const long ldc = g.ldc;
@@ -486,7 +490,7 @@ __global__ void __launch_bounds__(256, 1) k_volterra_cl(GroupDev g, const ProbDe
                 else cl_les_diag_big<S, VIE>(g, p, n, b, jlo, jhi, nb, acc, sig, wb, ibd, panel, ws, lane);
             }
         }
-        cl_sync();
+        if (!sy.sync()) return;
         if (b + 1 == nblk) break;
         // phase G: trailing update of every row still to be solved
         {
@@ -509,8 +513,80 @@ __global__ void __launch_bounds__(256, 1) k_volterra_cl(GroupDev g, const ProbDe
                 }
             }
         }
-        cl_sync();
+        if (!sy.sync()) return;
     }
+}
+
+struct ClusterSync {
+    __device__ __forceinline__ int rank() const { return (int)cl_rank(); }
+    __device__ __forceinline__ int nrank() const { return (int)cl_nrank(); }
+    __device__ __forceinline__ bool sync() const {
+        cl_sync();
+        return true;
+    }
+};
+
+// Grid: CL x nclusters CTAs of 256 threads (cluster dimension CL along x); cluster c owns the
+// problems c*PT .. min(nact, (c+1)*PT)-1 of the group.
+template <int S, bool VIE, bool RET, int BN>
+__global__ void __launch_bounds__(256, 1) k_volterra_cl(GroupDev g, const ProbDev *__restrict__ probs, int n,
+                                                        int nact, int PT, double2 *acc, double2 *panel) {
+    const int p0 = (int)(blockIdx.x / cl_nrank()) * PT;
+    volterra_blocked<S, VIE, RET, BN>(g, probs, n, p0, min(PT, nact - p0), PT, acc, panel, ClusterSync{});
+}
+
+// Barrier of all CTAs of a cooperative launch (all resident at once): an arrival counter and a
+// generation word in global memory; thread 0 of each CTA arrives and waits, bounded by limit_ns of
+// %globaltimer.  A wait that gives up sets *err = NESSI_ERR_TIMEOUT and *abort = 1; a waiter that
+// sees *abort gives up too, and the kernel returns from its block loop.  count and abort are zero
+// at launch (the host clears them before every launch).  Data written before the barrier by other
+// CTAs are read after it through L2 (ld.global.cg), as in the cluster form.
+struct GridSync {
+    unsigned *count, *gen;
+    int *abort, *err;
+    long long limit_ns;
+    __device__ __forceinline__ int rank() const { return (int)blockIdx.x; }
+    __device__ __forceinline__ int nrank() const { return (int)gridDim.x; }
+    __device__ bool sync() const {
+        __shared__ int s_ok;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            const unsigned g0 = *(volatile unsigned *)gen;
+            __threadfence();
+            if (atomicAdd(count, 1u) == gridDim.x - 1) {
+                atomicExch(count, 0u);
+                __threadfence();
+                atomicAdd(gen, 1u);
+            } else {
+                const unsigned long long t0 = global_ns_cl();
+                while (*(volatile unsigned *)gen == g0) {
+                    if (*(volatile int *)abort) { ok = 0; break; }
+                    if ((long long)(global_ns_cl() - t0) > limit_ns) {
+                        atomicExch(err, 5);  // NESSI_ERR_TIMEOUT
+                        atomicExch(abort, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+            if (*(volatile int *)abort) ok = 0;
+            s_ok = ok;
+        }
+        __syncthreads();
+        return s_ok != 0;
+    }
+};
+
+// The whole grid (one cooperative launch, one CTA per SM) owns the problems p0 .. p0+np-1: the
+// trailing GEMM of every block is spread over all SMs, which suits groups of few problems with
+// long histories (size1 >= 3), where a cluster's 8 SMs would hold the whole group.
+template <int S, bool VIE, bool RET, int BN>
+__global__ void __launch_bounds__(256, 1) k_volterra_grid(GroupDev g, const ProbDev *__restrict__ probs, int n,
+                                                          int p0, int np, double2 *acc, double2 *panel, GridSync gs) {
+    volterra_blocked<S, VIE, RET, BN>(g, probs, n, p0, np, np, acc, panel, gs);
 }
 
 // ---- start blocks of the cluster path (one CTA per problem) ---------------------------------

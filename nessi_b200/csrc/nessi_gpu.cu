@@ -174,6 +174,7 @@ struct nessi_batch {
     int tv_kernel = 0;
     int nsm = 0;                        // SMs of the device
     int *d_err = nullptr;               // set by a device wait that gave up (NESSI_ERR_TIMEOUT)
+    unsigned *d_gbar = nullptr;         // grid barrier of k_volterra_grid: count, generation, abort
     long long wait_ns = 2000000000LL;   // bound of every mbarrier wait in the batch's kernels
 
     void prof_mark(int id, cudaStream_t st = nullptr) {
@@ -279,6 +280,7 @@ int zgemm_launch(const LA &la, const LB &lb, const ST &st, int M, int N, int K, 
 
 // Volterra choice code of the group-wide cluster path (k_ret_start / k_les_start + k_volterra_cl)
 #define NESSI_VOLTERRA_CLUSTER 100
+#define NESSI_VOLTERRA_GRID 101  // the blocked recursion by one cooperative launch over all SMs
 #define NESSI_CL 8  // CTAs per cluster (portable cluster size)
 
 template <int S> size_t ret_start_smem(int k) {
@@ -377,11 +379,70 @@ int cluster_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret
     return cluster_kernel_launch<S, VIE, false, 32>(gd, g, n, nact, PT, ncl, acc, g.panel, st);
 }
 
-// One Volterra recursion (ret or les) of a step: the one-problem kernels (pp = -1) or the
-// multi-problem tensor-core kernels with pp problems per CTA (size1 <= 2).
-template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &g, int n, int nact, bool ret, int pp,
-                                               cudaStream_t st) {
+template <int S, bool VIE, bool RET, int BN>
+int grid_kernel_launch(nessi_batch *b, const GroupDev &gd, const Group &g, int n, int p0, int np, double2 *acc,
+                       cudaStream_t st) {
+    const size_t sm = (size_t)std::max(ClSmem<S>::diag, ClGemm<BN>::smem) * sizeof(double2);
+    auto kern = k_volterra_grid<S, VIE, RET, BN>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm));
+    if (per < 1) { set_err("k_volterra_grid: no CTA fits on an SM"); return NESSI_ERR_CUDA; }
+    // barrier words: arrival counter, generation, abort flag (cleared before every launch)
+    CK(cudaMemsetAsync(b->d_gbar, 0, 4 * sizeof(unsigned), st));
+    GridSync gs{b->d_gbar, b->d_gbar + 1, (int *)(b->d_gbar + 2), b->d_err, b->wait_ns};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->nsm);  // one CTA per SM, all resident (cooperative launch)
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kern, gd, (const ProbDev *)g.d_probs, n, p0, np, acc, g.panel, gs));
+    return NESSI_OK;
+}
+
+// Group-wide recursion by the whole GPU: the start block of every problem (one CTA each), then
+// the blocked recursion with every block's trailing GEMM over all SMs, in chunks of at most
+// nsm x ClCfg::DWMAX problems (one chain warp each).
+template <int S, bool VIE>
+int grid_launch(nessi_batch *b, const GroupDev &gd, const Group &g, int n, int nact, bool ret, cudaStream_t st) {
+    if (ret) {
+        const size_t sm = ret_start_smem<S>(gd.k);
+        CK(cudaFuncSetAttribute(k_ret_start<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_ret_start<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+    } else {
+        const size_t sm = les_start_smem<S>(gd.k);
+        CK(cudaFuncSetAttribute(k_les_start<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_les_start<S, VIE><<<nact, 256, sm, st>>>(gd, g.d_probs, n);
+    }
+    CK(cudaGetLastError());
+    if (n - gd.k <= 0) return NESSI_OK;
+    double2 *acc = ret ? g.accr : g.accl;
+    const int chunk = b->nsm * ClCfg<S>::DWMAX;
+    for (int p0 = 0; p0 < nact; p0 += chunk) {
+        const int np = std::min(chunk, nact - p0);
+        if (np * S > 32) {
+            if (ret) CKR((grid_kernel_launch<S, VIE, true, 64>(b, gd, g, n, p0, np, acc, st)));
+            else CKR((grid_kernel_launch<S, VIE, false, 64>(b, gd, g, n, p0, np, acc, st)));
+        } else {
+            if (ret) CKR((grid_kernel_launch<S, VIE, true, 32>(b, gd, g, n, p0, np, acc, st)));
+            else CKR((grid_kernel_launch<S, VIE, false, 32>(b, gd, g, n, p0, np, acc, st)));
+        }
+    }
+    return NESSI_OK;
+}
+
+// One Volterra recursion (ret or les) of a step: the one-problem kernels (pp = -1), the
+// multi-problem tensor-core kernels with pp problems per CTA (size1 <= 2), or the blocked
+// recursion by clusters (pp = NESSI_VOLTERRA_CLUSTER) or by the whole GPU (NESSI_VOLTERRA_GRID).
+template <int S, bool VIE> int volterra_launch(nessi_batch *b, const GroupDev &gd, const Group &g, int n, int nact,
+                                               bool ret, int pp, cudaStream_t st) {
     if (pp == NESSI_VOLTERRA_CLUSTER) return cluster_launch<S, VIE>(gd, g, n, nact, ret, st);
+    if (pp == NESSI_VOLTERRA_GRID) return grid_launch<S, VIE>(b, gd, g, n, nact, ret, st);
     if constexpr (S <= 2) {
         if (pp > 0) {
             const size_t sm = (size_t)MpCfg<S>::total * sizeof(double2);
@@ -427,16 +488,19 @@ template <int S, bool VIE> int volterra_launch(const GroupDev &gd, const Group &
 template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const GroupDev &gd, int n, int nact, bool ret,
                                              cudaStream_t st) {
     int &choice = ret ? g.pp_ret : g.pp_les;
-    if (b->volterra_pp != 0) return volterra_launch<S, VIE>(gd, g, n, nact, ret, b->volterra_pp, st);
-    if (choice != 0) return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);
+    if (b->volterra_pp != 0) return volterra_launch<S, VIE>(b, gd, g, n, nact, ret, b->volterra_pp, st);
+    if (choice != 0) return volterra_launch<S, VIE>(b, gd, g, n, nact, ret, choice, st);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cap));
     const int tune_n = std::max(std::min(128, g.ntmax), (3 * g.ntmax) / 4);
-    if (cap != cudaStreamCaptureStatusNone || n < tune_n) return volterra_launch<S, VIE>(gd, g, n, nact, ret, -1, st);
-    // candidates: one problem per CTA, the per-CTA tensor-core kernels (size1 <= 2), the cluster path
-    const int cand_small[5] = {-1, 2, 4, 8, NESSI_VOLTERRA_CLUSTER}, cand_big[2] = {-1, NESSI_VOLTERRA_CLUSTER};
+    if (cap != cudaStreamCaptureStatusNone || n < tune_n)
+        return volterra_launch<S, VIE>(b, gd, g, n, nact, ret, -1, st);
+    // candidates: one problem per CTA, the per-CTA tensor-core kernels (size1 <= 2), the cluster
+    // path; for size1 >= 3 also the whole-GPU path
+    const int cand_small[5] = {-1, 2, 4, 8, NESSI_VOLTERRA_CLUSTER};
+    const int cand_big[3] = {-1, NESSI_VOLTERRA_CLUSTER, NESSI_VOLTERRA_GRID};
     const int *cand = S <= 2 ? cand_small : cand_big;
-    const int ncand = S <= 2 ? 5 : 2;
+    const int ncand = S <= 2 ? 5 : 3;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -446,7 +510,7 @@ template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const Gro
         for (int ic = 0; ic < ncand; ic++) {
             const int c = cand[ic];
             CK(cudaEventRecord(e0, st));
-            CKR((volterra_launch<S, VIE>(gd, g, n, nact, ret, c, st)));
+            CKR((volterra_launch<S, VIE>(b, gd, g, n, nact, ret, c, st)));
             CK(cudaEventRecord(e1, st));
             CK(cudaEventSynchronize(e1));
             float ms = 0;
@@ -456,7 +520,7 @@ template <int S, bool VIE> int volterra_step(nessi_batch *b, Group &g, const Gro
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     choice = bestc;
-    return volterra_launch<S, VIE>(gd, g, n, nact, ret, choice, st);  // the kept variant writes last
+    return volterra_launch<S, VIE>(b, gd, g, n, nact, ret, choice, st);  // the kept variant writes last
 }
 
 // Decomposition of k_tv_stream: tau chunk width tw <= TWMAX chosen to balance the items
@@ -815,7 +879,8 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
     b->precision = precision;
     if (const char *v = getenv("NESSI_VOLTERRA_PP")) {
         const int pp = atoi(v);
-        if (pp == -1 || pp == 0 || pp == 1 || pp == 2 || pp == 4 || pp == 8 || pp == NESSI_VOLTERRA_CLUSTER)
+        if (pp == -1 || pp == 0 || pp == 1 || pp == 2 || pp == 4 || pp == 8 || pp == NESSI_VOLTERRA_CLUSTER ||
+            pp == NESSI_VOLTERRA_GRID)
             b->volterra_pp = pp;
     }
     if (const char *v = getenv("NESSI_TV_KERNEL")) b->tv_kernel = strcmp(v, "regs") == 0 ? 1 : 0;
@@ -832,6 +897,13 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
         }
         b->allocs.push_back(q);
         b->d_err = (int *)q;
+        q = nullptr;
+        if (cudaMalloc(&q, 4 * sizeof(unsigned)) != cudaSuccess || cudaMemset(q, 0, 4 * sizeof(unsigned)) != cudaSuccess) {
+            set_err("cudaMalloc of the grid barrier failed");
+            return fail(NESSI_ERR_OOM);
+        }
+        b->allocs.push_back(q);
+        b->d_gbar = (unsigned *)q;
     }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
         set_err("stream creation failed");

@@ -102,10 +102,10 @@ def volterra_pp(monkeypatch):
 
 
 @pytest.mark.parametrize("s", [1, 2])
-@pytest.mark.parametrize("pp", [-1, 1, 2, 4, 8, 100])
+@pytest.mark.parametrize("pp", [-1, 1, 2, 4, 8, 100, 101])
 def test_volterra_problems_per_cta(oracle, volterra_pp, s, pp):
-    """Every grouping of problems per CTA (and the one-problem kernels, -1, and the group-wide
-    cluster recursion, 100) gives the oracle's numbers on an uneven batch whose histories span
+    """Every grouping of problems per CTA (and the one-problem kernels, -1, the group-wide
+    cluster recursion, 100, and the whole-GPU recursion, 101) gives the oracle's numbers on an uneven batch whose histories span
     several 32-row blocks; the batch size is not a multiple of the grouping, so partly filled CTAs
     are exercised too."""
     volterra_pp(pp)
@@ -116,10 +116,11 @@ def test_volterra_problems_per_cta(oracle, volterra_pp, s, pp):
 
 
 @pytest.mark.parametrize("s,nt", [(3, 40), (4, 36), (5, 30), (8, 28)])
-@pytest.mark.parametrize("pp", [-1, 100])
+@pytest.mark.parametrize("pp", [-1, 100, 101])
 def test_volterra_large_orbitals(oracle, volterra_pp, s, nt, pp):
-    """size1 >= 3: the one-problem kernels and the cluster recursion (blocks of 8 rows, several
-    blocks per step, an uneven batch) against the oracle."""
+    """size1 >= 3: the one-problem kernels, the cluster recursion and the whole-GPU recursion
+    (blocks of 16 rows for size1 3-4, 8 above; several blocks per step, an uneven batch) against
+    the oracle."""
     volterra_pp(pp)
     errs = _run(oracle, s, [nt, nt - 9, nt, 12], 8, seed=60 + s)
     for e in errs:
@@ -127,10 +128,11 @@ def test_volterra_large_orbitals(oracle, volterra_pp, s, nt, pp):
             assert v < TOL, (comp, v)
 
 
-def test_cluster_recursion_many_problems(oracle, volterra_pp):
+@pytest.mark.parametrize("pp", [100, 101])
+def test_cluster_recursion_many_problems(oracle, volterra_pp, pp):
     """More problems than one cluster holds (several clusters, the last one partly filled), each
-    history spanning several blocks."""
-    volterra_pp(100)
+    history spanning several blocks; the same batch through the whole-GPU recursion."""
+    volterra_pp(pp)
     errs = _run(oracle, 1, [70] * 40 + [33, 51], 10, seed=77)
     for e in errs:
         for comp, v in e.items():

@@ -10,10 +10,15 @@ from builders import make_H, make_lattice, make_sigma, rel_err, solve_oracle, co
 pytestmark = pytest.mark.gpu
 
 
-def test_graph_replay_dyson(oracle):
+@pytest.mark.parametrize("s,pp", [(2, None), (4, 101)])
+def test_graph_replay_dyson(oracle, monkeypatch, s, pp):
+    """pp = 101: the whole-GPU Volterra recursion, a cooperative launch with its barrier reset,
+    inside the graph."""
     from nessi_b200 import gpu
+    if pp is not None:
+        monkeypatch.setenv("NESSI_VOLTERRA_PP", str(pp))
     rng = np.random.default_rng(21)
-    nt, ntau, s, beta, h, k, mu = 60, 20, 2, 4.0, 0.05, 5, 0.1
+    nt, ntau, beta, h, k, mu = 60, 20, 4.0, 0.05, 5, 0.1
     Sig = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h)
     Hs, Go, G0 = [], [], []
     for _ in range(3):

@@ -245,10 +245,12 @@ def test_vie2_mat_and_whole_pipeline(oracle, s):
 
 
 @pytest.mark.parametrize("s", [3, 5])
-def test_vie2_cluster_recursion_large_orbitals(oracle, monkeypatch, s):
-    """The VIE2 form of the cluster recursion for size1 >= 3 (element-parallel chains)."""
+@pytest.mark.parametrize("pp", [100, 101])
+def test_vie2_cluster_recursion_large_orbitals(oracle, monkeypatch, s, pp):
+    """The VIE2 form of the cluster and whole-GPU recursions for size1 >= 3 (element-parallel
+    chains)."""
     from nessi_b200 import gpu
-    monkeypatch.setenv("NESSI_VOLTERRA_PP", "100")
+    monkeypatch.setenv("NESSI_VOLTERRA_PP", str(pp))
     rng = np.random.default_rng(700 + s)
     nt, ntau, beta, h, k = 30, 8, 4.0, 0.05, 5
     F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
