@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from builders import make_H, make_sigma, rel_err
-from nessi_b200 import herm_matrix
+from nessi_b200 import herm_matrix, workloads
 
 pytestmark = pytest.mark.gpu
 
@@ -23,9 +23,12 @@ def _propagate(oracle, monkeypatch, kernel, s, nprob, nt, ntau, prec, seed, nts=
                   precision=prec)
     b.set_sigma(0, Sig)
     for p in range(nprob):
-        b.set_H(p, make_H(rng, nts[p], s, h))
-    b.dyson_mat()
-    b.dyson_start()
+        H = make_H(rng, nts[p], s, h)
+        b.set_H(p, H)
+        boot = workloads.bootstrap_free(H.get_value(-1), mu, beta, h, k, ntau)  # any ntau, odd included
+        b.set_timestep(p, -1, boot.mat)
+        for t in range(k + 1):
+            b.set_timestep(p, t, boot.get_timestep(t))
     for n in range(k + 1, nt + 1):
         b.dyson_timestep(n)
     b.synchronize()
@@ -38,12 +41,13 @@ def _propagate(oracle, monkeypatch, kernel, s, nprob, nt, ntau, prec, seed, nts=
     return out
 
 
-@pytest.mark.parametrize("s,nprob,nt,ntau", [(1, 3, 30, 301), (1, 160, 16, 100), (2, 5, 24, 61), (3, 2, 20, 40),
-                                             (4, 3, 18, 33)])
+@pytest.mark.parametrize("s,nprob,nt,ntau", [(1, 3, 30, 300), (1, 160, 16, 101), (2, 5, 24, 60), (3, 2, 20, 41),
+                                             (4, 3, 18, 32)])
 @pytest.mark.parametrize("prec", [0, 1])
 def test_stream_matches_register_kernel(oracle, monkeypatch, s, nprob, nt, ntau, prec):
-    """Odd and even ntau + 1 (FP32 segments that start 8 bytes past a 16-byte boundary), one
-    chunk per problem (160 problems) and several, FP64 and mixed precision."""
+    """Odd and even ntau + 1 (odd: FP32 segments that start 8 bytes past a 16-byte boundary), one
+    chunk per problem (160 problems) and several, FP64 and mixed precision; the bootstrap is the
+    free propagator of H(-1)."""
     a = _propagate(oracle, monkeypatch, "stream", s, nprob, nt, ntau, prec, seed=s)
     r = _propagate(oracle, monkeypatch, "regs", s, nprob, nt, ntau, prec, seed=s)
     for p in range(nprob):
@@ -72,9 +76,12 @@ def test_stream_wait_timeout_is_reported(oracle, monkeypatch):
     b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=1, sig=-1, solve_order=k, beta=beta, h=h, mu=0.0)] * 2)
     b.set_sigma(0, Sig)
     for p in range(2):
-        b.set_H(p, make_H(rng, nt, 1, h))
-    b.dyson_mat()
-    b.dyson_start()
+        H = make_H(rng, nt, 1, h)
+        b.set_H(p, H)
+        boot = workloads.bootstrap_free(H.get_value(-1), 0.0, beta, h, k, ntau)
+        b.set_timestep(p, -1, boot.mat)
+        for t in range(k + 1):
+            b.set_timestep(p, t, boot.get_timestep(t))
     b.synchronize()
     b.set_wait_limit(0)
     b.dyson_timestep(k + 1)
