@@ -18,11 +18,11 @@
 
 #define MP_JB 32  // rows per block (lane = row)
 #define MP_NW 16  // warps per CTA: warps 0..PP-1 own a problem's chain, all of them share phase A
-// Registers per thread of the multi-problem kernels.  For size1 = 1, 512 threads x 96 leave 16384
-// of an SM's 65536 registers to a CTA of the tv history stream (k_tv_stream), which runs beside
-// them on the main stream while they run on the side stream (at the cost of ~100-250 bytes of
-// spills per thread); size1 = 2 would spill over 1 KB at 96 and keeps the 128 of 512 threads.
-#define MP_MAXREG(S) ((S) == 1 ? 96 : 128)
+// Registers per thread of the multi-problem kernels: 128 (the most a 512-thread CTA can have).
+// Capping size1 = 1 at 96, so that a k_tv_stream CTA fits beside, cost ~100-270 bytes of spills
+// per thread and made the lesser recursion 20 % slower in the config-4 step, while the tv stream
+// gained nothing from the company; so both kernels keep their own SMs' registers.
+#define MP_MAXREG(S) 128
 
 template <int S> struct MpCfg {
     static constexpr int s2 = S * S;

@@ -169,9 +169,9 @@ struct nessi_batch {
     int volterra_pp = 0;
     double2 *scratch = nullptr;  // G^tv in libcntr layout during layout conversion (size1 > 1)
     long scratch_n = 0;
-    // kernel of the tv row for size1 <= 4: 0 (default) = k_tv_stream (history through shared
-    // memory by bulk copies), 1 = k_tv (register loads); size1 > 4 always uses k_tv
-    int tv_kernel = 0;
+    // kernel of the tv row: 1 (default) = k_tv (register loads, every size1), 0 = k_tv_stream
+    // (history through shared memory by bulk copies, size1 <= 4; NESSI_TV_KERNEL=stream)
+    int tv_kernel = 1;
     int nsm = 0;                        // SMs of the device
     int *d_err = nullptr;               // set by a device wait that gave up (NESSI_ERR_TIMEOUT)
     unsigned *d_gbar = nullptr;         // grid barrier of k_volterra_grid: count, generation, abort
@@ -447,17 +447,11 @@ template <int S, bool VIE> int volterra_launch(nessi_batch *b, const GroupDev &g
         if (pp > 0) {
             const size_t sm = (size_t)MpCfg<S>::total * sizeof(double2);
             const unsigned grid = (unsigned)((nact + pp - 1) / pp);
-            // the largest shared-memory carveout, so that an SM holding one of these CTAs can also
-            // take a k_tv_stream CTA without reconfiguring
             if (ret) {
                 CK(cudaFuncSetAttribute(k_ret_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                CK(cudaFuncSetAttribute(k_ret_mp<S, VIE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        cudaSharedmemCarveoutMaxShared));
                 k_ret_mp<S, VIE><<<grid, MP_NW * 32, sm, st>>>(gd, g.d_probs, n, nact, pp);
             } else {
                 CK(cudaFuncSetAttribute(k_les_mp<S, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                CK(cudaFuncSetAttribute(k_les_mp<S, VIE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        cudaSharedmemCarveoutMaxShared));
                 k_les_mp<S, VIE><<<grid, MP_NW * 32, sm, st>>>(gd, g.d_probs, n, nact, pp);
             }
             CK(cudaGetLastError());
@@ -591,8 +585,6 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
         b->prof_end(NESSI_KERNEL_PREP, 0.0);
         g.dense_valid = n - 1;
     }
-    CK(cudaEventRecord(b->ev_fork, st));
-    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     // VIE2 moves the convolution to the right-hand side: gles = -(tv*vt + les*adv)
     const double alpha = VIE ? -1.0 : 1.0;
     // Matsubara part of the tv row: Cmat = K_n Gmat_all (one GEMM for the group)
@@ -617,8 +609,9 @@ template <int S, bool VIE> int step_group(nessi_batch *b, Group &g, int n, int n
     }
     const int m = nact * S, nn = (n + 1) * S;
     const long ldL = (long)(g.ntmax + 1) * S, ldT = (long)(g.ntau + 1) * S;
-    // side stream: retarded row, then les*adv = Ldense * badv (needs only G^R(n, .)); forked
-    // before the Matsubara operator and its GEMM, which only the tv row reads
+    // side stream: retarded row, then les*adv = Ldense * badv (needs only G^R(n, .))
+    CK(cudaEventRecord(b->ev_fork, st));
+    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     {
         b->prof_mark(NESSI_KERNEL_RET, b->side);
         CKR((volterra_step<S, VIE>(b, g, gd, n, nact, true, b->side)));
@@ -883,7 +876,7 @@ int nessi_gpu_batch_create(nessi_batch **out, const nessi_problem_desc *desc, in
             pp == NESSI_VOLTERRA_GRID)
             b->volterra_pp = pp;
     }
-    if (const char *v = getenv("NESSI_TV_KERNEL")) b->tv_kernel = strcmp(v, "regs") == 0 ? 1 : 0;
+    if (const char *v = getenv("NESSI_TV_KERNEL")) b->tv_kernel = strcmp(v, "stream") == 0 ? 0 : 1;
     auto fail = [&](int r) { nessi_gpu_batch_destroy(b); return r; };
     if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess || b->nsm <= 0) {
         set_err("SM count query failed");
