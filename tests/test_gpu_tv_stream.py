@@ -1,5 +1,5 @@
 """The tv row's two kernels for size1 <= 4: k_tv_stream (history read into shared memory by bulk
-copies, the default) against k_tv (register loads; NESSI_TV_KERNEL=regs) on the same inputs, and
+copies; NESSI_TV_KERNEL=stream) against k_tv (register loads, the default) on the same inputs, and
 the bounded-wait path of the stream kernel.  The two kernels sum the same terms in a different
 order, so they agree to rounding: max|x - y| / max|y| < 1e-12 per component.  Parity of the default
 path with the oracle is in test_gpu_dyson.py / test_gpu_vie2.py / test_gpu_config_shapes.py."""
