@@ -5,22 +5,21 @@
 //   G^tv(n, tau) = Minv_les[n] Q(tau)
 // a_j = tvcoef (k_prep_group), Cmat = K_n Gmat_all (the Matsubara integral as one group GEMM).
 //
-// The history stream is the HBM-bound part of a time step.  It runs on the main stream while the
-// multi-problem Volterra kernels of the side stream hold one CTA of 512 threads on most SMs.  The
-// register-load form (k_tv: a thread per (tau, column), 4 rows in flight) keeps ~16 KB in flight
-// per SM and needs every SM to reach the HBM roofline.  Here a CTA of 160 threads keeps up to three
-// stages of <= 32 KB in flight, so one CTA per SM streams at the SM's share of the bandwidth, and
-// it fits beside a Volterra CTA (512 x 96 registers + 160 x <= 64 registers <= 65536).
+// The history stream is the HBM-bound part of a time step.  The register-load form (k_tv: a
+// thread per (tau, column), 4 rows in flight per thread) needs 64 warps per SM to keep enough bytes
+// in flight.  Here one persistent CTA per SM keeps up to five stages of ~32 KB in flight through
+// the bulk-copy engine, and 8 consumer warps reduce them.
 //
 // Work items are (problem, tau chunk of width tw); CTA b takes items b, b + G, b + 2G, ... and the
-// stages of all its items form one sequence through a ring of STAGES buffers.  A stage holds rows
-// r0 .. r0+nr-1 of an item's history, each row as s^2 segments (one per element plane e = b s + d
-// of the plane layout (t s^2 + e)(ntau+1) + tau) of tw complex: FP32 rows first (mixed precision,
-// j < n-k-1), then FP64 rows.  Lane 0 of warp 4 issues the copies.  An FP64 segment starts on a
+// stages of all its items form one sequence through a ring of STAGES buffers.  A stage holds the
+// coefficients a_j of rows r0 .. r0+nr-1 and those rows of the item's history, each row as s^2
+// segments (one per element plane e = b s + d of the plane layout (t s^2 + e)(ntau+1) + tau) of tw
+// complex: FP32 rows first (mixed precision, j < n-k-1), then FP64 rows.  Lane 0 of warp 8 issues
+// the copies.  An FP64 segment starts on a
 // 16-byte boundary; an FP32 segment may start 8 bytes past one, and then its copy starts 8 bytes
 // early and ends on the next boundary (the consumers index one element on).  The <= 8 bytes read
 // before and after a segment lie in the same problem's G^tv buffer: in the previous plane or row,
-// or in row n, which exists since n <= nt.  Warps 0-3 own (tau, d) pairs q = t + 128 i and
+// or in row n, which exists since n <= nt.  Warps 0-7 own (tau, d) pairs q = t + 256 i and
 // accumulate sum_b a_j[a][b] G^tv(j)[b][d](tau) in registers over the rows in order; the solve
 // with Minv_les[n] needs only the pair's own column, so there is no reduction.
 //
@@ -32,17 +31,17 @@
 #include "kernels_dyson.cuh"
 
 namespace tvs {
-constexpr int NCW = 4;                // consumer warps
+constexpr int NCW = 8;                // consumer warps
 constexpr int NCT = NCW * 32;         // consumer threads
 constexpr int NTH = NCT + 32;         // + the producer warp
-constexpr int STAGES = 4;             // ring buffers
-constexpr int STAGE_TARGET = 32768;   // bytes of one stage (at least one history row of an item)
+constexpr int STAGES = 6;             // ring buffers
+constexpr int SEG_TARGET = 32768;     // bytes of a stage's history segments (at least one row)
 constexpr int TIMEOUT_CODE = 5;       // NESSI_ERR_TIMEOUT
 }  // namespace tvs
 
-// (tau, d) pairs per consumer thread; the widest tau chunk is SLOTS * 128 / S
+// (tau, d) pairs per consumer thread; the widest tau chunk is SLOTS * 256 / S
 template <int S> struct TvsCfg {
-    static constexpr int SLOTS = S == 1 ? 8 : (S == 2 ? 4 : (S == 3 ? 3 : 2));
+    static constexpr int SLOTS = S == 1 ? 4 : (S <= 3 ? 2 : 1);
     static constexpr int TWMAX = SLOTS * tvs::NCT / S;
 };
 
@@ -53,7 +52,8 @@ struct TvsPlan {
     int items;           // nact * nch
     int r64, r32;        // history rows per stage, FP64 / FP32
     int slot64, slot32;  // bytes of one segment's slot in a stage (multiples of 16)
-    int stb;             // bytes of one stage (multiple of 16)
+    int coef;            // bytes of a stage's coefficient area (max(r64, r32) s^2 complex)
+    int stb;             // bytes of one stage: coef + segments (multiple of 16)
     long long wait_ns;   // bound of every mbarrier wait
     int *err;            // set to NESSI_ERR_TIMEOUT when a wait gave up
 };
@@ -154,16 +154,18 @@ __global__ void __maxnreg__(64) k_tv_stream(GroupDev g, const ProbDev *__restric
                 const bool f32 = si < ns32;
                 const int r0 = f32 ? si * pl.r32 : j64 + (si - ns32) * pl.r64;
                 const int nr = f32 ? min(pl.r32, j64 - r0) : min(pl.r64, n - r0);
-                const uint32_t fb = smem_u32(&bar_full[buf]), dst0 = sbase + (uint32_t)buf * (uint32_t)pl.stb;
+                const uint32_t fb = smem_u32(&bar_full[buf]), st0 = sbase + (uint32_t)buf * (uint32_t)pl.stb;
+                const uint32_t cbytes = (uint32_t)(nr * s2 * 16), dst0 = st0 + (uint32_t)pl.coef;
                 if (f32) {
                     const float2 *g32 = p->gtv32;
-                    uint32_t bytes = 0;
+                    uint32_t bytes = cbytes;
                     for (int r = 0; r < nr; r++)
                         for (int e = 0; e < s2; e++) {
                             const float2 *src = g32 + ((long)(r0 + r) * s2 + e) * M + tau0;
                             bytes += (uint32_t)(((tw + f32_off(src)) * 8 + 15) & ~15);
                         }
                     mbar_arrive_expect_tx(fb, bytes);
+                    bulk_g2s(st0, g.tvcoef + (long)r0 * s2, cbytes, fb);
                     for (int r = 0; r < nr; r++)
                         for (int e = 0; e < s2; e++) {
                             const float2 *src = g32 + ((long)(r0 + r) * s2 + e) * M + tau0;
@@ -173,7 +175,8 @@ __global__ void __maxnreg__(64) k_tv_stream(GroupDev g, const ProbDev *__restric
                         }
                 } else {
                     const double2 *g64 = p->gtv;
-                    mbar_arrive_expect_tx(fb, (uint32_t)(nr * s2 * tw * 16));
+                    mbar_arrive_expect_tx(fb, cbytes + (uint32_t)(nr * s2 * tw * 16));
+                    bulk_g2s(st0, g.tvcoef + (long)r0 * s2, cbytes, fb);
                     for (int r = 0; r < nr; r++)
                         for (int e = 0; e < s2; e++)
                             bulk_g2s(dst0 + (uint32_t)((r * s2 + e) * pl.slot64),
@@ -183,14 +186,34 @@ __global__ void __maxnreg__(64) k_tv_stream(GroupDev g, const ProbDev *__restric
             s_issued = i;
         }
     } else {
-        // ---- consumers: warps 0..3 ----
+        // ---- consumers: warps 0..7 ----
         const int t = threadIdx.x;
         long i = 0;
         for (int ii = 0; ii < nmine; ii++) {
             const int item = (int)blockIdx.x + ii * (int)gridDim.x;
             const ProbDev *p = probs + item / pl.nch;
             const int tau0 = (item % pl.nch) * pl.tw, tw = min(pl.tw, M - tau0), npair = tw * S;
-            const float2 *g32 = MIXED ? p->gtv32 : nullptr;
+            // the thread's pairs: plane offset d and tau offset tl, hoisted out of the row loops
+            int sd[SL], stl[SL];
+            bool sv[SL];
+#pragma unroll
+            for (int sl = 0; sl < SL; sl++) {
+                const int q = t + sl * NCT;
+                sv[sl] = q < npair;
+                sd[sl] = S == 1 ? 0 : q / tw;
+                stl[sl] = q - sd[sl] * tw;
+            }
+            // FP32 segments: parity of the first element's 8-byte offset at row 0, per (slot, b);
+            // row j adds j s^2 M (the planes of one row are M apart)
+            int par0[SL][S];
+            if (MIXED) {
+                const long base = (long)(((uintptr_t)p->gtv32 >> 3) & 1);
+#pragma unroll
+                for (int sl = 0; sl < SL; sl++)
+#pragma unroll
+                    for (int b = 0; b < S; b++) par0[sl][b] = (int)((base + (long)(b * S + sd[sl]) * M + tau0) & 1);
+            }
+            const int rowpar = (int)(rowe & 1);
             double2 acc[SL][S];
 #pragma unroll
             for (int sl = 0; sl < SL; sl++)
@@ -214,42 +237,30 @@ __global__ void __maxnreg__(64) k_tv_stream(GroupDev g, const ProbDev *__restric
                 const int r0 = f32 ? si * pl.r32 : j64 + (si - ns32) * pl.r64;
                 const int nr = f32 ? min(pl.r32, j64 - r0) : min(pl.r64, n - r0);
                 const unsigned char *stg = tsm + (long)buf * pl.stb;
+                const double2 *cst = (const double2 *)stg;
+                const unsigned char *seg0 = stg + pl.coef;
                 for (int r = 0; r < nr; r++) {
-                    const int j = r0 + r;
-                    const double2 *cj = g.tvcoef + (long)j * s2;
-                    // size1 <= 2: the row's coefficients in registers; larger: read from L1 per use
-                    constexpr int NC = S <= 2 ? s2 : 1;
-                    double2 c[NC];
-                    if constexpr (S <= 2) {
-#pragma unroll
-                        for (int ab = 0; ab < NC; ab++) c[ab] = __ldg(cj + ab);
-                    }
+                    const double2 *cj = cst + r * s2;  // a_j, broadcast from shared memory
+                    const int pj = MIXED ? (((r0 + r) & rowpar)) : 0;
 #pragma unroll
                     for (int sl = 0; sl < SL; sl++) {
-                        const int q = t + sl * NCT;
-                        if (q < npair) {
-                            const int d = S == 1 ? 0 : q / tw, tl = q - d * tw;
+                        if (sv[sl]) {
                             double2 x[S];
 #pragma unroll
                             for (int b = 0; b < S; b++) {
-                                const int seg = r * s2 + b * S + d;
+                                const int seg = r * s2 + b * S + sd[sl];
                                 if (MIXED && f32) {
-                                    const int off = f32_off(g32 + ((long)j * s2 + b * S + d) * M + tau0);
-                                    const float2 f = *(const float2 *)(stg + (long)seg * pl.slot32 + (off + tl) * 8);
+                                    const int off = par0[sl][b] ^ pj;
+                                    const float2 f = *(const float2 *)(seg0 + seg * pl.slot32 + (off + stl[sl]) * 8);
                                     x[b] = cmk((double)f.x, (double)f.y);
                                 } else {
-                                    x[b] = *(const double2 *)(stg + (long)seg * pl.slot64 + tl * 16);
+                                    x[b] = *(const double2 *)(seg0 + seg * pl.slot64 + stl[sl] * 16);
                                 }
                             }
 #pragma unroll
                             for (int a = 0; a < S; a++)
 #pragma unroll
-                                for (int b = 0; b < S; b++) {
-                                    double2 cab;
-                                    if constexpr (S <= 2) cab = c[a * S + b];
-                                    else cab = __ldg(cj + a * S + b);
-                                    acc[sl][a] = cfma(cab, x[b], acc[sl][a]);
-                                }
+                                for (int b = 0; b < S; b++) acc[sl][a] = cfma(cj[a * S + b], x[b], acc[sl][a]);
                         }
                     }
                 }
@@ -265,9 +276,8 @@ __global__ void __maxnreg__(64) k_tv_stream(GroupDev g, const ProbDev *__restric
             const int col = p->col;
 #pragma unroll
             for (int sl = 0; sl < SL; sl++) {
-                const int q = t + sl * NCT;
-                if (q < npair) {
-                    const int d = S == 1 ? 0 : q / tw, tau = tau0 + (q - d * tw);
+                if (sv[sl]) {
+                    const int d = sd[sl], tau = tau0 + stl[sl];
                     double2 v[S];
 #pragma unroll
                     for (int a = 0; a < S; a++) {

@@ -526,6 +526,7 @@ TvsPlan tv_stream_plan(int S, int M, int nact, int nsm, int twmax) {
     const int nch0 = (M + twmax - 1) / twmax;
     for (int nch = nch0; nch < nch0 + 16; nch++) {
         const int tw = (M + nch - 1) / nch, nchr = (M + tw - 1) / tw;
+        if (nch > 1 && tw < 32) break;  // segments of at least 512 bytes
         const long items = (long)nact * nchr, grid = std::min<long>(items, nsm);
         const double cost = (double)((items + grid - 1) / grid) * (tw + 16);
         if (cost < best - 1e-9) {
@@ -538,9 +539,16 @@ TvsPlan tv_stream_plan(int S, int M, int nact, int nsm, int twmax) {
     const int s2 = S * S;
     pl.slot64 = pl.tw * 16;
     pl.slot32 = ((pl.tw + 2) * 8 + 15) & ~15;
-    pl.r64 = std::max(1, tvs::STAGE_TARGET / (s2 * pl.slot64));
-    pl.stb = std::max(pl.r64 * s2 * pl.slot64, s2 * pl.slot32);
-    pl.r32 = pl.stb / (s2 * pl.slot32);
+    pl.r64 = std::min(64, std::max(1, tvs::SEG_TARGET / (s2 * pl.slot64)));
+    pl.r32 = std::min(64, std::max(1, tvs::SEG_TARGET / (s2 * pl.slot32)));
+    for (;;) {  // the ring within 216 KB of shared memory
+        pl.coef = std::max(pl.r64, pl.r32) * s2 * 16;
+        pl.stb = pl.coef + std::max(pl.r64 * s2 * pl.slot64, pl.r32 * s2 * pl.slot32);
+        if (tvs::STAGES * pl.stb <= 216 * 1024 || (pl.r64 == 1 && pl.r32 == 1)) break;
+        if (pl.r32 * pl.slot32 >= pl.r64 * pl.slot64 && pl.r32 > 1) pl.r32--;
+        else if (pl.r64 > 1) pl.r64--;
+        else pl.r32--;
+    }
     return pl;
 }
 
@@ -550,14 +558,8 @@ int tv_stream_launch(nessi_batch *b, const GroupDev &gd, const Group &g, int n, 
     pl.wait_ns = b->wait_ns;
     pl.err = b->d_err;
     const size_t sm = (size_t)tvs::STAGES * pl.stb;
-    static bool attr_set[64] = {false};  // per device
-    if (!attr_set[b->device & 63]) {
-        CK(cudaFuncSetAttribute(k_tv_stream<S, MIXED, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tvs::STAGES * tvs::STAGE_TARGET));
-        CK(cudaFuncSetAttribute(k_tv_stream<S, MIXED, VIE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                cudaSharedmemCarveoutMaxShared));
-        attr_set[b->device & 63] = true;
-    }
+    if (sm > 220 * 1024) { set_err("k_tv_stream: %zu bytes of shared memory", sm); return NESSI_ERR_ARG; }
+    CK(cudaFuncSetAttribute(k_tv_stream<S, MIXED, VIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = std::min(pl.items, b->nsm);
     k_tv_stream<S, MIXED, VIE><<<grid, tvs::NTH, sm, st>>>(gd, g.d_probs, n, pl);
     CK(cudaGetLastError());
