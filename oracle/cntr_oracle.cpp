@@ -1066,13 +1066,14 @@ void dyson_mat_fourier_t(HM &G, HM &Sigma, double mu, const cplx *H0, double bet
 // ------------------------------------------------------------------------------------
 // Dyson (cntr_dyson_impl.hpp)
 // ------------------------------------------------------------------------------------
-// dyson_timestep_ret (:80-222)
+// Time step n of G^R: row n zeroed, G^R(n,n) = -i, and the start values G^R(n, n-j), j = 1..k,
+// from the k x k block system of the conjugate equation (cntr_dyson_impl.hpp:98-170; the
+// OpenMP variant repeats it, cntr_dyson_omp_impl.hpp:55-129).
 template <int S1>
-void dyson_timestep_ret_t(int n, HM &G, double mu, const cplx *H, HM &Sigma, const Integ &In, double h) {
+void ret_start_block_t(int n, HM &G, double mu, const cplx *H, HM &Sigma, const Integ &In, double h) {
     El<S1> E(G.s);
-    int k = In.k, k1 = k + 1, k2 = 2 * k1, es = E.es, ss = Sigma.es;
-    std::vector<cplx> gtemp((long)k * es), diffw(k1 + 1), qq((long)(n + 1) * es), one(es),
-        mm((long)k * k * es), hj(es), stemp(es);
+    int k = In.k, es = E.es;
+    std::vector<cplx> gtemp((long)k * es), qq((long)k * es), one(es), mm((long)k * k * es), stemp(es);
     E.set_diag(one.data(), 1.0);
     for (long i = 0; i < (long)(n + 1) * es; i++) G.retptr(n, 0)[i] = 0;
     E.set_diag(G.retptr(n, n), -kI);
@@ -1105,6 +1106,16 @@ void dyson_timestep_ret_t(int n, HM &G, double mu, const cplx *H, HM &Sigma, con
     }
     E.linsolve_left(k, gtemp.data(), mm.data(), qq.data());
     for (int j = 1; j <= k; j++) E.set(G.retptr(n, n - j), gtemp.data() + (long)(j - 1) * es);
+}
+
+// dyson_timestep_ret (:80-222)
+template <int S1>
+void dyson_timestep_ret_t(int n, HM &G, double mu, const cplx *H, HM &Sigma, const Integ &In, double h) {
+    El<S1> E(G.s);
+    int k = In.k, k1 = k + 1, k2 = 2 * k1, es = E.es, ss = Sigma.es;
+    std::vector<cplx> diffw(k1 + 1), qq((long)(n + 1) * es), one(es), mm((long)k * k * es), hj(es), stemp(es);
+    E.set_diag(one.data(), 1.0);
+    ret_start_block_t<S1>(n, G, mu, H, Sigma, In, h);
     for (long i = 0; i < (long)(n + 1) * es; i++) qq[i] = 0;
     for (int m = n - k; m <= n; m++) {
         const cplx *gret = G.retptr(n, m);
@@ -1559,6 +1570,346 @@ template <int S1> void extrapolate_t(int n, HM &G, const Integ &In) {
     }
 }
 
+// ------------------------------------------------------------------------------------
+// incr_convolution (cntr_convolution_impl.hpp:4164-4810): C += alpha [A * ft * B] at time
+// step tstp, output element by output element, for the elements whose mask entry is set (the
+// OpenMP solvers split the masks over threads).  ft points to F(0) of function data (F(t) at
+// ft + t s^2) or is null; f0 = F(-1).  Run here in one thread's order.
+// ------------------------------------------------------------------------------------
+// incr_convolution_mat (:4164-4200)
+template <int S1>
+void incr_conv_mat_t(const char *mask, cplx alpha, HM &C, HM &A, const cplx *f0, HM &B, const Integ &In,
+                     double beta) {
+    El<S1> E(C.s);
+    int ntau = A.ntau(), es = C.es;
+    cplx adtau = alpha * beta * (1.0 / ntau);
+    std::vector<cplx> ctemp(es), bmat1;
+    const cplx *bm = B.matptr(0);
+    if (f0) {
+        bmat1.resize((long)(ntau + 1) * es);
+        for (int m = 0; m <= ntau; m++) E.mult(bmat1.data() + (long)m * es, f0, B.matptr(m));
+        bm = bmat1.data();
+    }
+    for (int m = 0; m <= ntau; m++) {
+        if (!mask[m]) continue;
+        matsubara_integral_1<S1>(E, m, ntau, ctemp.data(), A.matptr(0), bm, In, A.sig());
+        E.incr(C.matptr(m), adtau, ctemp.data());
+    }
+}
+
+// aret[j] = A^R(tstp, j) F(j), j = 0..n1, with A^R(tstp, j) = -Acc^R(j, tstp)^dagger for j > tstp
+// (:4265-4297, 4417-4445)
+template <int S1>
+std::vector<cplx> incr_aret(const El<S1> &E, int tstp, int n1, HM &A, HM &Acc, const cplx *ft) {
+    int es = E.es;
+    std::vector<cplx> aret((long)(n1 + 1) * es), at(es);
+    for (int j = 0; j <= n1; j++) {
+        if (j <= tstp) E.set(at.data(), A.retptr(tstp, j));
+        else E.minusconj(at.data(), Acc.retptr(j, tstp));
+        if (ft) E.mult(aret.data() + (long)j * es, at.data(), ft + (long)j * es);
+        else E.set(aret.data() + (long)j * es, at.data());
+    }
+    return aret;
+}
+
+// incr_convolution_ret (:4243-4360): C^R(tstp, n) += alpha h int_n^tstp A^R(tstp, j) F(j) B^R(j, n)
+template <int S1>
+void incr_conv_ret_t(int tstp, const char *mask, cplx alpha, HM &C, HM &A, HM &Acc, const cplx *ft, HM &B,
+                     HM &Bcc, const Integ &In, double h) {
+    El<S1> E(C.s);
+    int es = C.es, k = In.k, n1 = tstp >= k ? tstp : k;
+    cplx adt = alpha * h;
+    std::vector<cplx> aret = incr_aret<S1>(E, tstp, n1, A, Acc, ft), ct(es), bt(es);
+    auto ar = [&](int j) { return aret.data() + (long)j * es; };
+    for (int n = 0; n <= tstp; n++) {
+        if (!mask[n]) continue;
+        int n2 = tstp - n;
+        // B^R(j, n), continued by -Bcc^R(n, j)^dagger for j < n
+        auto bx = [&](int j) -> const cplx * {
+            if (j >= n) return B.retptr(j, n);
+            E.minusconj(bt.data(), Bcc.retptr(n, j));
+            return bt.data();
+        };
+        E.zero(ct.data());
+        if (tstp < k) {
+            for (int j = 0; j <= k; j++) E.incr(ct.data(), In.poly_integration(n, tstp, j), ar(j), bx(j));
+        } else if (n2 < k) {
+            for (int l = 0; l <= k; l++) E.incr(ct.data(), In.gregory_weights(n2, l), ar(tstp - l), bx(tstp - l));
+        } else if (n2 <= 2 * k + 2) {
+            for (int l = 0; l <= n2; l++) E.incr(ct.data(), In.gregory_weights(n2, l), ar(n + l), B.retptr(n + l, n));
+        } else {
+            for (int j = n; j <= n + k; j++) E.incr(ct.data(), In.gregory_omega(j - n), ar(j), B.retptr(j, n));
+            for (int j = n + k + 1; j < tstp - k; j++) E.incr(ct.data(), ar(j), B.retptr(j, n));
+            for (int l = 0; l <= k; l++) E.incr(ct.data(), In.gregory_omega(l), ar(tstp - l), B.retptr(tstp - l, n));
+        }
+        E.incr(C.retptr(tstp, n), adt, ct.data());
+    }
+}
+
+// incr_convolution_tv (:4396-4500): C^tv(tstp, m) += alpha [ dtau int A^tv(tstp, .) f0 B^mat
+//   + h sum_j w(tstp, j) A^R(tstp, j) F(j) B^tv(j, m) ]
+template <int S1>
+void incr_conv_tv_t(int tstp, const char *mask, cplx alpha, HM &C, HM &A, HM &Acc, const cplx *f0,
+                    const cplx *ft, HM &B, HM &Bcc, const Integ &In, double beta, double h) {
+    El<S1> E(C.s);
+    int es = C.es, k = In.k, ntau = A.ntau(), n1 = tstp >= k ? tstp : k;
+    cplx adt = alpha * h, adtau = alpha * beta * (1.0 / ntau);
+    std::vector<cplx> aret = incr_aret<S1>(E, tstp, n1, A, Acc, ft), bmat1, c1(es), c2(es);
+    const cplx *bm = B.matptr(0);
+    if (f0) {
+        bmat1.resize((long)(ntau + 1) * es);
+        for (int m = 0; m <= ntau; m++) E.mult(bmat1.data() + (long)m * es, f0, B.matptr(m));
+        bm = bmat1.data();
+    }
+    auto ar = [&](int j) { return aret.data() + (long)j * es; };
+    for (int m = 0; m <= ntau; m++) {
+        if (!mask[m]) continue;
+        matsubara_integral_2<S1>(E, m, ntau, c1.data(), A.tvptr(tstp, 0), bm, In, B.sig());
+        E.smul(c1.data(), adtau);
+        E.zero(c2.data());
+        if (tstp <= 2 * k + 2) {
+            for (int n = 0; n <= n1; n++) E.incr(c2.data(), In.gregory_weights(tstp, n), ar(n), B.tvptr(n, m));
+        } else {
+            for (int n = 0; n <= k; n++) E.incr(c2.data(), In.gregory_omega(n), ar(n), B.tvptr(n, m));
+            for (int n = k + 1; n < tstp - k; n++) E.incr(c2.data(), ar(n), B.tvptr(n, m));
+            for (int n = tstp - k; n <= tstp; n++) E.incr(c2.data(), In.gregory_omega(tstp - n), ar(n), B.tvptr(n, m));
+        }
+        E.smul(c2.data(), adt);
+        E.incr(C.tvptr(tstp, m), c1.data());
+        E.incr(C.tvptr(tstp, m), c2.data());
+    }
+}
+
+// incr_convolution_les (:4539-4760): C^<(n, tstp) += alpha [ h A^R * F B^< + h A^< * F B^A
+//   - i dtau A^tv * f0 B^vt ](n, tstp); the tau integral always uses the end-corrected
+//   (omega) weights.
+template <int S1>
+void incr_conv_les_t(int tstp, const char *mask, cplx alpha, HM &C, HM &A, HM &Acc, const cplx *f0,
+                     const cplx *ft, HM &B, HM &Bcc, const Integ &In, double beta, double h) {
+    El<S1> E(C.s);
+    int es = C.es, k = In.k, ntau = A.ntau(), n1 = tstp >= k ? tstp : k;
+    cplx adt = alpha * h, adtau = alpha * beta * (1.0 / ntau);
+    std::vector<cplx> badv((long)(n1 + 1) * es), bles((long)(n1 + 1) * es), bvt((long)(ntau + 1) * es), bt(es),
+        at(es), c1(es), c2(es), c3(es);
+    auto lmul = [&](cplx *z, const cplx *f, const cplx *x) {  // z = f x (f may be null)
+        if (f) E.mult(z, f, x); else E.set(z, x);
+    };
+    for (int j = 0; j <= n1; j++) {
+        const cplx *fj = ft ? ft + (long)j * es : nullptr;
+        if (j <= tstp) {
+            E.conj(bt.data(), Bcc.retptr(tstp, j));
+            lmul(badv.data() + (long)j * es, fj, bt.data());
+            lmul(bles.data() + (long)j * es, fj, B.lesptr(j, tstp));
+        } else {
+            lmul(badv.data() + (long)j * es, fj, B.retptr(j, tstp));
+            E.smul(badv.data() + (long)j * es, -1.0);
+            E.minusconj(bt.data(), Bcc.lesptr(tstp, j));
+            lmul(bles.data() + (long)j * es, fj, bt.data());
+        }
+    }
+    for (int m = 0; m <= ntau; m++) {
+        if (B.sig() == -1) E.conj(bt.data(), Bcc.tvptr(tstp, ntau - m));
+        else E.minusconj(bt.data(), Bcc.tvptr(tstp, ntau - m));
+        lmul(bvt.data() + (long)m * es, f0, bt.data());
+    }
+    auto bl = [&](int j) { return bles.data() + (long)j * es; };
+    auto ba = [&](int j) { return badv.data() + (long)j * es; };
+    auto bv = [&](int m) { return bvt.data() + (long)m * es; };
+    for (int n = 0; n <= tstp; n++) {
+        if (!mask[n]) continue;
+        // A^<(n, j), continued by -Acc^<(j, n)^dagger (j < n)
+        auto lx = [&](int j) -> const cplx * {
+            if (j < n) { E.minusconj(at.data(), Acc.lesptr(j, n)); return at.data(); }
+            return A.lesptr(n, j);
+        };
+        int nup = n > k ? n : k;
+        E.zero(c1.data());
+        if (n <= 2 * k + 2) {
+            for (int j = 0; j <= nup; j++) {
+                if (j <= n) E.incr(c1.data(), In.gregory_weights(n, j), A.retptr(n, j), bl(j));
+                else {
+                    E.minusconj(at.data(), Acc.retptr(j, n));
+                    E.incr(c1.data(), In.gregory_weights(n, j), at.data(), bl(j));
+                }
+            }
+        } else {
+            for (int j = 0; j <= k; j++) E.incr(c1.data(), In.gregory_omega(j), A.retptr(n, j), bl(j));
+            for (int j = k + 1; j < n - k; j++) E.incr(c1.data(), A.retptr(n, j), bl(j));
+            for (int j = n - k; j <= n; j++) E.incr(c1.data(), In.gregory_omega(n - j), A.retptr(n, j), bl(j));
+        }
+        E.zero(c2.data());
+        for (int m = 0; m <= k; m++) E.incr(c2.data(), In.gregory_omega(m), A.tvptr(n, m), bv(m));
+        for (int m = k + 1; m < ntau - k; m++) E.incr(c2.data(), A.tvptr(n, m), bv(m));
+        for (int m = ntau - k; m <= ntau; m++) E.incr(c2.data(), In.gregory_omega(ntau - m), A.tvptr(n, m), bv(m));
+        E.zero(c3.data());
+        if (tstp <= 2 * k + 2) {
+            for (int j = 0; j <= n; j++) {
+                E.minusconj(at.data(), Acc.lesptr(j, n));
+                E.incr(c3.data(), In.gregory_weights(tstp, j), at.data(), ba(j));
+            }
+            for (int j = n + 1; j <= n1; j++) E.incr(c3.data(), In.gregory_weights(tstp, j), A.lesptr(n, j), ba(j));
+        } else {
+            for (int j = 0; j <= k; j++) E.incr(c3.data(), In.gregory_omega(j), lx(j), ba(j));
+            for (int j = k + 1; j < tstp - k; j++) E.incr(c3.data(), lx(j), ba(j));
+            for (int j = tstp - k; j <= tstp; j++) E.incr(c3.data(), In.gregory_omega(tstp - j), lx(j), ba(j));
+        }
+        E.incr(C.lesptr(n, tstp), adt, c1.data());
+        E.incr(C.lesptr(n, tstp), adt, c3.data());
+        E.incr(C.lesptr(n, tstp), adtau * cplx(0.0, -1.0), c2.data());
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// dyson_timestep_omp (cntr_dyson_omp_impl.hpp:37-611): G^R(n, j) and G^<(j, n) for
+// j < n - k from the equation in the other time argument, every j independent (the
+// OpenMP loop), with BD(k+1) derivatives; G^tv as the serial step, with the masked
+// convolution.  In one thread's order: every convolution of a component is complete
+// before its solves.
+// ------------------------------------------------------------------------------------
+// dyson_timestep_ret_omp (:37-176)
+template <int S1>
+void dyson_timestep_ret_omp_t(int n, HM &G, double mu, const cplx *H, HM &Sigma, const Integ &In, double h) {
+    El<S1> E(G.s);
+    int k = In.k, k1 = k + 1, es = E.es;
+    ret_start_block_t<S1>(n, G, mu, H, Sigma, In, h);
+    std::vector<char> mask(n + 1, 0);
+    for (int i = 0; i < n - k; i++) mask[i] = 1;
+    incr_conv_ret_t<S1>(n, mask.data(), 1.0, G, Sigma, Sigma, nullptr, G, G, In, h);
+    std::vector<cplx> diffw(k1 + 1), qq(es), mm(es);
+    for (int p = 0; p <= k1; p++) diffw[p] = In.bd_weights(p) * kI / h;
+    cplx w0 = h * In.gregory_omega(0);
+    for (int j = 0; j < n - k; j++) {
+        E.set(qq.data(), G.retptr(n, j));
+        for (int p = 1; p <= k1; p++) E.incr(qq.data(), -diffw[p], G.retptr(n - p, j));
+        E.set_diag(mm.data(), diffw[0] + mu);
+        E.incr(mm.data(), -w0, Sigma.retptr(j, j));
+        E.incr(mm.data(), -1.0, H + (long)n * es);
+        E.linsolve_right(1, G.retptr(n, j), mm.data(), qq.data());
+    }
+}
+
+// dyson_timestep_tv_omp (:179-235)
+template <int S1>
+void dyson_timestep_tv_omp_t(int n, HM &G, double mu, const cplx *Hn, HM &Sigma, const Integ &In, double beta,
+                             double h) {
+    El<S1> E(G.s);
+    int k = In.k, k1 = k + 1, es = E.es, ntau = G.ntau();
+    cplx ih(0, 1.0 / h);
+    for (int m = 0; m <= ntau; m++) E.zero(G.tvptr(n, m));
+    std::vector<char> mask(ntau + 1, 1);
+    incr_conv_tv_t<S1>(n, mask.data(), 1.0, G, Sigma, Sigma, nullptr, nullptr, G, G, In, beta, h);
+    std::vector<cplx> diffw(k1 + 1), qq(es), mm(es);
+    E.set_diag(mm.data(), ih * In.bd_weights(0) + mu);
+    E.incr(mm.data(), -1.0, Hn);
+    E.incr(mm.data(), -h * In.gregory_weights(n, 0), Sigma.retptr(n, n));
+    for (int p = 0; p <= k1; p++) diffw[p] = ih * In.bd_weights(p);
+    for (int m = 0; m <= ntau; m++) {
+        E.set(qq.data(), G.tvptr(n, m));
+        for (int p = 1; p <= k1; p++) E.incr(qq.data(), -diffw[p], G.tvptr(n - p, m));
+        E.linsolve_right(1, G.tvptr(n, m), mm.data(), qq.data());
+    }
+}
+
+// dyson_timestep_les_omp (:298-414); the serial step for n < 2k+1
+template <int S1>
+void dyson_timestep_les_omp_t(int n, HM &G, double mu, const cplx *H, HM &Sigma, const Integ &In, double beta,
+                              double h) {
+    int k = In.k, k1 = k + 1;
+    if (n < 2 * k + 1) { dyson_timestep_les_t<S1>(n, G, mu, H, Sigma, In, beta, h); return; }
+    El<S1> E(G.s);
+    int es = E.es;
+    for (int j = 0; j <= n; j++) E.zero(G.lesptr(j, n));
+    std::vector<char> mask(n + 1, 0);
+    for (int i = 0; i < n - k; i++) mask[i] = 1;
+    // G^<(j, n) from the conjugate equation: [G * Sigma]^<(j, n) into G
+    incr_conv_les_t<S1>(n, mask.data(), 1.0, G, G, G, nullptr, nullptr, Sigma, Sigma, In, beta, h);
+    std::vector<cplx> diffw(k1 + 1), qq(es), mm(es), stemp(es);
+    for (int p = 0; p <= k1; p++) diffw[p] = In.bd_weights(p) * kI / h;
+    cplx w0 = h * In.gregory_omega(0);
+    for (int j = 0; j < n - k; j++) {
+        E.set(qq.data(), G.lesptr(j, n));
+        for (int p = 1; p <= k1; p++) E.incr(qq.data(), diffw[p], G.lesptr(j, n - p));
+        E.set_diag(mm.data(), -diffw[0] + mu);
+        E.conj(stemp.data(), Sigma.retptr(j, j));
+        E.incr(mm.data(), -w0, stemp.data());
+        E.incr(mm.data(), -1.0, H + (long)n * es);
+        E.linsolve_left(1, G.lesptr(j, n), mm.data(), qq.data());
+    }
+    // G^<(j, n), j = n-k..n, from the equation in the first argument (:370-410)
+    std::vector<cplx> gles((long)(n + 1) * es, 0.0);
+    conv_les_tvvt<S1>(n, n - k, n, gles.data(), G, Sigma, Sigma, G, G, In, beta, h);
+    conv_les_lesadv<S1>(n, n - k, n, gles.data(), G, Sigma, Sigma, G, G, In, beta, h);
+    for (int j = n - k; j <= n; j++) {
+        E.set(qq.data(), gles.data() + (long)j * es);
+        for (int p = 1; p <= k1; p++) E.incr(qq.data(), -kI / h * In.bd_weights(p), G.lesptr(j - p, n));
+        E.set_diag(mm.data(), kI / h * In.bd_weights(0) + mu);
+        E.incr(mm.data(), -1.0, H + (long)j * es);
+        E.incr(mm.data(), -h * In.gregory_weights(j, j), Sigma.retptr(j, j));
+        for (int m = 0; m < j; m++) E.incr(qq.data(), h * In.gregory_weights(j, m), Sigma.retptr(j, m), G.lesptr(m, n));
+        E.linsolve_right(1, G.lesptr(j, n), mm.data(), qq.data());
+    }
+}
+
+// vie2_timestep_omp_dispatch (cntr_vie2_impl.hpp:1851-1980) for tstp > k: [1 + F] G = Q with
+// every element of the time step independent.  G^R(tstp, .), G^tv(tstp, .) and G^<(. , tstp)
+// enter their own convolutions as zero; G^<(tstp, tstp) last.  Q is left unchanged (the
+// reference restores it).
+template <int S1>
+void vie2_timestep_omp_t(int tstp, HM &G, HM &F, HM &Fcc, HM &Q, const Integ &In, double beta, double h) {
+    El<S1> E(G.s);
+    int es = E.es, kt = In.k, ntau = G.ntau();
+    std::vector<cplx> qret((long)(tstp + 1) * es), qtv((long)(ntau + 1) * es), qles((long)(tstp + 1) * es);
+    for (int n = 0; n <= tstp; n++) {
+        E.set(qret.data() + (long)n * es, Q.retptr(tstp, n));
+        E.set(qles.data() + (long)n * es, Q.lesptr(n, tstp));
+    }
+    for (int m = 0; m <= ntau; m++) E.set(qtv.data() + (long)m * es, Q.tvptr(tstp, m));
+    for (int n = 0; n <= tstp; n++) { E.zero(G.retptr(tstp, n)); E.zero(G.lesptr(n, tstp)); }
+    for (int m = 0; m <= ntau; m++) E.zero(G.tvptr(tstp, m));
+    std::vector<cplx> mtemp(es), one(es), mm(es);
+    E.set(mtemp.data(), F.retptr(tstp, tstp));
+    E.smul(mtemp.data(), h);
+    E.set_diag(one.data(), 1.0);
+    std::vector<char> all_ret(tstp + 1, 1), all_tv(ntau + 1, 1), les_mask(tstp + 1, 1);
+    les_mask[tstp] = 0;
+    // retarded: Q1 = Q - F * G with G^R(tstp, .) = 0
+    incr_conv_ret_t<S1>(tstp, all_ret.data(), -1.0, Q, F, Fcc, nullptr, G, G, In, h);
+    for (int n = 0; n <= tstp; n++) {
+        double wt = tstp < kt ? In.poly_integration(n, tstp, tstp) : In.gregory_weights(tstp - n, 0);
+        E.set(mm.data(), one.data());
+        E.incr(mm.data(), wt, mtemp.data());
+        E.linsolve_right(1, G.retptr(tstp, n), mm.data(), Q.retptr(tstp, n));
+    }
+    // left-mixing
+    incr_conv_tv_t<S1>(tstp, all_tv.data(), -1.0, Q, F, Fcc, nullptr, nullptr, G, G, In, beta, h);
+    for (int m = 0; m <= ntau; m++) {
+        E.set(mm.data(), one.data());
+        E.incr(mm.data(), In.gregory_weights(tstp, tstp), mtemp.data());
+        E.linsolve_right(1, G.tvptr(tstp, m), mm.data(), Q.tvptr(tstp, m));
+    }
+    // lesser, n < tstp: Q1 = Q - G * Fcc with G^<(., tstp) = 0
+    incr_conv_les_t<S1>(tstp, les_mask.data(), -1.0, Q, G, G, nullptr, nullptr, Fcc, F, In, beta, h);
+    for (int n = 0; n < tstp; n++) {
+        E.set(mm.data(), one.data());
+        E.incr(mm.data(), In.gregory_weights(tstp, tstp), mtemp.data());
+        E.conj_inplace(mm.data());
+        E.linsolve_left(1, G.lesptr(n, tstp), mm.data(), Q.lesptr(n, tstp));
+    }
+    // G^<(tstp, tstp), which reads this step's G^R, G^tv and G^<(n < tstp, tstp)
+    std::vector<char> last(tstp + 1, 0);
+    last[tstp] = 1;
+    incr_conv_les_t<S1>(tstp, last.data(), -1.0, Q, G, G, nullptr, nullptr, Fcc, F, In, beta, h);
+    E.set(mm.data(), one.data());
+    E.incr(mm.data(), In.gregory_weights(tstp, tstp), mtemp.data());
+    E.conj_inplace(mm.data());
+    E.linsolve_left(1, G.lesptr(tstp, tstp), mm.data(), Q.lesptr(tstp, tstp));
+    for (int n = 0; n <= tstp; n++) {
+        E.set(Q.retptr(tstp, n), qret.data() + (long)n * es);
+        E.set(Q.lesptr(n, tstp), qles.data() + (long)n * es);
+    }
+    for (int m = 0; m <= ntau; m++) E.set(Q.tvptr(tstp, m), qtv.data() + (long)m * es);
+}
+
 #define ORC_DISPATCH(fn, ...) do { if (s1 == 1) fn<1>(__VA_ARGS__); else fn<0>(__VA_ARGS__); } while (0)
 
 }  // namespace
@@ -1774,6 +2125,59 @@ void orc_vie2_timestep_sin(int n, orc_hm *Gh, cplx *Gsin, orc_hm *Fh, orc_hm *Fc
         for (long i = 0; i < (long)(t + 1) * es; i++) q.lesptr(0, t)[i] -= f1.lesptr(0, t)[i];
     }
     orc_vie2_timestep(n, Gh, &tF, &tFcc, &tQ, k, beta, h, 2);
+}
+
+// One component of incr_convolution (cntr_convolution_impl.hpp:4164-4760): which = 0 mat,
+// 1 ret, 2 tv, 3 les; mask has ntau+1 (mat, tv) or tstp+1 (ret, les) entries (null: all set);
+// ftdata = function data with F(-1) first, or null.
+void orc_incr_convolution_part(int which, int tstp, const char *mask, double are, double aim, orc_hm *Ch,
+                               orc_hm *Ah, orc_hm *Acch, const cplx *ftdata, orc_hm *Bh, orc_hm *Bcch, int k,
+                               double beta, double h) {
+    HM C(Ch), A(Ah), Acc(Acch), B(Bh), Bcc(Bcch);
+    int s1 = C.s;
+    cplx alpha(are, aim);
+    const cplx *f0 = ftdata, *ft = ftdata ? ftdata + C.es : nullptr;
+    std::vector<char> all((which == 0 || which == 2 ? C.ntau() : tstp) + 1, 1);
+    const char *mk = mask ? mask : all.data();
+    const Integ &In = I(k);
+    if (which == 0) ORC_DISPATCH(incr_conv_mat_t, mk, alpha, C, A, f0, B, In, beta);
+    else if (which == 1) ORC_DISPATCH(incr_conv_ret_t, tstp, mk, alpha, C, A, Acc, ft, B, Bcc, In, h);
+    else if (which == 2) ORC_DISPATCH(incr_conv_tv_t, tstp, mk, alpha, C, A, Acc, f0, ft, B, Bcc, In, beta, h);
+    else ORC_DISPATCH(incr_conv_les_t, tstp, mk, alpha, C, A, Acc, f0, ft, B, Bcc, In, beta, h);
+}
+
+// incr_convolution (:4786-4807): every element of time step tstp (tstp = -1: Matsubara)
+void orc_incr_convolution(int tstp, double are, double aim, orc_hm *C, orc_hm *A, orc_hm *Acc, const cplx *ftdata,
+                          orc_hm *B, orc_hm *Bcc, int k, double beta, double h) {
+    if (tstp == -1) {
+        orc_incr_convolution_part(0, tstp, nullptr, are, aim, C, A, Acc, ftdata, B, Bcc, k, beta, h);
+    } else if (tstp >= 0) {
+        for (int which = 1; which <= 3; which++)
+            orc_incr_convolution_part(which, tstp, nullptr, are, aim, C, A, Acc, ftdata, B, Bcc, k, beta, h);
+    }
+}
+
+// dyson_timestep_omp (cntr_dyson_omp_impl.hpp:577-605); k + 1 <= n
+void orc_dyson_timestep_omp(int n, orc_hm *Gh, double mu, const cplx *H, orc_hm *Sh, int k, double beta,
+                            double h) {
+    HM G(Gh), S(Sh);
+    int s1 = G.s;
+    const cplx *H0 = H + G.es;
+    const Integ &In = I(k);
+    ORC_DISPATCH(dyson_timestep_ret_omp_t, n, G, mu, H0, S, In, h);
+    ORC_DISPATCH(dyson_timestep_tv_omp_t, n, G, mu, H0 + (long)n * G.es, S, In, beta, h);
+    ORC_DISPATCH(dyson_timestep_les_omp_t, n, G, mu, H0, S, In, beta, h);
+}
+
+// vie2_timestep_omp (cntr_vie2_impl.hpp:2125-2190): tstp = -1 vie2_mat, tstp <= k vie2_start of
+// order tstp, else the element-parallel step
+void orc_vie2_timestep_omp(int tstp, orc_hm *Gh, orc_hm *Fh, orc_hm *Fcch, orc_hm *Qh, int k, double beta, double h,
+                           int method) {
+    if (tstp == -1) { orc_vie2_mat(Gh, Fh, Fcch, Qh, beta, k, method); return; }
+    if (tstp <= k) { orc_vie2_start(Gh, Fh, Fcch, Qh, tstp, beta, h); return; }
+    HM G(Gh), F(Fh), Fcc(Fcch), Q(Qh);
+    int s1 = G.s;
+    ORC_DISPATCH(vie2_timestep_omp_t, tstp, G, F, Fcc, Q, I(k), beta, h);
 }
 
 void orc_extrapolate_timestep(int n, orc_hm *Gh, int k) {

@@ -71,6 +71,21 @@ void orc_vie2_timestep(int n, orc_hm *G, orc_hm *F, orc_hm *Fcc, orc_hm *Q, int 
 void orc_vie2_timestep_sin(int n, orc_hm *G, ocplx *Gsin, orc_hm *F, orc_hm *Fcc, const ocplx *Fsin, orc_hm *Q,
                            const ocplx *Qsin, int k, double beta, double h);
 
+// incr_convolution (cntr_convolution_impl.hpp:4164-4807): C += alpha A * F * B at time step tstp.
+// which = 0 mat, 1 ret, 2 tv, 3 les; mask (ntau+1 or tstp+1 entries) null = all; ftdata =
+// function data with F(-1) first, or null.
+void orc_incr_convolution_part(int which, int tstp, const char *mask, double are, double aim, orc_hm *C,
+                               orc_hm *A, orc_hm *Acc, const ocplx *ftdata, orc_hm *B, orc_hm *Bcc, int k,
+                               double beta, double h);
+void orc_incr_convolution(int tstp, double are, double aim, orc_hm *C, orc_hm *A, orc_hm *Acc, const ocplx *ftdata,
+                          orc_hm *B, orc_hm *Bcc, int k, double beta, double h);
+// The OpenMP solvers' discretization (cntr_dyson_omp_impl.hpp:37-605, cntr_vie2_impl.hpp:1851-2190),
+// run in one thread's order.
+void orc_dyson_timestep_omp(int n, orc_hm *G, double mu, const ocplx *H, orc_hm *Sigma, int k, double beta,
+                            double h);
+void orc_vie2_timestep_omp(int tstp, orc_hm *G, orc_hm *F, orc_hm *Fcc, orc_hm *Q, int k, double beta, double h,
+                           int method);
+
 // Utilities (cntr_utilities_impl.hpp:22-170, 607-650, 2077-2110).
 void orc_extrapolate_timestep(int n, orc_hm *G, int k);
 double orc_distance_norm2(int tstp, orc_hm *g1, orc_hm *g2);

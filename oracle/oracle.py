@@ -73,6 +73,10 @@ def lib():
             "orc_lattice2b_start": (i, [i, P, P, P, vp, d, vp, ctypes.c_long, i, d, d, i, d,
                                         ctypes.POINTER(ctypes.c_double), i]),
             "orc_lattice2b_timestep": (None, [i, i, P, P, P, vp, d, vp, ctypes.c_long, i, d, d, i, i]),
+            "orc_incr_convolution_part": (None, [i, i, vp, d, d, P, P, P, vp, P, P, i, d, d]),
+            "orc_incr_convolution": (None, [i, d, d, P, P, P, vp, P, P, i, d, d]),
+            "orc_dyson_timestep_omp": (None, [i, P, d, vp, P, i, d, d]),
+            "orc_vie2_timestep_omp": (None, [i, P, P, P, P, i, d, d, i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -173,6 +177,61 @@ def dyson_timestep(n, G, mu, H, Sigma, beta, h, k=5):
     g, s = hm(G), hm(Sigma)
     Ha, hp = _H(H)
     lib().orc_dyson_timestep(n, ctypes.byref(g), mu, hp, ctypes.byref(s), k, beta, h)
+
+
+def _ft(ft):
+    """function data with F(-1) first (a cntr::function-like object or its array), or None"""
+    if ft is None:
+        return None, None
+    a = ft.data if hasattr(ft, "data") and not isinstance(ft, np.ndarray) else ft
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a, a.ctypes.data
+
+
+def incr_convolution(tstp, alpha, C, A, Acc, B, Bcc, beta, h, k=5, ft=None):
+    """cntr incr_convolution (cntr_convolution_impl.hpp:4786-4807): C += alpha A * ft * B at tstp."""
+    c, a, acc, b, bcc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    fa, fp = _ft(ft)
+    alpha = complex(alpha)
+    lib().orc_incr_convolution(tstp, alpha.real, alpha.imag, ctypes.byref(c), ctypes.byref(a), ctypes.byref(acc), fp,
+                               ctypes.byref(b), ctypes.byref(bcc), k, beta, h)
+
+
+def incr_convolution_part(which, tstp, mask, alpha, C, A, Acc, B, Bcc, beta, h, k=5, ft=None):
+    """One component of incr_convolution (0 mat, 1 ret, 2 tv, 3 les) restricted to a mask
+    (sequence of bools, ntau+1 or tstp+1 entries; None = all)."""
+    c, a, acc, b, bcc = hm(C), hm(A), hm(Acc), hm(B), hm(Bcc)
+    fa, fp = _ft(ft)
+    mk = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.int8))
+    alpha = complex(alpha)
+    lib().orc_incr_convolution_part(which, tstp, None if mk is None else mk.ctypes.data, alpha.real, alpha.imag,
+                                    ctypes.byref(c), ctypes.byref(a), ctypes.byref(acc), fp, ctypes.byref(b),
+                                    ctypes.byref(bcc), k, beta, h)
+
+
+def convolution_timestep_new(n, C, A, Acc, B, Bcc, beta, h, k=5, ft=None):
+    """cntr convolution_timestep_new (cntr_convolution_impl.hpp:4811-4976): time step n of C
+    zeroed, then incr_convolution with alpha = 1."""
+    if n == -1:
+        C.mat[...] = 0
+    else:
+        _zero_timestep(C, n)
+    incr_convolution(n, 1.0, C, A, Acc, B, Bcc, beta, h, k, ft)
+
+
+def dyson_timestep_omp(n, G, mu, H, Sigma, beta, h, k=5):
+    """cntr::dyson_timestep_omp (cntr_dyson_omp_impl.hpp:577-605), k + 1 <= n."""
+    assert k + 1 <= n
+    g, s = hm(G), hm(Sigma)
+    Ha, hp = _H(H)
+    lib().orc_dyson_timestep_omp(n, ctypes.byref(g), mu, hp, ctypes.byref(s), k, beta, h)
+
+
+def vie2_timestep_omp(n, G, F, Fcc, Q, beta, h, k=5, method=CNTR_MAT_FIXPOINT):
+    """cntr::vie2_timestep_omp (cntr_vie2_impl.hpp:2125-2190)."""
+    g, f, fc, q = hm(G), hm(F), hm(Fcc), hm(Q)
+    lib().orc_vie2_timestep_omp(n, ctypes.byref(g), ctypes.byref(f), ctypes.byref(fc), ctypes.byref(q), k, beta, h,
+                                method)
 
 
 def vie2_mat(G, F, Fcc, Q, beta, k=5, method=CNTR_MAT_FIXPOINT):
