@@ -17,6 +17,7 @@
 #pragma once
 
 #include <complex>
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -556,6 +557,86 @@ void convolution(HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta, double h, i
 }
 template <class HM> void convolution(HM &C, HM &A, HM &B, double beta, double h, int SolveOrder = 5) {
     convolution(C, A, A, B, B, beta, h, SolveOrder);
+}
+
+// ---- the element-parallel routines of libcntr's OpenMP path ----------------------------------
+// omp_num_threads is accepted for the signature and ignored: every element is a GPU thread.
+//
+// incr_convolution(tstp, alpha, C, A, Acc, f0, ft, B, Bcc, I, beta, h)
+// (cntr_convolution_impl.hpp:4786-4807): C(tstp) += alpha A * F * B; F is a cntr::function
+// (F(-1) as f0, F(t) as ft); the overload without F takes F = 1 (f0 = ft = NULL in the reference).
+namespace detail {
+template <class HM>
+void incr_convolution_raw(int tstp, std::complex<double> alpha, HM &C, HM &A, HM &Acc, const void *fdata, HM &B,
+                          HM &Bcc, double beta, double h, int SolveOrder) {
+    nessi_hm_ptrs c = hm_ptrs(C), a = hm_ptrs(A), acc = hm_ptrs(Acc), b = hm_ptrs(B), bcc = hm_ptrs(Bcc);
+    check(nessi_gpu_incr_convolution_timestep_host(tstp, alpha.real(), alpha.imag(), &c, &a, &acc, fdata, &b, &bcc,
+                                                   C.nt(), C.ntau(), C.size1(), A.sig(), B.sig(), SolveOrder, beta, h));
+}
+}  // namespace detail
+template <class HM, class FN>
+void incr_convolution(int tstp, std::complex<double> alpha, HM &C, HM &A, HM &Acc, FN &F, HM &B, HM &Bcc, double beta,
+                      double h, int SolveOrder = 5) {
+    detail::incr_convolution_raw(tstp, alpha, C, A, Acc, (const void *)F.ptr(-1), B, Bcc, beta, h, SolveOrder);
+}
+template <class HM>
+void incr_convolution(int tstp, std::complex<double> alpha, HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta,
+                      double h, int SolveOrder = 5) {
+    detail::incr_convolution_raw(tstp, alpha, C, A, Acc, nullptr, B, Bcc, beta, h, SolveOrder);
+}
+// convolution_timestep_new (:4916-4976) and convolution_timestep_omp (:5808-5851): C's time step
+// tstp zeroed, then incr_convolution with alpha = 1
+template <class HM>
+void convolution_timestep_new(int tstp, HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta, double h,
+                              int SolveOrder = 5) {
+    const long es = (long)C.size1() * C.size1();
+    if (tstp < 0) {
+        std::fill(C.matptr(0), C.matptr(0) + (C.ntau() + 1) * es, std::complex<double>(0.0));
+    } else {  // C.set_timestep_zero(tstp): ret row, tv row, les column
+        std::fill(C.retptr(tstp, 0), C.retptr(tstp, 0) + (tstp + 1) * es, std::complex<double>(0.0));
+        std::fill(C.tvptr(tstp, 0), C.tvptr(tstp, 0) + (C.ntau() + 1) * es, std::complex<double>(0.0));
+        std::fill(C.lesptr(0, tstp), C.lesptr(0, tstp) + (tstp + 1) * es, std::complex<double>(0.0));
+    }
+    detail::incr_convolution_raw(tstp, 1.0, C, A, Acc, nullptr, B, Bcc, beta, h, SolveOrder);
+}
+template <class HM>
+void convolution_timestep_omp(int omp_num_threads, int tstp, HM &C, HM &A, HM &Acc, HM &B, HM &Bcc, double beta,
+                              double h, int SolveOrder = 5) {
+    (void)omp_num_threads;
+    convolution_timestep_new(tstp, C, A, Acc, B, Bcc, beta, h, SolveOrder);
+}
+template <class HM>
+void convolution_timestep_omp(int omp_num_threads, int tstp, HM &C, HM &A, HM &B, double beta, double h,
+                              int SolveOrder = 5) {
+    convolution_timestep_omp(omp_num_threads, tstp, C, A, A, B, B, beta, h, SolveOrder);
+}
+
+// cntr::dyson_timestep_omp(omp_num_threads, n, G, lam0, H, Sigma, beta, h, SolveOrder)
+// (cntr_dyson_omp_decl.hpp, cntr_dyson_omp_impl.hpp:577-605): the OpenMP solver's
+// discretization of the step, on the device; requires SolveOrder + 1 <= n
+template <class HM, class FN>
+void dyson_timestep_omp(int omp_num_threads, int n, HM &G, double lam0, FN &H, HM &Sigma, double beta, double h,
+                        int SolveOrder = 5) {
+    (void)omp_num_threads;
+    nessi_hm_ptrs g = hm_ptrs(G), s = hm_ptrs(Sigma);
+    check(nessi_gpu_dyson_timestep_omp_host(n, &g, &s, H.ptr(-1), lam0, G.nt(), G.ntau(), G.size1(), G.sig(),
+                                            SolveOrder, beta, h));
+}
+
+// cntr::vie2_timestep_omp(omp_num_threads, tstp, G, F, Fcc, Q, beta, h, SolveOrder, matsubara_method)
+// (cntr_vie2_impl.hpp:2125-2190): tstp = -1 vie2_mat, tstp <= SolveOrder a vie2_start of order
+// tstp (as vie2_timestep above), else the element-parallel step
+template <class HM>
+void vie2_timestep_omp(int omp_num_threads, int tstp, HM &G, HM &F, HM &Fcc, HM &Q, double beta, double h,
+                       int SolveOrder = 5, int matsubara_method = MAT_FIXPOINT) {
+    (void)omp_num_threads;
+    if (tstp <= SolveOrder) {
+        vie2_timestep(tstp, G, F, Fcc, Q, beta, h, SolveOrder, matsubara_method);
+        return;
+    }
+    nessi_hm_ptrs g = hm_ptrs(G), f = hm_ptrs(F), fcc = hm_ptrs(Fcc), q = hm_ptrs(Q);
+    check(nessi_gpu_vie2_timestep_omp_host(tstp, &g, &f, &fcc, &q, G.nt(), G.ntau(), G.size1(), G.sig(), SolveOrder,
+                                           beta, h));
 }
 
 }  // namespace cntr_gpu

@@ -248,6 +248,77 @@ int nessi_gpu_convolution_host(const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, c
                                const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1,
                                int sig_a, int sig_b, int solve_order, double beta, double h);
 
+/* ---- the element-parallel path (the routines of libcntr's OpenMP solvers) ---------------------
+ * Same data conventions as nessi_gpu_convolution_timestep: caller-owned DEVICE pointers in
+ * libcntr's layout, `count` independent problems of equal shape, queued on `stream`, nothing
+ * allocated.  `ft` is NULL or a host array of `count` device pointers to cntr::function data
+ * (F(-1) first, (nt+2) blocks of s^2; a NULL entry means no function).
+ *
+ * incr_convolution(tstp, alpha, C, A, Acc, f0, ft, B, Bcc, I, beta, h)
+ * (cntr_convolution_impl.hpp:4786-4807; components :4164-4760): C(tstp) += alpha [A * F * B](tstp),
+ * every component of time step tstp (mat for tstp = -1), with the reference's per-element
+ * quadrature (the tau integral of the lesser part always end-corrected). */
+int nessi_gpu_incr_convolution_timestep(int tstp, int count, double alpha_re, double alpha_im, const nessi_hm_ptrs *C,
+                                        const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc, const void *const *ft,
+                                        const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1,
+                                        int sig_a, int sig_b, int solve_order, double beta, double h, void *stream);
+
+/* One component of incr_convolution: which = 0 incr_convolution_mat (:4164, tstp = -1), 1 _ret
+ * (:4243), 2 _tv (:4396), 3 _les (:4539), for the output indices whose byte in the DEVICE array
+ * `mask` is nonzero (ntau+1 entries for mat and tv, tstp+1 for ret and les; NULL = all), as the
+ * reference's masks select them. */
+int nessi_gpu_incr_convolution_component(int which, int tstp, const unsigned char *mask, int count, double alpha_re,
+                                         double alpha_im, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                         const nessi_hm_ptrs *Acc, const void *const *ft, const nessi_hm_ptrs *B,
+                                         const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a, int sig_b,
+                                         int solve_order, double beta, double h, void *stream);
+
+/* convolution_timestep_new(tstp, C, A, Acc, [ft,] B, Bcc, I, beta, h) (cntr_convolution_impl.hpp:4811-4976)
+ * and convolution_timestep_omp (:5596-5812), which computes the same elements over threads:
+ * C's time step tstp zeroed, then incr_convolution with alpha = 1. */
+int nessi_gpu_convolution_timestep_new(int tstp, int count, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                       const nessi_hm_ptrs *Acc, const void *const *ft, const nessi_hm_ptrs *B,
+                                       const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a, int sig_b,
+                                       int solve_order, double beta, double h, void *stream);
+
+/* cntr::dyson_timestep_omp(omp_num_threads, n, G, mu, H, Sigma, beta, h, SolveOrder)
+ * (cntr_dyson_omp_impl.hpp:37-605): the OpenMP solver's discretization, every element of the
+ * step a GPU thread: G^R(n, j) and, for n >= 2k+1, G^<(j, n) for j < n-k from the equation in
+ * the other time argument (BD(k+1) derivatives), the k x k start block and the last k+1 lesser
+ * rows as the serial step; G^tv as the serial step.  Not the serial dyson_timestep's
+ * discretization: the two differ by O(h^(k+1)).  H[i] is a device pointer to problem i's
+ * cntr::function H (H(-1) first), mu[i] its chemical potential (host array); requires
+ * SolveOrder + 1 <= n.  If `status` (a DEVICE int) is not NULL it is set to 1 when a step matrix
+ * is singular.  No counterpart of the thread count: the device decides. */
+int nessi_gpu_dyson_timestep_omp(int n, int count, const nessi_hm_ptrs *G, const nessi_hm_ptrs *Sigma,
+                                 const void *const *H, const double *mu, int nt, int ntau, int size1, int sig,
+                                 int solve_order, double beta, double h, int *status, void *stream);
+
+/* cntr::vie2_timestep_omp(omp_num_threads, tstp, G, F, Fcc, Q, beta, h, SolveOrder)
+ * (cntr_vie2_impl.hpp:1851-2190) for tstp > SolveOrder: [1 + F] G = Q with every element of the
+ * time step independent (the reference's vie2_timestep_omp_dispatch); Q is not modified.  The
+ * reference dispatches tstp = -1 to vie2_mat and tstp <= SolveOrder to vie2_start of order tstp:
+ * use nessi_gpu_vie2_mat / nessi_gpu_vie2_start (the C++ front end does).  `status` as above. */
+int nessi_gpu_vie2_timestep_omp(int n, int count, const nessi_hm_ptrs *G, const nessi_hm_ptrs *F,
+                                const nessi_hm_ptrs *Fcc, const nessi_hm_ptrs *Q, int nt, int ntau, int size1, int sig,
+                                int solve_order, double beta, double h, int *status, void *stream);
+
+/* The three above on HOST herm_matrix data (libcntr layout), for single calls with libcntr's
+ * signatures (cntr_gpu.hpp): the operands (whole herm_matrix objects; ft and H as cntr::function
+ * data, F(-1) first) are copied to the device, the step is computed there and the output's time
+ * step (C's for incr_convolution, G's for the solvers; mat for tstp = -1) is copied back.
+ * Allocates and frees device memory and waits; NESSI_ERR_SINGULAR for a singular step matrix. */
+int nessi_gpu_incr_convolution_timestep_host(int tstp, double alpha_re, double alpha_im, const nessi_hm_ptrs *C,
+                                             const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc, const void *ft,
+                                             const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau,
+                                             int size1, int sig_a, int sig_b, int solve_order, double beta, double h);
+int nessi_gpu_dyson_timestep_omp_host(int n, const nessi_hm_ptrs *G, const nessi_hm_ptrs *Sigma, const void *H,
+                                      double mu, int nt, int ntau, int size1, int sig, int solve_order, double beta,
+                                      double h);
+int nessi_gpu_vie2_timestep_omp_host(int n, const nessi_hm_ptrs *G, const nessi_hm_ptrs *F, const nessi_hm_ptrs *Fcc,
+                                     const nessi_hm_ptrs *Q, int nt, int ntau, int size1, int sig, int solve_order,
+                                     double beta, double h);
+
 /* cntr::distance_norm2(tstp, g1, g2) (cntr_utilities_decl.hpp, cntr_utilities_impl.hpp:607-650) between two
  * herm_matrix held on the device (libcntr layout, caller-owned device pointers, tv as
  * (t(ntau+1)+tau) s^2): the sum over the elements of time step tstp (ret row, tv row, les column;

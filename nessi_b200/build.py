@@ -7,6 +7,7 @@ No GPU is needed to build.
 """
 import os
 import subprocess
+import time
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -59,8 +60,12 @@ def build(force=False, verbose=False):
     cmd = [NVCC] + FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd))
+    start = time.time()
     subprocess.check_call(cmd, cwd=CSRC)
     os.replace(tmp, LIB)  # a process that has the old library loaded keeps its copy
+    # stamp the library with the time the compile read its sources, so that a source edited
+    # while nvcc ran is newer than the library and the next build compiles it
+    os.utime(LIB, (start, start))
     return LIB
 
 

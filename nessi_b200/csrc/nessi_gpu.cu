@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/nessi_gpu.h"
@@ -19,6 +20,7 @@
 #include "kernels_start.cuh"
 #include "kernels_mat.cuh"
 #include "kernels_conv.cuh"
+#include "kernels_omp.cuh"
 #include "kernels_lattice.cuh"
 
 
@@ -1985,4 +1987,461 @@ extern "C" int nessi_gpu_gw_sigma_timestep(int tstp, int nk, const nessi_hm_ptrs
                                            void *stream) {
     NvtxRange nvtx_("nessi::gw_sigma_timestep");
     return gw_launch(2, tstp, nk, G, W, S, w, nt, ntau, size1, 1, stream, "gw_sigma_timestep");
+}
+
+// =====================================================================================
+// The element-parallel path: incr_convolution, convolution_timestep_new, dyson_timestep_omp,
+// vie2_timestep_omp on device-resident herm_matrix data (kernels_omp.cuh)
+// =====================================================================================
+namespace {
+ConvHM omp_hm(const nessi_hm_ptrs &x) {
+    ConvHM y;
+    y.ret = (double2 *)x.ret; y.les = (double2 *)x.les; y.tv = (double2 *)x.tv; y.mat = (double2 *)x.mat;
+    return y;
+}
+
+template <class Fn> int size_dispatch(int size1, Fn &&fn) {
+    switch (size1) {
+        case 1: return fn(std::integral_constant<int, 1>{});
+        case 2: return fn(std::integral_constant<int, 2>{});
+        case 3: return fn(std::integral_constant<int, 3>{});
+        case 4: return fn(std::integral_constant<int, 4>{});
+        case 5: return fn(std::integral_constant<int, 5>{});
+        case 6: return fn(std::integral_constant<int, 6>{});
+        case 7: return fn(std::integral_constant<int, 7>{});
+        case 8: return fn(std::integral_constant<int, 8>{});
+    }
+    set_err("size1 %d unsupported", size1);
+    return NESSI_ERR_ARG;
+}
+
+unsigned omp_grid(long items) { return (unsigned)std::min<long>(std::max<long>(1, (items + 127) / 128), 1024); }
+
+// one incr_convolution component (0 mat, 1 ret, 2 tv, 3 les) over output indices [ob.lo, ob.hi)
+template <int S> int incr_launch(const OmpBatch &ob, int which, int tstp, cudaStream_t st) {
+    const long items = (long)(ob.hi - ob.lo) * S * S;
+    if (items <= 0 || ob.count <= 0) return NESSI_OK;
+    const dim3 grid(omp_grid(items), ob.count);
+    if (which == 0) k_incr_mat<S><<<grid, 128, 0, st>>>(ob);
+    else if (which == 1) k_incr_ret<S><<<grid, 128, 0, st>>>(ob, tstp);
+    else if (which == 2) k_incr_tv<S><<<grid, 128, 0, st>>>(ob, tstp);
+    else k_incr_les<S><<<grid, 128, 0, st>>>(ob, tstp);
+    CK(cudaGetLastError());
+    return NESSI_OK;
+}
+
+int omp_common_checks(const char *name, int tstp, int nt, int ntau, int size1, int solve_order, double beta, double h) {
+    if (size1 < 1 || size1 > NESSI_MAXS || solve_order < 1 || solve_order > CNTR_KMAX || nt < solve_order ||
+        ntau < solve_order || tstp < -1 || tstp > nt || !(beta > 0) || !(h > 0)) {
+        set_err("%s: bad dimensions (tstp=%d nt=%d ntau=%d size1=%d k=%d)", name, tstp, nt, ntau, size1, solve_order);
+        return NESSI_ERR_ARG;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) { set_err("%s: device index %d unsupported", name, dev); return NESSI_ERR_ARG; }
+    return ensure_tables(dev);
+}
+
+// incr_convolution over components `which` (-1: every component of tstp, mat for tstp = -1)
+int incr_run(const char *name, int which, int tstp, const unsigned char *mask, int count, double2 alpha,
+             const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc, const void *const *ft,
+             const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a, int sig_b,
+             int solve_order, double beta, double h, void *stream) {
+    if (count < 0 || (count > 0 && (!C || !A || !Acc || !B || !Bcc)) || (sig_a != 1 && sig_a != -1) ||
+        (sig_b != 1 && sig_b != -1) || which < -1 || which > 3 || (which == 0 && tstp != -1) ||
+        (which > 0 && tstp < 0)) {
+        set_err("%s: bad arguments", name);
+        return NESSI_ERR_ARG;
+    }
+    for (int i = 0; i < count; i++) {
+        bool ok = B[i].mat && (tstp >= 0 || (A[i].mat && C[i].mat));
+        const nessi_hm_ptrs *all[5] = {&C[i], &A[i], &Acc[i], &B[i], &Bcc[i]};
+        if (tstp >= 0)
+            for (const nessi_hm_ptrs *x : all) ok = ok && x->ret && x->les && x->tv;
+        if (!ok) { set_err("%s: problem %d has a null pointer it needs", name, i); return NESSI_ERR_ARG; }
+    }
+    CKR(omp_common_checks(name, tstp, nt, ntau, size1, solve_order, beta, h));
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int i0 = 0; i0 < count; i0 += NESSI_OMP_MAXP) {
+        OmpBatch ob;
+        std::memset(&ob, 0, sizeof ob);
+        ob.count = std::min(NESSI_OMP_MAXP, count - i0);
+        for (int i = 0; i < ob.count; i++) {
+            OmpProb &P = ob.p[i];
+            P.C = P.Cin = omp_hm(C[i0 + i]); P.A = omp_hm(A[i0 + i]); P.Acc = omp_hm(Acc[i0 + i]);
+            P.B = omp_hm(B[i0 + i]); P.Bcc = omp_hm(Bcc[i0 + i]);
+            P.f = ft ? (const double2 *)ft[i0 + i] : nullptr;
+        }
+        ob.mask = mask; ob.alpha = alpha; ob.ntau = ntau; ob.sig_a = sig_a; ob.sig_b = sig_b; ob.k = solve_order;
+        ob.h = h; ob.beta = beta; ob.out_mode = 0; ob.skip_tstp = 0;
+        const int w0 = which >= 0 ? which : (tstp < 0 ? 0 : 1), w1 = which >= 0 ? which : (tstp < 0 ? 0 : 3);
+        for (int w = w0; w <= w1; w++) {
+            ob.lo = 0;
+            ob.hi = (w == 0 || w == 2) ? ntau + 1 : tstp + 1;
+            CKR(size_dispatch(size1, [&](auto sz) { return incr_launch<decltype(sz)::value>(ob, w, tstp, st); }));
+        }
+    }
+    return NESSI_OK;
+}
+}  // namespace
+
+extern "C" int nessi_gpu_incr_convolution_timestep(int tstp, int count, double alpha_re, double alpha_im,
+                                                   const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                                   const nessi_hm_ptrs *Acc, const void *const *ft,
+                                                   const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau,
+                                                   int size1, int sig_a, int sig_b, int solve_order, double beta,
+                                                   double h, void *stream) {
+    NvtxRange nvtx_("nessi::incr_convolution");
+    return incr_run("incr_convolution", -1, tstp, nullptr, count, cmk(alpha_re, alpha_im), C, A, Acc, ft, B, Bcc, nt,
+                    ntau, size1, sig_a, sig_b, solve_order, beta, h, stream);
+}
+
+extern "C" int nessi_gpu_incr_convolution_component(int which, int tstp, const unsigned char *mask, int count,
+                                                    double alpha_re, double alpha_im, const nessi_hm_ptrs *C,
+                                                    const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc,
+                                                    const void *const *ft, const nessi_hm_ptrs *B,
+                                                    const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a,
+                                                    int sig_b, int solve_order, double beta, double h, void *stream) {
+    NvtxRange nvtx_("nessi::incr_convolution_component");
+    if (which < 0) { set_err("incr_convolution_component: which = %d", which); return NESSI_ERR_ARG; }
+    return incr_run("incr_convolution_component", which, tstp, mask, count, cmk(alpha_re, alpha_im), C, A, Acc, ft,
+                    B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, stream);
+}
+
+extern "C" int nessi_gpu_convolution_timestep_new(int tstp, int count, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                                  const nessi_hm_ptrs *Acc, const void *const *ft,
+                                                  const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau,
+                                                  int size1, int sig_a, int sig_b, int solve_order, double beta,
+                                                  double h, void *stream) {
+    NvtxRange nvtx_("nessi::convolution_timestep_new");
+    if (count < 0 || (count > 0 && !C) || size1 < 1 || size1 > NESSI_MAXS || tstp < -1 || tstp > nt || ntau < 0) {
+        set_err("convolution_timestep_new: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    // C.set_timestep_zero(tstp): ret row, tv row and les column of tstp are contiguous
+    const long s2 = (long)size1 * size1, M = ntau + 1;
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int i = 0; i < count; i++) {
+        if (tstp < 0) {
+            if (!C[i].mat) { set_err("convolution_timestep_new: problem %d has no mat", i); return NESSI_ERR_ARG; }
+            CK(cudaMemsetAsync(C[i].mat, 0, (size_t)M * s2 * 16, st));
+        } else {
+            if (!C[i].ret || !C[i].tv || !C[i].les) {
+                set_err("convolution_timestep_new: problem %d has a null pointer", i);
+                return NESSI_ERR_ARG;
+            }
+            CK(cudaMemsetAsync((char *)C[i].ret + tri_h(tstp) * s2 * 16, 0, (size_t)(tstp + 1) * s2 * 16, st));
+            CK(cudaMemsetAsync((char *)C[i].tv + (long)tstp * M * s2 * 16, 0, (size_t)M * s2 * 16, st));
+            CK(cudaMemsetAsync((char *)C[i].les + tri_h(tstp) * s2 * 16, 0, (size_t)(tstp + 1) * s2 * 16, st));
+        }
+    }
+    return incr_run("convolution_timestep_new", -1, tstp, nullptr, count, cmk(1.0, 0.0), C, A, Acc, ft, B, Bcc, nt,
+                    ntau, size1, sig_a, sig_b, solve_order, beta, h, stream);
+}
+
+namespace {
+template <int S> int dyson_omp_launch(int n, const OmpBatch &base, int ntau, int *status, cudaStream_t st) {
+    const int k = base.k, M = ntau + 1, KS = k * S, s2 = S * S;
+    const dim3 tb(128);
+    auto grid = [&](long items) { return dim3(omp_grid(items), base.count); };
+    // retarded: start block, the convolution for columns j < n-k (G^R(n, j) read as zero), solves
+    {
+        OmpBatch ob = base;  // C = B = Bcc = G, A = Acc = Sigma
+        const size_t smem = (size_t)(2 * KS * KS + 2 * k * s2) * 16 + 16;
+        CK(cudaFuncSetAttribute(k_omp_ret_start<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_omp_ret_start<S><<<base.count, 256, smem, st>>>(ob, n, status);
+        CK(cudaGetLastError());
+        ob.lo = 0; ob.hi = n - k; ob.out_mode = 2; ob.skip_tstp = 1;
+        CKR(incr_launch<S>(ob, 1, n, st));
+        k_omp_ret_solve<S><<<grid(n - k), tb, 0, st>>>(ob, n, status);
+        CK(cudaGetLastError());
+    }
+    // left-mixing: the convolution (G^tv(n, .) read as zero), then the BDF solves
+    {
+        OmpBatch ob = base;
+        ob.lo = 0; ob.hi = M; ob.out_mode = 2; ob.skip_tstp = 1;
+        CKR(incr_launch<S>(ob, 2, n, st));
+        k_omp_tv_solve<S><<<grid(M), tb, 0, st>>>(ob, n, status);
+        CK(cudaGetLastError());
+    }
+    // lesser: rows j < n-k from the conjugate equation (n >= 2k+1), then rows n-k..n in sequence
+    const bool full = n < 2 * k + 1;
+    if (!full) {
+        OmpBatch ob = base;  // [G * Sigma]^<: A = Acc = G, B = Bcc = Sigma
+        for (int i = 0; i < ob.count; i++) {
+            ob.p[i].A = ob.p[i].Acc = base.p[i].C;
+            ob.p[i].B = ob.p[i].Bcc = base.p[i].A;
+        }
+        ob.lo = 0; ob.hi = n - k; ob.out_mode = 2; ob.skip_tstp = 1;
+        CKR(incr_launch<S>(ob, 3, n, st));
+        OmpBatch os = base;
+        k_omp_les_solve<S><<<grid(n - k), tb, 0, st>>>(os, n, status);
+        CK(cudaGetLastError());
+    }
+    {
+        OmpBatch ob = base;  // A = Sigma, B = Bcc = G (the serial step's gles)
+        const int nthr = 256, ngrp = nthr / s2;
+        const size_t smem = (size_t)(ngrp * s2 + 2 * s2 + KS * KS + KS * S) * 16 + 16;
+        k_omp_les_serial<S><<<base.count, nthr, smem, st>>>(ob, n, full ? 1 : 0, status);
+        CK(cudaGetLastError());
+    }
+    return NESSI_OK;
+}
+
+template <int S> int vie2_omp_launch(int tstp, const OmpBatch &base, int ntau, int *status, cudaStream_t st) {
+    const int M = ntau + 1;
+    const dim3 tb(128);
+    auto grid = [&](long items) { return dim3(omp_grid(items), base.count); };
+    // base: C = G, Cin = Q, A = F, Acc = Fcc, B = Bcc = G, alpha = -1, Q as the base
+    {
+        OmpBatch ob = base;
+        ob.lo = 0; ob.hi = tstp + 1;
+        CKR(incr_launch<S>(ob, 1, tstp, st));
+        k_omp_vie2_solve<S><<<grid(tstp + 1), tb, 0, st>>>(ob, tstp, 0, status);
+        CK(cudaGetLastError());
+    }
+    {
+        OmpBatch ob = base;
+        ob.lo = 0; ob.hi = M;
+        CKR(incr_launch<S>(ob, 2, tstp, st));
+        k_omp_vie2_solve<S><<<grid(M), tb, 0, st>>>(ob, tstp, 1, status);
+        CK(cudaGetLastError());
+    }
+    {
+        // lesser: Q - G * Fcc with A = Acc = G, B = Fcc, Bcc = F; rows below tstp, then row tstp
+        OmpBatch ob = base;
+        for (int i = 0; i < ob.count; i++) {
+            ob.p[i].A = ob.p[i].Acc = base.p[i].C;
+            ob.p[i].B = base.p[i].Acc;
+            ob.p[i].Bcc = base.p[i].A;
+        }
+        OmpBatch os = base;  // the solves read F^R(tstp, tstp) from A
+        for (int part = 0; part < 2; part++) {
+            ob.lo = os.lo = part ? tstp : 0;
+            ob.hi = os.hi = part ? tstp + 1 : tstp;
+            if (ob.hi <= ob.lo) continue;
+            CKR(incr_launch<S>(ob, 3, tstp, st));
+            k_omp_vie2_solve<S><<<grid(ob.hi - ob.lo), tb, 0, st>>>(os, tstp, 2, status);
+            CK(cudaGetLastError());
+        }
+    }
+    return NESSI_OK;
+}
+}  // namespace
+
+extern "C" int nessi_gpu_dyson_timestep_omp(int n, int count, const nessi_hm_ptrs *G, const nessi_hm_ptrs *Sigma,
+                                            const void *const *H, const double *mu, int nt, int ntau, int size1,
+                                            int sig, int solve_order, double beta, double h, int *status,
+                                            void *stream) {
+    NvtxRange nvtx_("nessi::dyson_timestep_omp");
+    if (count < 0 || (count > 0 && (!G || !Sigma || !H || !mu)) || (sig != 1 && sig != -1)) {
+        set_err("dyson_timestep_omp: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    if (n < solve_order + 1) {
+        set_err("dyson_timestep_omp: n = %d must exceed SolveOrder = %d (dyson_start covers n <= k)", n, solve_order);
+        return NESSI_ERR_ARG;
+    }
+    for (int i = 0; i < count; i++) {
+        const nessi_hm_ptrs *all[2] = {&G[i], &Sigma[i]};
+        bool ok = H[i] && G[i].mat;
+        for (const nessi_hm_ptrs *x : all) ok = ok && x->ret && x->les && x->tv;
+        if (!ok) { set_err("dyson_timestep_omp: problem %d has a null pointer it needs", i); return NESSI_ERR_ARG; }
+    }
+    CKR(omp_common_checks("dyson_timestep_omp", n, nt, ntau, size1, solve_order, beta, h));
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int i0 = 0; i0 < count; i0 += NESSI_OMP_MAXP) {
+        OmpBatch ob;
+        std::memset(&ob, 0, sizeof ob);
+        ob.count = std::min(NESSI_OMP_MAXP, count - i0);
+        for (int i = 0; i < ob.count; i++) {
+            OmpProb &P = ob.p[i];
+            P.C = P.Cin = P.B = P.Bcc = omp_hm(G[i0 + i]);
+            P.A = P.Acc = omp_hm(Sigma[i0 + i]);
+            P.H = (const double2 *)H[i0 + i];
+            P.mu = mu[i0 + i];
+        }
+        ob.alpha = cmk(1.0, 0.0); ob.ntau = ntau; ob.sig_a = sig; ob.sig_b = sig; ob.k = solve_order;
+        ob.h = h; ob.beta = beta;
+        CKR(size_dispatch(size1, [&](auto sz) { return dyson_omp_launch<decltype(sz)::value>(n, ob, ntau, status, st); }));
+    }
+    return NESSI_OK;
+}
+
+extern "C" int nessi_gpu_vie2_timestep_omp(int n, int count, const nessi_hm_ptrs *G, const nessi_hm_ptrs *F,
+                                           const nessi_hm_ptrs *Fcc, const nessi_hm_ptrs *Q, int nt, int ntau,
+                                           int size1, int sig, int solve_order, double beta, double h, int *status,
+                                           void *stream) {
+    NvtxRange nvtx_("nessi::vie2_timestep_omp");
+    if (count < 0 || (count > 0 && (!G || !F || !Fcc || !Q)) || (sig != 1 && sig != -1)) {
+        set_err("vie2_timestep_omp: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    if (n < solve_order + 1) {
+        set_err("vie2_timestep_omp: n = %d must exceed SolveOrder = %d (vie2_start / vie2_mat cover n <= k)", n,
+                solve_order);
+        return NESSI_ERR_ARG;
+    }
+    for (int i = 0; i < count; i++) {
+        const nessi_hm_ptrs *all[4] = {&G[i], &F[i], &Fcc[i], &Q[i]};
+        bool ok = G[i].mat;
+        for (const nessi_hm_ptrs *x : all) ok = ok && x->ret && x->les && x->tv;
+        if (!ok) { set_err("vie2_timestep_omp: problem %d has a null pointer it needs", i); return NESSI_ERR_ARG; }
+    }
+    CKR(omp_common_checks("vie2_timestep_omp", n, nt, ntau, size1, solve_order, beta, h));
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int i0 = 0; i0 < count; i0 += NESSI_OMP_MAXP) {
+        OmpBatch ob;
+        std::memset(&ob, 0, sizeof ob);
+        ob.count = std::min(NESSI_OMP_MAXP, count - i0);
+        for (int i = 0; i < ob.count; i++) {
+            OmpProb &P = ob.p[i];
+            P.C = P.B = P.Bcc = omp_hm(G[i0 + i]);
+            P.Cin = omp_hm(Q[i0 + i]);
+            P.A = omp_hm(F[i0 + i]);
+            P.Acc = omp_hm(Fcc[i0 + i]);
+        }
+        ob.alpha = cmk(-1.0, 0.0); ob.ntau = ntau; ob.sig_a = sig; ob.sig_b = sig; ob.k = solve_order;
+        ob.h = h; ob.beta = beta; ob.out_mode = 1; ob.skip_tstp = 1;
+        CKR(size_dispatch(size1, [&](auto sz) { return vie2_omp_launch<decltype(sz)::value>(n, ob, ntau, status, st); }));
+    }
+    return NESSI_OK;
+}
+
+// ---- the same on HOST herm_matrix data (single calls with libcntr's signatures) ------------
+namespace {
+// Device copies of host herm_matrix data and function arrays for one call; the output's time
+// step comes back on success.  Every allocation is freed on every path.
+struct HostMirror {
+    int nt, ntau;
+    long s2, M;
+    std::vector<void *> owned;
+    std::string err;
+    HostMirror(int nt_, int ntau_, int size1) : nt(nt_), ntau(ntau_), s2((long)size1 * size1), M(ntau_ + 1) {}
+    ~HostMirror() { for (void *q : owned) cudaFree(q); }
+    int upload(const void *src, long count, void **dst) {
+        *dst = nullptr;
+        if (!src) return NESSI_OK;
+        if (cudaMalloc(dst, (size_t)count * 16) != cudaSuccess) { set_err("cudaMalloc failed"); return NESSI_ERR_OOM; }
+        owned.push_back(*dst);
+        if (cudaMemcpy(*dst, src, (size_t)count * 16, cudaMemcpyHostToDevice) != cudaSuccess) {
+            set_err("upload failed");
+            return NESSI_ERR_CUDA;
+        }
+        return NESSI_OK;
+    }
+    int hm(const nessi_hm_ptrs *h, nessi_hm_ptrs *d) {
+        const long tri = tri_h(nt + 1) * s2;
+        CKR(upload(h->ret, tri, &d->ret));
+        CKR(upload(h->les, tri, &d->les));
+        CKR(upload(h->tv, (long)(nt + 1) * M * s2, &d->tv));
+        return upload(h->mat, M * s2, &d->mat);
+    }
+    // time step n of the device herm_matrix d back into the host one (mat for n = -1)
+    int download_step(int n, const nessi_hm_ptrs *h, const nessi_hm_ptrs &d) {
+        if (cudaDeviceSynchronize() != cudaSuccess) { set_err("device step failed"); return NESSI_ERR_CUDA; }
+        auto back = [&](void *hp, const void *dp, long off, long cnt) {
+            if (!hp || !dp) return cudaSuccess;
+            return cudaMemcpy((char *)hp + off * 16, (const char *)dp + off * 16, (size_t)cnt * 16, cudaMemcpyDeviceToHost);
+        };
+        cudaError_t e;
+        if (n < 0) {
+            e = back(h->mat, d.mat, 0, M * s2);
+        } else {
+            e = back(h->ret, d.ret, tri_h(n) * s2, (long)(n + 1) * s2);
+            if (e == cudaSuccess) e = back(h->tv, d.tv, (long)n * M * s2, M * s2);
+            if (e == cudaSuccess) e = back(h->les, d.les, tri_h(n) * s2, (long)(n + 1) * s2);
+        }
+        if (e != cudaSuccess) { set_err("download failed"); return NESSI_ERR_CUDA; }
+        return NESSI_OK;
+    }
+};
+
+int device_status(int *d_status) {
+    int hs = 0;
+    if (cudaMemcpy(&hs, d_status, sizeof hs, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_err("status read failed");
+        return NESSI_ERR_CUDA;
+    }
+    if (hs) { set_err("a step matrix is singular"); return NESSI_ERR_SINGULAR; }
+    return NESSI_OK;
+}
+}  // namespace
+
+extern "C" int nessi_gpu_incr_convolution_timestep_host(int tstp, double alpha_re, double alpha_im,
+                                                        const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+                                                        const nessi_hm_ptrs *Acc, const void *ft,
+                                                        const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt,
+                                                        int ntau, int size1, int sig_a, int sig_b, int solve_order,
+                                                        double beta, double h) {
+    if (!C || !A || !Acc || !B || !Bcc || nt < 0 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS || tstp < -1 ||
+        tstp > nt) {
+        set_err("incr_convolution_timestep_host: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    CK(cudaSetDevice(g_device));
+    HostMirror hm(nt, ntau, size1);
+    nessi_hm_ptrs d[5];
+    const nessi_hm_ptrs *hs[5] = {C, A, Acc, B, Bcc};
+    for (int i = 0; i < 5; i++) CKR(hm.hm(hs[i], &d[i]));
+    void *dft = nullptr;
+    CKR(hm.upload(ft, (long)(nt + 2) * size1 * size1, &dft));
+    const void *fts[1] = {dft};
+    CKR(nessi_gpu_incr_convolution_timestep(tstp, 1, alpha_re, alpha_im, &d[0], &d[1], &d[2], ft ? fts : nullptr, &d[3],
+                                            &d[4], nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, nullptr));
+    return hm.download_step(tstp, C, d[0]);
+}
+
+extern "C" int nessi_gpu_dyson_timestep_omp_host(int n, const nessi_hm_ptrs *G, const nessi_hm_ptrs *Sigma,
+                                                 const void *H, double mu, int nt, int ntau, int size1, int sig,
+                                                 int solve_order, double beta, double h) {
+    if (!G || !Sigma || !H || nt < 0 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS) {
+        set_err("dyson_timestep_omp_host: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    if (n < solve_order + 1 || n > nt) {
+        set_err("dyson_timestep_omp_host: n = %d outside SolveOrder+1..nt", n);
+        return NESSI_ERR_ARG;
+    }
+    CK(cudaSetDevice(g_device));
+    HostMirror hm(nt, ntau, size1);
+    nessi_hm_ptrs dG, dS;
+    CKR(hm.hm(G, &dG));
+    CKR(hm.hm(Sigma, &dS));
+    void *dH = nullptr, *dst = nullptr;
+    CKR(hm.upload(H, (long)(nt + 2) * size1 * size1, &dH));
+    if (cudaMalloc(&dst, 16) != cudaSuccess) { set_err("cudaMalloc failed"); return NESSI_ERR_OOM; }
+    hm.owned.push_back(dst);
+    CK(cudaMemset(dst, 0, 16));
+    const void *Hs[1] = {dH};
+    CKR(nessi_gpu_dyson_timestep_omp(n, 1, &dG, &dS, Hs, &mu, nt, ntau, size1, sig, solve_order, beta, h, (int *)dst,
+                                     nullptr));
+    CKR(hm.download_step(n, G, dG));
+    return device_status((int *)dst);
+}
+
+extern "C" int nessi_gpu_vie2_timestep_omp_host(int n, const nessi_hm_ptrs *G, const nessi_hm_ptrs *F,
+                                                const nessi_hm_ptrs *Fcc, const nessi_hm_ptrs *Q, int nt, int ntau,
+                                                int size1, int sig, int solve_order, double beta, double h) {
+    if (!G || !F || !Fcc || !Q || nt < 0 || ntau < 0 || size1 < 1 || size1 > NESSI_MAXS) {
+        set_err("vie2_timestep_omp_host: bad arguments");
+        return NESSI_ERR_ARG;
+    }
+    if (n < solve_order + 1 || n > nt) {
+        set_err("vie2_timestep_omp_host: n = %d outside SolveOrder+1..nt", n);
+        return NESSI_ERR_ARG;
+    }
+    CK(cudaSetDevice(g_device));
+    HostMirror hm(nt, ntau, size1);
+    nessi_hm_ptrs d[4];
+    const nessi_hm_ptrs *hs[4] = {G, F, Fcc, Q};
+    for (int i = 0; i < 4; i++) CKR(hm.hm(hs[i], &d[i]));
+    void *dst = nullptr;
+    if (cudaMalloc(&dst, 16) != cudaSuccess) { set_err("cudaMalloc failed"); return NESSI_ERR_OOM; }
+    hm.owned.push_back(dst);
+    CK(cudaMemset(dst, 0, 16));
+    CKR(nessi_gpu_vie2_timestep_omp(n, 1, &d[0], &d[1], &d[2], &d[3], nt, ntau, size1, sig, solve_order, beta, h,
+                                    (int *)dst, nullptr));
+    CKR(hm.download_step(n, G, d[0]));
+    return device_status((int *)dst);
 }

@@ -93,6 +93,33 @@ EXPORTS = {
                                             [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double]),
     "nessi_gpu_convolution_host": (ctypes.c_int, [ctypes.POINTER(HmPtrs)] * 5 + [ctypes.c_int] * 6 +
                                    [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_incr_convolution_timestep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double] +
+                                            [ctypes.POINTER(HmPtrs)] * 3 + [ctypes.c_void_p] +
+                                            [ctypes.POINTER(HmPtrs)] * 2 + [ctypes.c_int] * 6 +
+                                            [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    "nessi_gpu_incr_convolution_component": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                            ctypes.c_double, ctypes.c_double] +
+                                             [ctypes.POINTER(HmPtrs)] * 3 + [ctypes.c_void_p] +
+                                             [ctypes.POINTER(HmPtrs)] * 2 + [ctypes.c_int] * 6 +
+                                             [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    "nessi_gpu_convolution_timestep_new": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 3 +
+                                           [ctypes.c_void_p] + [ctypes.POINTER(HmPtrs)] * 2 + [ctypes.c_int] * 6 +
+                                           [ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    "nessi_gpu_dyson_timestep_omp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 2 +
+                                     [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 5 +
+                                     [ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
+    "nessi_gpu_vie2_timestep_omp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 4 +
+                                    [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                                          ctypes.c_void_p]),
+    "nessi_gpu_incr_convolution_timestep_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double] +
+                                                 [ctypes.POINTER(HmPtrs)] * 3 + [ctypes.c_void_p] +
+                                                 [ctypes.POINTER(HmPtrs)] * 2 + [ctypes.c_int] * 6 +
+                                                 [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_dyson_timestep_omp_host": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 2 +
+                                          [ctypes.c_void_p, ctypes.c_double] + [ctypes.c_int] * 5 +
+                                          [ctypes.c_double, ctypes.c_double]),
+    "nessi_gpu_vie2_timestep_omp_host": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(HmPtrs)] * 4 +
+                                         [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.c_double]),
     "nessi_gpu_distance_norm2": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(HmPtrs), ctypes.POINTER(HmPtrs)] +
                                  [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_void_p]),
     "nessi_gpu_gw_polarization_timestep": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -401,6 +428,86 @@ def convolution_timestep_dev(n, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b
                                                          ctypes.c_void_p(stream) if stream else None))
 
 
+def _hm_array(lst):
+    a = (HmPtrs * max(len(lst), 1))()
+    for i, t in enumerate(lst):
+        a[i] = HmPtrs(*[ctypes.c_void_p(x) if x else None for x in t])
+    return a
+
+
+def _ptr_array(lst):
+    """host array of device pointers (integers, 0 = none), or None for no list"""
+    if lst is None:
+        return None
+    a = (ctypes.c_void_p * max(len(lst), 1))()
+    for i, x in enumerate(lst):
+        a[i] = ctypes.c_void_p(x) if x else None
+    return a
+
+
+def _stream(stream):
+    return ctypes.c_void_p(stream) if stream else None
+
+
+def incr_convolution_dev(tstp, alpha, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, ft=None,
+                         stream=0):
+    """incr_convolution (cntr_convolution_impl.hpp:4786-4807): C(tstp) += alpha A * ft * B for len(C)
+    problems on device memory; C, A, Acc, B, Bcc are lists of (ret, les, tv, mat) device pointers,
+    ft None or a list of device pointers to function data (F(-1) first).  Allocates nothing."""
+    if not _inited:
+        init(0)
+    alpha = complex(alpha)
+    _check(load_library().nessi_gpu_incr_convolution_timestep(
+        tstp, len(C), alpha.real, alpha.imag, _hm_array(C), _hm_array(A), _hm_array(Acc), _ptr_array(ft), _hm_array(B),
+        _hm_array(Bcc), nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, _stream(stream)))
+
+
+def incr_convolution_component_dev(which, tstp, mask_ptr, alpha, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b,
+                                   solve_order, beta, h, ft=None, stream=0):
+    """One component of incr_convolution (0 mat, 1 ret, 2 tv, 3 les) for the output indices whose
+    byte in the device array at mask_ptr is nonzero (0 = all)."""
+    if not _inited:
+        init(0)
+    alpha = complex(alpha)
+    _check(load_library().nessi_gpu_incr_convolution_component(
+        which, tstp, ctypes.c_void_p(mask_ptr) if mask_ptr else None, len(C), alpha.real, alpha.imag, _hm_array(C),
+        _hm_array(A), _hm_array(Acc), _ptr_array(ft), _hm_array(B), _hm_array(Bcc), nt, ntau, size1, sig_a, sig_b,
+        solve_order, beta, h, _stream(stream)))
+
+
+def convolution_timestep_new_dev(tstp, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h, ft=None,
+                                 stream=0):
+    """convolution_timestep_new / convolution_timestep_omp (cntr_convolution_impl.hpp:4811-4976,
+    5596-5812): C's time step zeroed, then incr_convolution with alpha = 1."""
+    if not _inited:
+        init(0)
+    _check(load_library().nessi_gpu_convolution_timestep_new(
+        tstp, len(C), _hm_array(C), _hm_array(A), _hm_array(Acc), _ptr_array(ft), _hm_array(B), _hm_array(Bcc), nt,
+        ntau, size1, sig_a, sig_b, solve_order, beta, h, _stream(stream)))
+
+
+def dyson_timestep_omp_dev(n, G, Sigma, H, mu, nt, ntau, size1, sig, solve_order, beta, h, status_ptr=0, stream=0):
+    """cntr::dyson_timestep_omp (cntr_dyson_omp_impl.hpp:37-605) for len(G) problems on device
+    memory: G, Sigma lists of (ret, les, tv, mat) device pointers, H device pointers to function
+    data (H(-1) first), mu a list of floats; status_ptr an optional device int set on a singular
+    step matrix."""
+    if not _inited:
+        init(0)
+    mus = (ctypes.c_double * max(len(G), 1))(*[float(x) for x in mu])
+    _check(load_library().nessi_gpu_dyson_timestep_omp(
+        n, len(G), _hm_array(G), _hm_array(Sigma), _ptr_array(H), mus, nt, ntau, size1, sig, solve_order, beta, h,
+        ctypes.c_void_p(status_ptr) if status_ptr else None, _stream(stream)))
+
+
+def vie2_timestep_omp_dev(n, G, F, Fcc, Q, nt, ntau, size1, sig, solve_order, beta, h, status_ptr=0, stream=0):
+    """cntr::vie2_timestep_omp (cntr_vie2_impl.hpp:1851-2190) for n > solve_order on device memory."""
+    if not _inited:
+        init(0)
+    _check(load_library().nessi_gpu_vie2_timestep_omp(
+        n, len(G), _hm_array(G), _hm_array(F), _hm_array(Fcc), _hm_array(Q), nt, ntau, size1, sig, solve_order, beta,
+        h, ctypes.c_void_p(status_ptr) if status_ptr else None, _stream(stream)))
+
+
 # ---- cntr-style single-problem entry points ---------------------------------------------
 def convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder=5):
     """cntr::convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder) on host herm_matrix
@@ -412,6 +519,78 @@ def convolution_timestep(n, C, A, Acc, B, Bcc, beta, h, SolveOrder=5):
         return ctypes.byref(HmPtrs(_ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
     _check(load_library().nessi_gpu_convolution_timestep_host(n, hp(C), hp(A), hp(Acc), hp(B), hp(Bcc), C.nt, C.ntau,
                                                               C.size1, A.sig, B.sig, SolveOrder, beta, h))
+
+
+def _hp(G):
+    return ctypes.byref(HmPtrs(_ptr(G.ret), _ptr(G.les), _ptr(G.tv), _ptr(G.mat)))
+
+
+def _fn_data(F):
+    """cntr::function-like object (or its (nt+2, s, s) array) as a contiguous complex128 array"""
+    a = F.data if hasattr(F, "data") and not isinstance(F, np.ndarray) else F
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def incr_convolution(tstp, alpha, C, A, Acc, B, Bcc, beta, h, SolveOrder=5, ft=None):
+    """incr_convolution (cntr_convolution_impl.hpp:4786-4807) on host herm_matrix objects:
+    C(tstp) += alpha A * ft * B, written in place (ft: cntr::function or None)."""
+    if not _inited:
+        init(0)
+    alpha = complex(alpha)
+    fd = None if ft is None else _fn_data(ft)
+    _check(load_library().nessi_gpu_incr_convolution_timestep_host(
+        tstp, alpha.real, alpha.imag, _hp(C), _hp(A), _hp(Acc), None if fd is None else fd.ctypes.data, _hp(B),
+        _hp(Bcc), C.nt, C.ntau, C.size1, A.sig, B.sig, SolveOrder, beta, h))
+
+
+def convolution_timestep_omp(omp_num_threads, tstp, C, A, Acc, B, Bcc, beta, h, SolveOrder=5):
+    """cntr::convolution_timestep_omp / convolution_timestep_new (cntr_convolution_impl.hpp:4916-4976,
+    5596-5812) on host herm_matrix objects: C's time step zeroed, then incr_convolution with alpha = 1;
+    omp_num_threads is ignored (every element is a GPU thread)."""
+    if tstp == -1:
+        C.mat[...] = 0
+    else:
+        C.ret[C.ret_index(tstp, 0):C.ret_index(tstp, tstp) + 1] = 0
+        C.tv[tstp] = 0
+        C.les[C.les_index(0, tstp):C.les_index(tstp, tstp) + 1] = 0
+    incr_convolution(tstp, 1.0, C, A, Acc, B, Bcc, beta, h, SolveOrder)
+
+
+def dyson_timestep_omp(omp_num_threads, n, G, mu, H, Sigma, beta, h, SolveOrder=5):
+    """cntr::dyson_timestep_omp (cntr_dyson_omp_impl.hpp:577-605) on host herm_matrix objects: time
+    step n (> SolveOrder) of G in place, in the OpenMP solver's discretization."""
+    if not _inited:
+        init(0)
+    hd = _fn_data(H)
+    _check(load_library().nessi_gpu_dyson_timestep_omp_host(n, _hp(G), _hp(Sigma), hd.ctypes.data, mu, G.nt, G.ntau,
+                                                            G.size1, G.sig, SolveOrder, beta, h))
+
+
+def vie2_timestep_omp(omp_num_threads, n, G, F, Fcc, Q, beta, h, SolveOrder=5, matsubara_method=2):
+    """cntr::vie2_timestep_omp (cntr_vie2_impl.hpp:2125-2190) on host herm_matrix objects: n = -1
+    vie2_mat, n <= SolveOrder vie2_start of order n (as the reference dispatches), else the
+    element-parallel step on the GPU."""
+    if n <= SolveOrder:
+        if n == 0:
+            raise NessiGpuError(1, "vie2_timestep_omp: an order-0 start (n = 0) is not available")
+        b = Batch([dict(nt=G.nt, ntau=G.ntau, size1=G.size1, sig=G.sig, solve_order=SolveOrder if n < 0 else n,
+                        beta=beta, h=h)])
+        try:
+            b.set_F(0, F, Fcc)
+            b.set_Q(0, Q)
+            b.set_G(0, G)
+            if n < 0:
+                b.vie2_mat(matsubara_method)
+            else:
+                b.vie2_start()
+            b.get_G(0, G)
+        finally:
+            b.close()
+        return
+    if not _inited:
+        init(0)
+    _check(load_library().nessi_gpu_vie2_timestep_omp_host(n, _hp(G), _hp(F), _hp(Fcc), _hp(Q), G.nt, G.ntau, G.size1,
+                                                           G.sig, SolveOrder, beta, h))
 
 
 def convolution(C, A, Acc, B, Bcc, beta, h, SolveOrder=5):

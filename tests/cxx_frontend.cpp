@@ -69,7 +69,7 @@ static void save_hm(const HM &G, const std::string &base) {
 
 int main(int argc, char **argv) {
     if (argc != 3) {
-        std::fprintf(stderr, "usage: %s echo|algebra|mat|dyson|steps|correct|vie2|sin|conv <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s echo|algebra|mat|dyson|steps|correct|vie2|sin|omp|conv <dir>\n", argv[0]);
         return 2;
     }
     const std::string mode = argv[1], dir = std::string(argv[2]) + "/";
@@ -172,6 +172,30 @@ int main(int argc, char **argv) {
             for (int n = k; n <= nt; n++) cntr_gpu::vie2_timestep_sin(n, G, Gsin, F, Fcc, Fsin, Q, Qsin, beta, h, k);
             save_hm(G, dir + "out");
             save(Gsin.d_, dir + "out.fn");
+        } else if (mode == "omp") {  // the OpenMP-path drop-ins: dyson_timestep_omp, vie2_timestep_omp
+            HM Sigma(nt, ntau, s, sig), F(nt, ntau, s, sig), Fcc(nt, ntau, s, sig), G0(nt, ntau, s, sig);
+            HM A(nt, ntau, s, sig), B(nt, ntau, s, sig), C(nt, ntau, s, sig);
+            FN H(nt, s);
+            load_hm(Sigma, dir + "Sigma");
+            load(H.d_, dir + "H.fn");
+            load_hm(G, dir + "G");  // bootstrap (mat and steps 0..k) of the Dyson problem
+            for (int n = k + 1; n <= nt; n++) cntr_gpu::dyson_timestep_omp(4, n, G, mu, H, Sigma, beta, h, k);
+            save_hm(G, dir + "out");
+            // vie2_timestep_omp for every step -1..nt (the reference dispatches n <= k)
+            load_hm(F, dir + "F");
+            load_hm(Fcc, dir + "Fcc");
+            load_hm(G0, dir + "Q");
+            HM V(nt, ntau, s, sig);
+            for (int n = -1; n <= nt; n++) {
+                if (n == 0) continue;  // vie2_start of order n for 1 <= n <= k writes steps 0..n
+                cntr_gpu::vie2_timestep_omp(4, n, V, F, Fcc, G0, beta, h, k);
+            }
+            save_hm(V, dir + "outV");
+            // convolution_timestep_omp of the step k + 3
+            load_hm(A, dir + "Sigma");
+            load_hm(B, dir + "Q");
+            cntr_gpu::convolution_timestep_omp(4, k + 3, C, A, B, beta, h, k);
+            save_hm(C, dir + "outC");
         } else if (mode == "conv") {
             HM A(nt, ntau, s, sig), Acc(nt, ntau, s, sig), B(nt, ntau, s, sig);
             load_hm(A, dir + "A");

@@ -79,3 +79,29 @@ def test_null_arguments_are_rejected_before_the_device():
     assert L.nessi_gpu_convolution_timestep_host(2, None, None, None, None, None, 10, 8, 1, -1, -1, 5, 2.0, 0.05) == 1
     assert L.nessi_gpu_convolution_host(None, None, None, None, None, 10, 8, 1, -1, -1, 5, 2.0, 0.05) == 1
     assert L.nessi_gpu_set_G(None, 0, None, None, None, None) == 1   # no batch
+
+
+def test_element_parallel_entries_reject_bad_arguments_before_the_device():
+    """incr_convolution, convolution_timestep_new, dyson_timestep_omp and vie2_timestep_omp return
+    NESSI_ERR_ARG for null operands, a step the solver does not cover (n <= SolveOrder, which
+    libcntr asserts on: cntr_dyson_omp_impl.hpp:595, cntr_vie2_impl.hpp:2150) and bad
+    dimensions, without touching a device."""
+    import ctypes
+    from nessi_b200 import gpu
+    L = gpu.load_library()
+    z = gpu.HmPtrs(None, None, None, None)
+    one = (gpu.HmPtrs * 1)(z)
+    mu = (ctypes.c_double * 1)(0.0)
+    H = (ctypes.c_void_p * 1)(None)
+    assert L.nessi_gpu_incr_convolution_timestep(3, 1, 1.0, 0.0, one, one, one, None, one, one, 10, 8, 1, -1, -1, 5, 2.0,
+                                                 0.05, None) == 1
+    assert L.nessi_gpu_incr_convolution_component(2, -1, None, 1, 1.0, 0.0, one, one, one, None, one, one, 10, 8, 1,
+                                                  -1, -1, 5, 2.0, 0.05, None) == 1     # tv needs tstp >= 0
+    assert L.nessi_gpu_convolution_timestep_new(3, 1, one, one, one, None, one, one, 10, 8, 1, -1, -1, 5, 2.0, 0.05,
+                                                None) == 1
+    assert L.nessi_gpu_dyson_timestep_omp(5, 1, one, one, H, mu, 10, 8, 1, -1, 5, 2.0, 0.05, None, None) == 1
+    assert b"must exceed SolveOrder" in L.nessi_gpu_last_error()
+    assert L.nessi_gpu_dyson_timestep_omp(7, 1, one, one, H, mu, 10, 8, 1, -1, 5, 2.0, 0.05, None, None) == 1
+    assert L.nessi_gpu_vie2_timestep_omp(4, 1, one, one, one, one, 10, 8, 1, -1, 5, 2.0, 0.05, None, None) == 1
+    assert L.nessi_gpu_vie2_timestep_omp(7, 1, one, one, one, one, 10, 8, 1, -1, 5, 2.0, 0.05, None, None) == 1
+    assert b"null pointer" in L.nessi_gpu_last_error()

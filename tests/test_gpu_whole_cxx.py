@@ -235,3 +235,44 @@ def test_convolution_through_the_cxx_frontend(oracle, tmp_path):
     C = read_out(d, nt, ntau, s, -1)
     for c in ("ret", "les", "tv", "mat"):
         assert rel_err(getattr(C, c), getattr(R, c)) < TOL, c
+
+
+def _read_prefix(d, prefix, nt, ntau, s, sig):
+    G = herm_matrix(nt, ntau, s, sig)
+    for c in ("ret", "les", "tv", "mat"):
+        a = getattr(G, c)
+        a[...] = np.fromfile(str(d / ("%s.%s" % (prefix, c))), np.complex128).reshape(a.shape)
+    return G
+
+
+@pytest.mark.gpu
+def test_omp_dropins_through_the_cxx_frontend(oracle, tmp_path):
+    """cntr_gpu::dyson_timestep_omp (n = k+1..nt), cntr_gpu::vie2_timestep_omp (n = -1, 1..nt, with
+    the reference's dispatch of n <= k) and cntr_gpu::convolution_timestep_omp from a libcntr-style
+    program, against the oracle's restatement of the OpenMP path."""
+    exe = build_frontend(tmp_path)
+    rng = np.random.default_rng(53)
+    nt, ntau, s, beta, h, k, mu = 22, 14, 2, 3.0, 0.05, 4, 0.1
+    Sigma = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.6)
+    H = make_H(rng, nt, s, h)
+    G = herm_matrix(nt, ntau, s, -1)
+    oracle.dyson_mat(G, Sigma, mu, H, beta, k)
+    oracle.dyson_start(G, mu, H, Sigma, beta, h, k)
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Q = _source(oracle, rng, nt, ntau, s, beta, h)
+    d = tmp_path / "omp"
+    write_case(d, (nt, ntau, s, -1, k, beta, h, mu), Sigma=Sigma, G=G, F=F, Fcc=Fcc, Q=Q, H=H.data)
+    run(exe, "omp", d)
+    refG = G.copy()
+    for n in range(k + 1, nt + 1):
+        oracle.dyson_timestep_omp(n, refG, mu, H, Sigma, beta, h, k)
+    refV = herm_matrix(nt, ntau, s, -1)
+    for n in range(-1, nt + 1):
+        if n != 0:
+            oracle.vie2_timestep_omp(n, refV, F, Fcc, Q, beta, h, k)
+    refC = herm_matrix(nt, ntau, s, -1)
+    oracle.convolution_timestep_new(k + 3, refC, Sigma, Sigma, Q, Q, beta, h, k)
+    for prefix, ref in (("out", refG), ("outV", refV), ("outC", refC)):
+        got = _read_prefix(d, prefix, nt, ntau, s, -1)
+        for c in ("ret", "les", "tv", "mat"):
+            assert rel_err(getattr(got, c), getattr(ref, c)) < TOL, (prefix, c)
