@@ -94,6 +94,7 @@ template <class HM, class FN> class Batch {
     void set_F(HM &F, HM &Fcc, int group = 0) {
         check(nessi_gpu_set_F(b_, group, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0),
                               Fcc.retptr(0, 0), Fcc.lesptr(0, 0)));
+        check(nessi_gpu_set_Fcc_mat(b_, group, Fcc.matptr(0)));  // read by the steepest-descent vie2_mat
     }
     void set_Q(int p, HM &Q) {
         check(nessi_gpu_set_Q(b_, p, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0)));
@@ -168,7 +169,7 @@ constexpr int MAT_FOURIER = 0;
 constexpr int MAT_CG = 1;
 constexpr int MAT_FIXPOINT = 2;
 inline void require_device_method(int method, bool vie = false) {
-    if (method != MAT_FOURIER && method != MAT_FIXPOINT && (vie || method != MAT_CG))
+    if (method != MAT_FOURIER && method != MAT_FIXPOINT && method != MAT_CG)
         throw std::invalid_argument("cntr_gpu: Matsubara method " + std::to_string(method) +
                                     " is not available on the device for " + (vie ? "vie2_mat" : "dyson_mat"));
 }
@@ -338,6 +339,7 @@ template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double
                      : nessi_gpu_set_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));
     if (!rc) rc = nessi_gpu_set_F(b, 0, F.retptr(0, 0), F.lesptr(0, 0), F.tvptr(0, 0), F.matptr(0), Fcc.retptr(0, 0),
                                   Fcc.lesptr(0, 0));
+    if (!rc) rc = nessi_gpu_set_Fcc_mat(b, 0, Fcc.matptr(0));
     if (!rc) rc = nessi_gpu_set_Q(b, 0, Q.retptr(0, 0), Q.lesptr(0, 0), Q.tvptr(0, 0), Q.matptr(0));
     if (rc) {
         nessi_gpu_batch_destroy(b);
@@ -351,13 +353,13 @@ template <class HM> nessi_batch *vie2_batch(HM &G, HM &F, HM &Fcc, HM &Q, double
 template <class HM>
 void vie2_mat(HM &G, HM &F, HM &Fcc, HM &Q, double beta, int SolveOrder = 5, int method = MAT_FIXPOINT) {
     require_device_method(method, true);
-    (void)Fcc;  // F^mat alone enters the Matsubara equation
     nessi_problem_desc d;
     d.nt = SolveOrder; d.ntau = G.ntau(); d.size1 = G.size1(); d.sig = G.sig();
     d.solve_order = SolveOrder; d.sigma_group = 0; d.beta = beta; d.h = 1.0; d.mu = 0.0;
     nessi_batch *b = nullptr;
     check(nessi_gpu_batch_create(&b, &d, 1, NESSI_PREC_FP64));
     int rc = nessi_gpu_set_F(b, 0, nullptr, nullptr, nullptr, F.matptr(0), nullptr, nullptr);
+    if (!rc && method == MAT_CG) rc = nessi_gpu_set_Fcc_mat(b, 0, Fcc.matptr(0));  // steepest descent reads Fcc^mat
     if (!rc) rc = nessi_gpu_set_Q(b, 0, nullptr, nullptr, nullptr, Q.matptr(0));
     if (!rc) rc = nessi_gpu_vie2_mat_method(b, method);
     if (!rc) rc = nessi_gpu_get_G(b, 0, nullptr, nullptr, nullptr, G.matptr(0));

@@ -122,9 +122,13 @@ int nessi_gpu_set_Q_timestep(nessi_batch *b, int p, int tstp, const void *slice)
  * from the group's F^mat and the problem's Q^mat.  ntau must be even. */
 int nessi_gpu_vie2_mat(nessi_batch *b);
 /* The same with libcntr's method argument (cntr_vie2_impl.hpp:1229-1250): 0 = CNTR_MAT_FOURIER
- * (vie2_mat_fourier with 20 oversampling copies, no corrections), 2 = CNTR_MAT_FIXPOINT.
- * Method 1 (steepest descent) needs Fcc^mat, which nessi_gpu_set_F does not take: NESSI_ERR_ARG. */
+ * (vie2_mat_fourier with 20 oversampling copies, no corrections), 1 = CNTR_MAT_CG (vie2_mat_steep,
+ * :486-600: a Fourier start, then at most 40 conjugate-gradient iterations to 1e-12; needs the
+ * group's Fcc^mat from nessi_gpu_set_Fcc_mat, NESSI_ERR_ARG without it), 2 = CNTR_MAT_FIXPOINT. */
 int nessi_gpu_vie2_mat_method(nessi_batch *b, int method);
+/* Fcc^mat of a VIE2 group (the Matsubara part of the Fcc argument of cntr::vie2_mat,
+ * cntr_vie2_decl.hpp:63), host pointer, (ntau+1) s^2; read by the steepest-descent vie2_mat only. */
+int nessi_gpu_set_Fcc_mat(nessi_batch *b, int group, const void *cc_mat);
 /* cntr::vie2_start(G, F, Fcc, Q, SolveOrder, beta, h) (cntr_vie2_decl.hpp:67,
  * cntr_vie2_impl.hpp:1338-1420): time steps 0..k of every VIE2 problem from G^mat. */
 int nessi_gpu_vie2_start(nessi_batch *b);

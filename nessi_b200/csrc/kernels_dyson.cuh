@@ -37,6 +37,7 @@ struct GroupDev {
     double2 *Kmat;     // ((ntau+1)s) x ((ntau+1)s) row-major: Matsubara operator of the step
     double2 *Gmat_all; // ((ntau+1)s) x ldc: every problem's G^mat as columns
     double2 *Cmat;     // ((ntau+1)s) x ldc: Matsubara part of the tv right-hand side
+    const double2 *fccmat;  // Fcc^mat of a VIE2 group (steepest-descent vie2_mat), or null
     int ntmax, ntau, s, sig, k;
     int ldc;           // >= nprob * s
     double h, beta;

@@ -498,7 +498,9 @@ __global__ void __launch_bounds__(256) k_dyson_mat(GroupDev g, const ProbDev *__
 // 460-484, 1091-1160): G^mat = vie2_mat_fourier(F, Q) (:305-455), then 6 corrections
 // G -= fourier(F, F*G + G - Q).  F^mat is the group's (g.smat), Q^mat of the problem is in w.G0.
 // One CTA per problem.
-// method 0: the Fourier solve alone with 20 oversampling copies (vie2_mat_fourier, :1280-1336).
+// method 0: the Fourier solve alone with 20 oversampling copies (vie2_mat_fourier, :1280-1336);
+// method 1: steepest descent (vie2_mat_steep, :486-600, 1241-1244: 40 iterations, tol 1e-12) with
+// the group's Fcc^mat.
 template <int S>
 __global__ void __launch_bounds__(256) k_vie2_mat(GroupDev g, const ProbDev *__restrict__ probs, MatScratch *scr,
                                                   int method) {
@@ -519,6 +521,13 @@ __global__ void __launch_bounds__(256) k_vie2_mat(GroupDev g, const ProbDev *__r
     __syncthreads();
     if (method == 0) {
         vie2_mat_fourier_dev<S>(p.gmat, g.smat, w.G0, w.fdft, w.qdft, w.Z, qmasy, ntau, sig, beta, 20, tw);
+        return;
+    }
+    if (method == 1) {
+        __shared__ double red[256];  // blockDim.x = 256
+        // after the Fourier start the Fourier buffers hold the iteration: R = dG, P = fdft, AP = qdft, T = Z
+        vie2_mat_steep_dev<S>(p.gmat, g.smat, g.fccmat, w.G0, w.fdft, w.qdft, w.Z, qmasy, w.dG, w.fdft, w.qdft, w.Z,
+                              red, k, ntau, sig, beta, 40, 1.0e-12, tw);
         return;
     }
     const int pcf = 5;

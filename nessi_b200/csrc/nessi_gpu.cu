@@ -133,6 +133,7 @@ struct Group {
     bool vie = false;                // VIE2 group: s* hold F, fcc* hold Fcc (nessi_gpu_set_F)
     int pp_ret = 0, pp_les = 0;      // Volterra kernel chosen by the autotuner (0: not yet)
     double2 *fccret = nullptr, *fccles = nullptr;
+    double2 *fccmat = nullptr;       // Fcc^mat of a VIE2 group (nessi_gpu_set_Fcc_mat; steepest descent)
     double2 *U = nullptr;            // diagonal interaction U(t), (ntmax+2) x s, t = -1 first
     double2 *accr = nullptr, *accl = nullptr, *panel = nullptr;  // cluster Volterra path
     std::vector<int> members;        // problem indices, nt descending
@@ -223,6 +224,7 @@ GroupDev group_dev(const Group &g) {
     d.Ldense = g.Ldense; d.Tdense = g.Tdense; d.tvcoef = g.tvcoef;
     d.badv = g.badv; d.btv = g.btv; d.gles = g.gles;
     d.Kmat = g.Kmat; d.Gmat_all = g.Gmat_all; d.Cmat = g.Cmat;
+    d.fccmat = g.fccmat;
     d.ntmax = g.ntmax; d.ntau = g.ntau; d.s = g.s; d.sig = g.sig; d.k = g.k;
     d.ldc = g.ldc; d.h = g.h; d.beta = g.beta;
     return d;
@@ -1257,12 +1259,11 @@ int nessi_gpu_read_profile(nessi_batch *b, int kernel, double *ms, long long *la
 }
 
 // libcntr's Matsubara methods (cntr_global_settings.hpp): 0 Fourier, 1 steepest descent (CG), 2 fixpoint.
-// vie2_mat by steepest descent needs Fcc^mat, which a VIE2 group does not hold (set_F takes Fcc's
-// retarded and lesser components only), so it is refused there.
+// vie2_mat by steepest descent also needs Fcc^mat (nessi_gpu_set_Fcc_mat; checked per group).
 static int check_mat_method(int method, bool vie, const char *name) {
-    if (method == 0 || method == 2 || (method == 1 && !vie)) return NESSI_OK;
-    set_err("%s: method %d not available (%s)", name, method,
-            vie ? "0 = Fourier, 2 = fixpoint" : "0 = Fourier, 1 = steepest descent, 2 = fixpoint");
+    (void)vie;
+    if (method == 0 || method == 1 || method == 2) return NESSI_OK;
+    set_err("%s: method %d not available (0 = Fourier, 1 = steepest descent, 2 = fixpoint)", name, method);
     return NESSI_ERR_ARG;
 }
 
@@ -1320,6 +1321,10 @@ int nessi_gpu_vie2_mat_method(nessi_batch *b, int method) {
         if (!g.vie) continue;
         any = true;
         if (g.ntau % 2) { set_err("vie2_mat: ntau must be even (matsubara_inverse)"); return NESSI_ERR_ARG; }
+        if (method == 1 && !g.fccmat) {
+            set_err("vie2_mat: steepest descent needs Fcc^mat of the group (nessi_gpu_set_Fcc_mat)");
+            return NESSI_ERR_ARG;
+        }
         CKR(vie2_mat_dispatch(b, g, method));
     }
     if (!any) { set_err("vie2_mat: the batch has no VIE2 group (nessi_gpu_set_F)"); return NESSI_ERR_ARG; }
@@ -1395,6 +1400,19 @@ int nessi_gpu_set_F(nessi_batch *b, int group, const void *ret, const void *les,
     CKR(copy_cplx(b, g->fccles, cc_les, tri_h(N) * s2, cudaMemcpyHostToDevice));
     CK(cudaStreamSynchronize(b->stream));
     g->ret_valid = g->les_valid = g->dense_valid = -1;
+    return NESSI_OK;
+}
+
+int nessi_gpu_set_Fcc_mat(nessi_batch *b, int group, const void *cc_mat) {
+    Group *g;
+    CKR(find_group_checked(b, group, &g));
+    if (g->U) { set_err("set_Fcc_mat: group %d is a lattice (Dyson) group", group); return NESSI_ERR_ARG; }
+    if (!cc_mat) { set_err("set_Fcc_mat: null Fcc^mat"); return NESSI_ERR_ARG; }
+    CKR(ensure_fcc(b, *g));
+    const long M = g->ntau + 1, s2 = (long)g->s * g->s;
+    if (!g->fccmat) CKR(b->alloc(&g->fccmat, M * s2));
+    CKR(copy_cplx(b, g->fccmat, cc_mat, M * s2, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(b->stream));
     return NESSI_OK;
 }
 

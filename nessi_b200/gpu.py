@@ -70,6 +70,7 @@ EXPORTS = {
                                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p]),
     "nessi_gpu_set_F": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 6),
+    "nessi_gpu_set_Fcc_mat": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "nessi_gpu_set_F_timestep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                 ctypes.c_void_p]),
     "nessi_gpu_set_Q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 4),
@@ -260,6 +261,8 @@ class Batch:
         """Kernel F of a group (and its partner Fcc); makes the group a VIE2 group."""
         _check(load_library().nessi_gpu_set_F(self._h, group, _ptr(F.ret), _ptr(F.les), _ptr(F.tv), _ptr(F.mat),
                                               _ptr(Fcc.ret), _ptr(Fcc.les)))
+        if Fcc.mat is not None and Fcc.mat.size:  # Fcc^mat: the steepest-descent vie2_mat reads it
+            _check(load_library().nessi_gpu_set_Fcc_mat(self._h, group, _ptr(Fcc.mat)))
 
     def set_F_timestep(self, group, tstp, F_slice, Fcc_slice=None):
         fs = np.ascontiguousarray(F_slice, np.complex128)
@@ -666,18 +669,17 @@ def _value_at_minus1(X, s):
 def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None, method=2, force_hermitian=True):
     """cntr::dyson_mat(G, mu, H, Sigma, beta, SolveOrder, method, force_hermitian)
     (cntr_dyson_decl.hpp:77-79): writes G^mat; method 0 = Fourier (dyson_mat_fourier_dispatch,
-    cntr_dyson_impl.hpp:356-446), 1 = steepest descent (dyson_mat_steep_dispatch, :519-540; not with
-    SigmaMF), 2 = fixpoint (the default).  With ``SigmaMF`` (a cntr::function
-    or the (s, s) matrix of its value at -1) it is the mean-field overload
-    dyson_mat(G, mu, H, SigmaMF, Sigma, beta, SolveOrder, method) (:81-83; cntr_dyson_impl.hpp:
-    472-492, 1270-1298): the Fourier method takes H(-1) + SigmaMF(-1) as the one-body part; the
-    fixpoint method, with G0 the free propagator of H(-1), solves [1 + F] G = G0 with
-    F = -(G0 * Sigma + G0 SigmaMF(-1)); the convolution and the solves run on the GPU."""
+    cntr_dyson_impl.hpp:356-446), 1 = steepest descent (dyson_mat_steep_dispatch, :519-540), 2 =
+    fixpoint (the default).  With ``SigmaMF`` (a cntr::function or the (s, s) matrix of its value
+    at -1) it is the mean-field overload dyson_mat(G, mu, H, SigmaMF, Sigma, beta, SolveOrder,
+    method) (:81-83; cntr_dyson_impl.hpp:472-575, 1270-1298): the Fourier method takes
+    H(-1) + SigmaMF(-1) as the one-body part; with G0 the free propagator of H(-1), the fixpoint
+    method solves [1 + F] G = G0 with F = -(G0 * Sigma + G0 SigmaMF(-1)), and steepest descent the
+    same with Fcc = -(Sigma * G0 + SigmaMF(-1) G0) (:545-572); the convolutions and the solves run
+    on the GPU."""
     from .equilibrium import green_from_H
     k, s, ntau, sig = SolveOrder, G.size1, G.ntau, G.sig
     h0 = _value_at_minus1(H, s)
-    if SigmaMF is not None and method == 1:
-        raise ValueError("dyson_mat: the steepest-descent method with SigmaMF is not available on the device")
     if SigmaMF is not None and method == 0:
         h0 = h0 + _value_at_minus1(SigmaMF, s)
         SigmaMF = None
@@ -703,11 +705,17 @@ def dyson_mat(G, mu, H, Sigma, beta, SolveOrder=5, SigmaMF=None, method=2, force
     convolution_timestep(-1, C, G0, G0, Sk, Sk, beta, 1.0, k)  # convolution_matsubara(G0, Sigma)
     F = herm_matrix(k, ntau, s, sig)
     F.mat[...] = -(C.mat + G0.mat @ mf)
+    Fcc = F
+    if method == 1:
+        Cc = herm_matrix(k, ntau, s, sig)
+        convolution_timestep(-1, Cc, Sk, Sk, G0, G0, beta, 1.0, k)  # convolution_matsubara(Sigma, G0)
+        Fcc = herm_matrix(k, ntau, s, sig)
+        Fcc.mat[...] = -(Cc.mat + mf @ G0.mat)
     b = Batch([desc])
     try:
-        b.set_F(0, F, F)
+        b.set_F(0, F, Fcc)
         b.set_Q(0, G0)
-        b.vie2_mat()
+        b.vie2_mat(1 if method == 1 else 2)
         b.get_G(0, out)
     finally:
         b.close()

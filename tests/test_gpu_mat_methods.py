@@ -1,7 +1,7 @@
 """The Matsubara solvers' method argument on the GPU against the oracle: dyson_mat with
 CNTR_MAT_FOURIER (dyson_mat_fourier_dispatch, cntr_dyson_impl.hpp:356-446), CNTR_MAT_CG
 (dyson_mat_steep_dispatch, :519-540) and the fixpoint, force_hermitian on and off (:1393-1450),
-and vie2_mat with the Fourier method (cntr_vie2_impl.hpp:1229-1250).  Bar: 1e-10 relative; and
+and vie2_mat with the Fourier and steepest-descent methods (cntr_vie2_impl.hpp:1229-1250).  Bar: 1e-10 relative; and
 libcntr's own known answer for all three dyson_mat methods with its bounds."""
 import numpy as np
 import pytest
@@ -86,12 +86,39 @@ def _padded(S, nt):
     return P
 
 
-def test_vie2_mat_steepest_descent_refused():
+@pytest.mark.parametrize("s", [1, 2, 3])
+def test_vie2_mat_steepest_descent(oracle, s):
+    """vie2_mat by steepest descent (vie2_mat_steep, cntr_vie2_impl.hpp:486-600, 1241-1244) with a
+    non-hermitian kernel F = -A*B and its partner Fcc = -B*A, against the oracle; without
+    Fcc^mat the method is refused."""
     from nessi_b200 import gpu
-    b = gpu.Batch([dict(nt=6, ntau=10, size1=1, sig=-1, solve_order=5, beta=5.0, h=0.05, mu=0.0)])
-    F = herm_matrix(6, 10, 1, -1)
-    b.set_F(0, F, F)
-    b.set_Q(0, F)
+    rng = np.random.default_rng(950 + s)
+    nt, ntau, beta, h, k = 6, 16, 4.0, 0.05, 5
+    A = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.6)
+    B = make_sigma(oracle, rng, nt, ntau, s, -1, beta, h, lam=0.5)
+    F, Fcc = herm_matrix(nt, ntau, s, -1), herm_matrix(nt, ntau, s, -1)
+    oracle.convolution_matsubara(F, A, B, beta, k)
+    oracle.convolution_matsubara(Fcc, B, A, beta, k)
+    F.mat[...] *= -1.0
+    Fcc.mat[...] *= -1.0
+    Q = herm_matrix(nt, ntau, s, -1)
+    oracle.green_from_H(Q, 0.1, rand_herm(rng, s, 0.8), beta, h)
+    Go = herm_matrix(nt, ntau, s, -1)
+    oracle.vie2_mat(Go, F, Fcc, Q, beta, k, method=CG)
+    b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, beta=beta, h=h)])
+    b.set_F(0, F, Fcc)
+    b.set_Q(0, Q)
+    b.vie2_mat(CG)
+    m = np.zeros((ntau + 1, s, s), np.complex128)
+    b.get_timestep(0, -1, m)
+    b.close()
+    assert rel_err(m, Go.mat) < TOL
+    # a group given Fcc's ret and les only (no Fcc^mat) cannot run it
+    L = gpu.load_library()
+    b = gpu.Batch([dict(nt=nt, ntau=ntau, size1=s, sig=-1, solve_order=k, beta=beta, h=h)])
+    gpu._check(L.nessi_gpu_set_F(b._h, 0, gpu._ptr(F.ret), gpu._ptr(F.les), gpu._ptr(F.tv), gpu._ptr(F.mat),
+                                 gpu._ptr(Fcc.ret), gpu._ptr(Fcc.les)))
+    b.set_Q(0, Q)
     with pytest.raises(gpu.NessiGpuError) as ei:
         b.vie2_mat(CG)
     assert ei.value.code == 1

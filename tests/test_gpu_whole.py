@@ -111,6 +111,30 @@ def test_dyson_mat_mean_field_overload(oracle, s):
     assert rel_err(G.mat, alt.mat) < 1e-9    # the two formulations agree to the fixpoint's convergence
 
 
+@pytest.mark.parametrize("s", [1, 2])
+def test_dyson_mat_mean_field_steepest_descent(oracle, s):
+    """dyson_mat(G, mu, H, SigmaMF, Sigma, ..., CNTR_MAT_CG) (dyson_mat_steep_dispatch with SigmaMF,
+    cntr_dyson_impl.hpp:545-572): against the same steps on the oracle (F = -(G0 * Sigma + G0 SigmaMF),
+    Fcc = -(Sigma * G0 + SigmaMF G0), vie2_mat steepest descent, force_matsubara_hermitian)."""
+    from nessi_b200 import gpu
+    ntau, beta, k, mu = 200, 5.0, 5, 0.1
+    Sig, H, h0, mf = _mat_problem(oracle, 90 + s, s, ntau, beta)
+    G0 = herm_matrix(-1, ntau, s, -1)
+    oracle.green_from_H(G0, mu, h0, beta, 1.0)
+    C, Cc = herm_matrix(-1, ntau, s, -1), herm_matrix(-1, ntau, s, -1)
+    oracle.convolution_matsubara(C, G0, Sig, beta, k)
+    oracle.convolution_matsubara(Cc, Sig, G0, beta, k)
+    F, Fcc = herm_matrix(-1, ntau, s, -1), herm_matrix(-1, ntau, s, -1)
+    F.mat[...] = -(C.mat + G0.mat @ mf)
+    Fcc.mat[...] = -(Cc.mat + mf @ G0.mat)
+    ref = herm_matrix(-1, ntau, s, -1)
+    oracle.vie2_mat(ref, F, Fcc, G0, beta, k, method=1)
+    oracle.force_matsubara_hermitian(ref)
+    G = herm_matrix(-1, ntau, s, -1)
+    gpu.dyson_mat(G, mu, H, Sig, beta, k, SigmaMF=mf, method=1)
+    assert rel_err(G.mat, ref.mat) < TOL
+
+
 def test_vie2_timestep_sin(oracle):
     """gpu.vie2_timestep_sin through a propagation (n = -1, the start at n = k, then every step)
     against the oracle's restatement of cntr_vie2_impl.hpp:1779-1838, regular part and Gsin."""
