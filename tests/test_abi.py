@@ -105,3 +105,15 @@ def test_element_parallel_entries_reject_bad_arguments_before_the_device():
     assert L.nessi_gpu_vie2_timestep_omp(4, 1, one, one, one, one, 10, 8, 1, -1, 5, 2.0, 0.05, None, None) == 1
     assert L.nessi_gpu_vie2_timestep_omp(7, 1, one, one, one, one, 10, 8, 1, -1, 5, 2.0, 0.05, None, None) == 1
     assert b"null pointer" in L.nessi_gpu_last_error()
+
+
+def test_vie2_timestep_omp_order0_start_is_refused_without_a_device():
+    """The reference dispatches vie2_timestep_omp(0, ...) to an order-0 vie2_start, which this
+    library does not provide: the Python drop-in refuses it with NESSI_ERR_ARG before any device
+    call."""
+    import pytest
+    from nessi_b200 import gpu, herm_matrix
+    G = herm_matrix(8, 6, 1, -1)
+    with pytest.raises(gpu.NessiGpuError) as e:
+        gpu.vie2_timestep_omp(4, 0, G, G, G, G, 2.0, 0.05, 5)
+    assert e.value.code == 1

@@ -200,3 +200,44 @@ def test_vie2_omp_embedding_known_answer_on_gpu(oracle):
     Ga = dG.host()
     err = sum(O.distance_norm2(t, c["Gx"], Ga) for t in range(Nt + 1))
     assert err / Nt < 1.0e-6
+
+
+def test_python_dropins_on_host_data(oracle):
+    """The host-data drop-ins with libcntr's signatures: gpu.dyson_timestep_omp (n = k+1..nt),
+    gpu.vie2_timestep_omp (n = -1, 1..nt: vie2_mat, the starts of order n as the reference
+    dispatches them, then the element-parallel step), gpu.incr_convolution with a function F and
+    gpu.convolution_timestep_omp, each against the oracle."""
+    from nessi_b200 import gpu
+    from test_gpu_vie2 import _kernel_pair, _source
+    rng = np.random.default_rng(2024)
+    s, sig, k, nt, ntau, beta, h, mu = 2, -1, 4, 18, 12, 3.0, 0.05, 0.2
+    Sig = make_sigma(oracle, rng, nt, ntau, s, sig, beta, h, lam=0.6)
+    H = make_H(rng, nt, s, h)
+    G = herm_matrix(nt, ntau, s, sig)
+    oracle.dyson_mat(G, Sig, mu, H, beta, k)
+    oracle.dyson_start(G, mu, H, Sig, beta, h, k)
+    R = G.copy()
+    for n in range(k + 1, nt + 1):
+        gpu.dyson_timestep_omp(4, n, G, mu, H, Sig, beta, h, k)
+        oracle.dyson_timestep_omp(n, R, mu, H, Sig, beta, h, k)
+    for comp in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(G, comp), getattr(R, comp)) < TOL, ("dyson", comp)
+    F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
+    Q = _source(oracle, rng, nt, ntau, s, beta, h)
+    V, RV = herm_matrix(nt, ntau, s, sig), herm_matrix(nt, ntau, s, sig)
+    for n in [-1] + list(range(1, nt + 1)):
+        gpu.vie2_timestep_omp(4, n, V, F, Fcc, Q, beta, h, k)
+        oracle.vie2_timestep_omp(n, RV, F, Fcc, Q, beta, h, k)
+    for comp in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(V, comp), getattr(RV, comp)) < TOL, ("vie2", comp)
+    A, Acc = _pair(oracle, rng, nt, ntau, s, sig, beta, h, k)
+    ft = _func(rng, nt, s)
+    C = make_sigma(oracle, rng, nt, ntau, s, sig, beta, h, lam=0.3)
+    RC = C.copy()
+    for n in (-1, 2, 9, nt):
+        gpu.incr_convolution(n, 0.6 + 0.2j, C, A, Acc, Sig, Sig, beta, h, k, ft=ft)
+        oracle.incr_convolution(n, 0.6 + 0.2j, RC, A, Acc, Sig, Sig, beta, h, k, ft=ft)
+    gpu.convolution_timestep_omp(4, 11, C, A, Acc, Sig, Sig, beta, h, k)
+    oracle.convolution_timestep_new(11, RC, A, Acc, Sig, Sig, beta, h, k)
+    for comp in ("ret", "les", "tv", "mat"):
+        assert rel_err(getattr(C, comp), getattr(RC, comp)) < TOL, ("incr", comp)
