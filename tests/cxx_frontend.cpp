@@ -195,6 +195,11 @@ int main(int argc, char **argv) {
             load_hm(A, dir + "Sigma");
             load_hm(B, dir + "Q");
             cntr_gpu::convolution_timestep_omp(4, k + 3, C, A, B, beta, h, k);
+            // C += (0.5 - 0.25i) A * F * B at steps -1 and k + 1 with the function F of the case
+            FN Ff(nt, s);
+            load(Ff.d_, dir + "Ff.fn");
+            for (int n : {-1, k + 1})
+                cntr_gpu::incr_convolution(n, cplx(0.5, -0.25), C, A, A, Ff, B, B, beta, h, k);
             save_hm(C, dir + "outC");
         } else if (mode == "conv") {
             HM A(nt, ntau, s, sig), Acc(nt, ntau, s, sig), B(nt, ntau, s, sig);

@@ -248,8 +248,9 @@ def _read_prefix(d, prefix, nt, ntau, s, sig):
 @pytest.mark.gpu
 def test_omp_dropins_through_the_cxx_frontend(oracle, tmp_path):
     """cntr_gpu::dyson_timestep_omp (n = k+1..nt), cntr_gpu::vie2_timestep_omp (n = -1, 1..nt, with
-    the reference's dispatch of n <= k) and cntr_gpu::convolution_timestep_omp from a libcntr-style
-    program, against the oracle's restatement of the OpenMP path."""
+    the reference's dispatch of n <= k), cntr_gpu::convolution_timestep_omp and
+    cntr_gpu::incr_convolution with a function F from a libcntr-style program, against the
+    oracle's restatement of the OpenMP path."""
     exe = build_frontend(tmp_path)
     rng = np.random.default_rng(53)
     nt, ntau, s, beta, h, k, mu = 22, 14, 2, 3.0, 0.05, 4, 0.1
@@ -260,8 +261,12 @@ def test_omp_dropins_through_the_cxx_frontend(oracle, tmp_path):
     oracle.dyson_start(G, mu, H, Sigma, beta, h, k)
     F, Fcc = _kernel_pair(oracle, rng, nt, ntau, s, beta, h, k)
     Q = _source(oracle, rng, nt, ntau, s, beta, h)
+    Ff = np.zeros((nt + 2, s, s), np.complex128)
+    x = rng.normal(0, 0.4, (s, s)) + 1j * rng.normal(0, 0.4, (s, s))
+    for t in range(-1, nt + 1):
+        Ff[t + 1] = np.eye(s) + np.sin(0.2 * t) * x
     d = tmp_path / "omp"
-    write_case(d, (nt, ntau, s, -1, k, beta, h, mu), Sigma=Sigma, G=G, F=F, Fcc=Fcc, Q=Q, H=H.data)
+    write_case(d, (nt, ntau, s, -1, k, beta, h, mu), Sigma=Sigma, G=G, F=F, Fcc=Fcc, Q=Q, H=H.data, Ff=Ff)
     run(exe, "omp", d)
     refG = G.copy()
     for n in range(k + 1, nt + 1):
@@ -272,6 +277,8 @@ def test_omp_dropins_through_the_cxx_frontend(oracle, tmp_path):
             oracle.vie2_timestep_omp(n, refV, F, Fcc, Q, beta, h, k)
     refC = herm_matrix(nt, ntau, s, -1)
     oracle.convolution_timestep_new(k + 3, refC, Sigma, Sigma, Q, Q, beta, h, k)
+    for n in (-1, k + 1):
+        oracle.incr_convolution(n, 0.5 - 0.25j, refC, Sigma, Sigma, Q, Q, beta, h, k, ft=Ff)
     for prefix, ref in (("out", refG), ("outV", refV), ("outC", refC)):
         got = _read_prefix(d, prefix, nt, ntau, s, -1)
         for c in ("ret", "les", "tv", "mat"):
