@@ -2060,11 +2060,10 @@ int omp_common_checks(const char *name, int tstp, int nt, int ntau, int size1, i
     return ensure_tables(dev);
 }
 
-// incr_convolution over components `which` (-1: every component of tstp, mat for tstp = -1)
-int incr_run(const char *name, int which, int tstp, const unsigned char *mask, int count, double2 alpha,
-             const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc, const void *const *ft,
-             const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a, int sig_b,
-             int solve_order, double beta, double h, void *stream) {
+// the arguments of an incr_convolution call, checked before anything is queued
+int incr_check(const char *name, int which, int tstp, int count, const nessi_hm_ptrs *C, const nessi_hm_ptrs *A,
+               const nessi_hm_ptrs *Acc, const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau,
+               int size1, int sig_a, int sig_b, int solve_order, double beta, double h) {
     if (count < 0 || (count > 0 && (!C || !A || !Acc || !B || !Bcc)) || (sig_a != 1 && sig_a != -1) ||
         (sig_b != 1 && sig_b != -1) || which < -1 || which > 3 || (which == 0 && tstp != -1) ||
         (which > 0 && tstp < 0)) {
@@ -2078,7 +2077,15 @@ int incr_run(const char *name, int which, int tstp, const unsigned char *mask, i
             for (const nessi_hm_ptrs *x : all) ok = ok && x->ret && x->les && x->tv;
         if (!ok) { set_err("%s: problem %d has a null pointer it needs", name, i); return NESSI_ERR_ARG; }
     }
-    CKR(omp_common_checks(name, tstp, nt, ntau, size1, solve_order, beta, h));
+    return omp_common_checks(name, tstp, nt, ntau, size1, solve_order, beta, h);
+}
+
+// incr_convolution over components `which` (-1: every component of tstp, mat for tstp = -1)
+int incr_run(const char *name, int which, int tstp, const unsigned char *mask, int count, double2 alpha,
+             const nessi_hm_ptrs *C, const nessi_hm_ptrs *A, const nessi_hm_ptrs *Acc, const void *const *ft,
+             const nessi_hm_ptrs *B, const nessi_hm_ptrs *Bcc, int nt, int ntau, int size1, int sig_a, int sig_b,
+             int solve_order, double beta, double h, void *stream) {
+    CKR(incr_check(name, which, tstp, count, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b, solve_order, beta, h));
     cudaStream_t st = (cudaStream_t)stream;
     for (int i0 = 0; i0 < count; i0 += NESSI_OMP_MAXP) {
         OmpBatch ob;
@@ -2132,10 +2139,8 @@ extern "C" int nessi_gpu_convolution_timestep_new(int tstp, int count, const nes
                                                   int size1, int sig_a, int sig_b, int solve_order, double beta,
                                                   double h, void *stream) {
     NvtxRange nvtx_("nessi::convolution_timestep_new");
-    if (count < 0 || (count > 0 && !C) || size1 < 1 || size1 > NESSI_MAXS || tstp < -1 || tstp > nt || ntau < 0) {
-        set_err("convolution_timestep_new: bad arguments");
-        return NESSI_ERR_ARG;
-    }
+    CKR(incr_check("convolution_timestep_new", -1, tstp, count, C, A, Acc, B, Bcc, nt, ntau, size1, sig_a, sig_b,
+                   solve_order, beta, h));
     // C.set_timestep_zero(tstp): ret row, tv row and les column of tstp are contiguous
     const long s2 = (long)size1 * size1, M = ntau + 1;
     cudaStream_t st = (cudaStream_t)stream;
