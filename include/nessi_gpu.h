@@ -290,7 +290,10 @@ int nessi_gpu_convolution_timestep_new(int tstp, int count, const nessi_hm_ptrs 
  * step a GPU thread: G^R(n, j) and, for n >= 2k+1, G^<(j, n) for j < n-k from the equation in
  * the other time argument (BD(k+1) derivatives), the k x k start block and the last k+1 lesser
  * rows as the serial step; G^tv as the serial step.  Not the serial dyson_timestep's
- * discretization: the two differ by O(h^(k+1)).  H[i] is a device pointer to problem i's
+ * discretization: when G's mat and steps 0..k solve the same equation (dyson_mat, dyson_start)
+ * the two agree to the discretization error; from a start that does not, they can differ by far
+ * more, since the two time arguments' equations agree only for a solution.  H[i] is a device
+ * pointer to problem i's
  * cntr::function H (H(-1) first), mu[i] its chemical potential (host array); requires
  * SolveOrder + 1 <= n.  If `status` (a DEVICE int) is not NULL it is set to 1 when a step matrix
  * is singular.  No counterpart of the thread count: the device decides. */
